@@ -1,0 +1,221 @@
+/*
+ * paulib_b200.h -- C ABI of the B200 Pauli-sum library (libpaulib_b200.so).
+ *
+ * Plain pointers and sizes only; includable from C, C++ (g++) and nvcc
+ * translation units, like the reference seam include/gpu/paulib_gpu_api.h
+ * (:1-14).  A Pauli sum crosses the boundary as SoA planes:
+ *
+ *   x[k*stride + i], z[k*stride + i]   word k of term i (I=00, X=10, Z=01,
+ *                                       Y=11 in (x,z) bits)
+ *   flags[i]                            exponent of i^k: bit0 imaginary,
+ *                                       bit1 sign
+ *   val[i]                              FP64 coefficient
+ *
+ * where stride is the plane length (n for inputs, the stated capacity for
+ * outputs).  array_size = ceil(N/64) words per string, 1..16.
+ *
+ * Every pl_* entry point returns a status code (PL_OK on success) and never
+ * traps or aborts; the two launch_gpu_* drop-ins keep the reference's void
+ * signature and record their status for pl_get_last_error().
+ */
+#ifndef PAULIB_B200_H
+#define PAULIB_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#include <cuda_runtime_api.h>
+
+#if defined(__GNUC__)
+#define PL_API __attribute__((visibility("default")))
+#else
+#define PL_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------ */
+#define PL_OK 0
+#define PL_ERR_INVALID_ARG 1   /* bad size, array_size, pointer or option   */
+#define PL_ERR_OOM 2           /* device allocation failed                  */
+#define PL_ERR_TIMEOUT 3       /* a bounded device-side wait ran out        */
+#define PL_ERR_CUDA 4          /* a CUDA runtime call failed                */
+#define PL_ERR_CAPACITY 5      /* output would exceed the stated capacity   */
+#define PL_ERR_UNSUPPORTED 6   /* valid request outside what is built       */
+#define PL_ERR_INTERNAL 7      /* device-side consistency check failed      */
+
+#define PL_MAX_ARRAY_SIZE 16
+
+PL_API const char* pl_status_string(int status);
+/* Status of the most recent call on the calling host thread (the void
+ * drop-ins report through this). */
+PL_API int pl_get_last_error(void);
+PL_API const char* pl_last_error_message(void);
+PL_API int pl_version(void);
+
+/* ---- product and commutator ------------------------------------------- */
+
+/* Drop-in for launch_gpu_mul_soa (include/gpu/paulib_gpu_api.h:25-33):
+ * out[i*n + j] = lhs[j] * rhs[i] for j < n, i < m; out planes have stride
+ * n*m.  Device pointers, asynchronous on `stream`.  An unsupported
+ * array_size records PL_ERR_INVALID_ARG instead of trapping. */
+PL_API void launch_gpu_mul_soa(int array_size, const uint64_t* lhs_x, const uint64_t* lhs_z,
+                        const uint8_t* lhs_flags, const double* lhs_val,
+                        const uint64_t* rhs_x, const uint64_t* rhs_z,
+                        const uint8_t* rhs_flags, const double* rhs_val, uint64_t* out_x,
+                        uint64_t* out_z, uint8_t* out_flags, double* out_val, int n, int m,
+                        cudaStream_t stream);
+
+/* Drop-in for launch_gpu_commutator_soa (include/gpu/paulib_gpu_api.h:43-53):
+ * [lhs, rhs] (multiply_by_i = 0) or i[lhs, rhs] (= 1).  Anticommuting pairs
+ * emit lhs_j * rhs_i with value 2*lhs_val[j]*rhs_val[i] into planes of
+ * stride `capacity`, starting at slot *d_count (zeroed by the caller, as in
+ * the reference); *d_count ends at the number of emitted terms.  Unlike the
+ * reference's atomic slot claim, the emission order is deterministic:
+ * lhs-major, rhs-minor, the order of the reference's single-threaded CPU
+ * commutator_impl (PauliSumOperations.h:316-346).  Terms beyond `capacity`
+ * are not written and record PL_ERR_CAPACITY. */
+PL_API void launch_gpu_commutator_soa(int array_size, int multiply_by_i, const uint64_t* lhs_x,
+                               const uint64_t* lhs_z, const uint8_t* lhs_flags,
+                               const double* lhs_val, const uint64_t* rhs_x,
+                               const uint64_t* rhs_z, const uint8_t* rhs_flags,
+                               const double* rhs_val, uint64_t* out_x, uint64_t* out_z,
+                               uint8_t* out_flags, double* out_val,
+                               unsigned long long* d_count, int n, int m, long long capacity,
+                               cudaStream_t stream);
+
+/* Status-returning form of launch_gpu_mul_soa with 64-bit sizes
+ * (n*m < 2^40).  Replaces the same reference interface. */
+PL_API int pl_multiply(int array_size, const uint64_t* lhs_x, const uint64_t* lhs_z,
+                const uint8_t* lhs_flags, const double* lhs_val, int64_t n,
+                const uint64_t* rhs_x, const uint64_t* rhs_z, const uint8_t* rhs_flags,
+                const double* rhs_val, int64_t m, uint64_t* out_x, uint64_t* out_z,
+                uint8_t* out_flags, double* out_val, cudaStream_t stream);
+
+/* Status-returning form of launch_gpu_commutator_soa (same semantics and
+ * deterministic order); the pair count n*m must be below 2^40. */
+PL_API int pl_commutator(int array_size, int multiply_by_i, const uint64_t* lhs_x,
+                  const uint64_t* lhs_z, const uint8_t* lhs_flags, const double* lhs_val,
+                  int64_t n, const uint64_t* rhs_x, const uint64_t* rhs_z,
+                  const uint8_t* rhs_flags, const double* rhs_val, int64_t m, uint64_t* out_x,
+                  uint64_t* out_z, uint8_t* out_flags, double* out_val, int64_t capacity,
+                  unsigned long long* d_count, cudaStream_t stream);
+
+/* ---- collate: sort_and_combine / canonicalize / cutoff / weight ------- */
+
+/* canonicalize() (PauliSumUtils.h:315-328): fold the sign bit into the
+ * value, merge equal (x, z, phase), drop exact zeros.  Output sorted by
+ * (x[0..AS), z[0..AS), phase). */
+#define PL_COLLATE_CANONICALIZE 0
+/* sort_and_combine() (PauliSumOperations.h:369-461): key (x, z, flags)
+ * with the sign kept in the key; zero sums are kept. */
+#define PL_COLLATE_SORT_AND_COMBINE 1
+
+typedef struct {
+    int32_t mode;          /* PL_COLLATE_* */
+    int32_t reserved;
+    double cutoff;         /* > 0: then drop |c| < cutoff (cutoff(),
+                              PauliSumUtils.h:378-384) */
+    uint64_t max_weight;   /* != UINT64_MAX: then drop weight > max_weight
+                              (truncate_weight(), PauliSumUtils.h:387-393) */
+} pl_collate_opts;
+
+/* Workspace needed to collate n input terms. */
+PL_API int pl_collate_workspace_size(int array_size, int64_t n, size_t* bytes);
+
+/* Collate n terms (planes of stride n) into out planes of stride
+ * out_capacity.  Synchronous: returns after `stream` drained, with the
+ * output term count in *out_count (host pointer).  Within an output
+ * segment coefficients are summed in input-index order (segments longer
+ * than 32 terms use a fixed-order parallel reduction).  n < 2^30.
+ * Replaces PauliSum::canonicalize / sort_and_combine / cutoff /
+ * truncate_weight (PauliSumUtils.h:287-393, PauliSumOperations.h:369-461). */
+PL_API int pl_collate(int array_size, const uint64_t* x, const uint64_t* z, const uint8_t* flags,
+               const double* val, int64_t n, uint64_t* out_x, uint64_t* out_z,
+               uint8_t* out_flags, double* out_val, int64_t out_capacity, int64_t* out_count,
+               const pl_collate_opts* opts, void* workspace, size_t workspace_bytes,
+               cudaStream_t stream);
+
+/* Workspace needed by pl_multiply_collate for n x m products. */
+PL_API int pl_multiply_collate_workspace_size(int array_size, int64_t n, int64_t m, size_t* bytes);
+
+/* Fused `a *= b; a.canonicalize()` (PauliSumOperations.h:256-306 then
+ * PauliSumUtils.h:315-328): the n*m products (in the reference's i*n + j
+ * order) are generated inside the sort and never written to HBM.  Output
+ * and synchronisation as pl_collate.  n*m < 2^30. */
+PL_API int pl_multiply_collate(int array_size, const uint64_t* lhs_x, const uint64_t* lhs_z,
+                        const uint8_t* lhs_flags, const double* lhs_val, int64_t n,
+                        const uint64_t* rhs_x, const uint64_t* rhs_z,
+                        const uint8_t* rhs_flags, const double* rhs_val, int64_t m,
+                        uint64_t* out_x, uint64_t* out_z, uint8_t* out_flags, double* out_val,
+                        int64_t out_capacity, int64_t* out_count, const pl_collate_opts* opts,
+                        void* workspace, size_t workspace_bytes, cudaStream_t stream);
+
+/* ---- single-pass term kernels ----------------------------------------- */
+
+/* apply_CNOT(c, t) in place (PauliSumClifford.h:213-239); order kept. */
+PL_API int pl_apply_cnot(int array_size, uint64_t* x, uint64_t* z, uint8_t* flags, int64_t n,
+                  int64_t stride, int control, int target, cudaStream_t stream);
+
+/* zero_state_expectation (PauliSumUtils.h:163-177) into *d_result (device
+ * double).  Fixed-order reduction, so run-to-run deterministic. */
+PL_API int pl_zero_state_expectation(int array_size, const uint64_t* x, const uint8_t* flags,
+                              const double* val, int64_t n, int64_t stride, double* d_result,
+                              cudaStream_t stream);
+
+/* ---- device-resident propagation state -------------------------------- */
+
+/* TruncationOptions<double> (PauliPropagation.h:27-31). */
+typedef struct {
+    uint64_t max_weight;          /* UINT64_MAX = disabled */
+    double coefficient_cutoff;    /* <= 0 = disabled */
+    uint64_t max_terms;           /* UINT64_MAX = disabled */
+} pl_truncation;
+
+/* Circuit ops, rows of int32 (kind, a, b) in application order. */
+#define PL_OP_ROTATION 0   /* rotation number a of the rotation table */
+#define PL_OP_CNOT 1       /* CNOT control a, target b */
+
+typedef struct pl_state pl_state;
+
+/* A Pauli sum kept in device memory between gates.  capacity_hint sizes
+ * the initial buffers (terms); the state grows on demand. */
+PL_API int pl_state_create(pl_state** state, int array_size, int64_t capacity_hint,
+                    cudaStream_t stream);
+PL_API int pl_state_destroy(pl_state* state);
+/* Host planes (stride n) -> device. */
+PL_API int pl_state_upload(pl_state* state, const uint64_t* x, const uint64_t* z,
+                    const uint8_t* flags, const double* val, int64_t n);
+/* Device -> host planes of stride *n (call with x == NULL to query n). */
+PL_API int pl_state_download(pl_state* state, uint64_t* x, uint64_t* z, uint8_t* flags,
+                      double* val, int64_t capacity, int64_t* n);
+PL_API int pl_state_size(pl_state* state, int64_t* n);
+
+/* PauliSum::evolve(rotations) (PauliSumOperations.h:107-183): the n_rot
+ * rotations (host planes, stride n_rot; val = angle) applied in order,
+ * each followed by the reference's `+=` merge only. */
+PL_API int pl_state_evolve(pl_state* state, const uint64_t* rot_x, const uint64_t* rot_z,
+                    const uint8_t* rot_flags, const double* rot_theta, int64_t n_rot);
+/* apply_truncation (PauliPropagation.h:36-47). */
+PL_API int pl_state_apply_truncation(pl_state* state, const pl_truncation* opts);
+PL_API int pl_state_canonicalize(pl_state* state);
+PL_API int pl_state_sort_and_combine(pl_state* state);
+PL_API int pl_state_cutoff(pl_state* state, double eps);
+PL_API int pl_state_truncate_weight(pl_state* state, uint64_t max_weight);
+PL_API int pl_state_apply_cnot(pl_state* state, int control, int target);
+PL_API int pl_state_zero_state_expectation(pl_state* state, double* result);
+
+/* propagate (PauliPropagation.h:54-63): ops walked in reverse; a rotation
+ * is evolve + apply_truncation, a CNOT is apply_CNOT.  ops == NULL means
+ * "every rotation in order", the reference's rotation-only circuit. */
+PL_API int pl_propagate(pl_state* state, const uint64_t* rot_x, const uint64_t* rot_z,
+                 const uint8_t* rot_flags, const double* rot_theta, int64_t n_rot,
+                 const int32_t* ops, int64_t n_ops, const pl_truncation* opts);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* PAULIB_B200_H */

@@ -1,0 +1,1596 @@
+// pl_propagate.cu -- device-resident Pauli propagation (evolve + truncate).
+//
+// Reference semantics (PauLIB):
+//   evolve            PauliSumOperations.h:107-183  per rotation (P, theta):
+//                     ps = iP; fast paths at theta ~ 0, pi, +-pi/2 (isCloseOne,
+//                     eps 1e-14); otherwise anticommuting Q keeps cos*c in place
+//                     and appends (Q*ps, -sin*c), then `+=` (sort_and_combine).
+//   apply_truncation  PauliPropagation.h:36-47  canonicalize, truncate_weight,
+//                     cutoff (trim when max_terms is set).
+//   propagate         PauliPropagation.h:54-63  gates in reverse order.
+//   apply_CNOT        PauliSumClifford.h:213-239.
+//
+// Fast path (the state is canonical: sorted by (x, z, phase), sign folded,
+// keys distinct; the generator is a single-qubit Pauli).  Per rotation:
+//   A  k_expand        anticommutation test; each anticommuting term's child
+//                      Q*ps goes to one of two runs by the value of the
+//                      flipped bit.  Flipping one bit preserves the order
+//                      inside each run (the only local inversion, between
+//                      the phase-0 / phase-1 twins of one string, is fixed
+//                      in place), so no sort is needed.
+//   B  k_merge_runs    merge-path merge of the two runs.
+//   C  k_merge_reduce  merge-path merge of the scaled old terms with the
+//                      children, segment reduce, zero / weight / cutoff
+//                      filter and look-back compaction into the other buffer.
+// Every canonical key receives at most one old and one new contribution, so
+// the two-stage order of the reference (`+=` then canonicalize) reduces to
+// S(sign 0) - S(sign 1) of at most two terms: bit-identical to the reference.
+// Overflow of the output buffer is detected on the device; the host replays
+// from the failing gate after growing the buffers, so the fast path never
+// waits for the host.
+//
+// Other states and generators take the general path: materialise old and
+// new terms, then the collate engine (pl_collate.cu) in the matching mode.
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "pl_collate.cuh"
+
+namespace pl {
+namespace {
+
+constexpr int kPT = 256;
+constexpr int kExpItems = 8;
+constexpr u32 kExpTile = kPT * kExpItems;
+constexpr u64 kF2Agg = 1ull << 62, kF2Pre = 2ull << 62;
+constexpr u64 kC31 = (1ull << 31) - 1;
+
+template <int AS>
+struct PItems {
+    static constexpr int v = AS == 1 ? 8 : AS == 2 ? 4 : AS <= 4 ? 2 : 1;
+};
+template <int AS>
+constexpr int ptile() {
+    return kPT * PItems<AS>::v;
+}
+
+struct Buf {
+    u64* x;
+    u64* z;
+    u8* f;
+    double* v;
+    i64 cap;
+};
+
+enum RotMode : int { kSkip = 0, kNegate = 1, kHalfPos = 2, kHalfNeg = 3, kGeneral = 4 };
+
+template <int AS>
+struct GateP {
+    u64 px[AS], pz[AS];
+    u32 psf;     // flags of ps = P with its phase flipped
+    int cw;      // class bit: word,
+    u64 cmask;   //            mask,
+    int cls_x;   //            and plane (1: x, 0: z)
+};
+
+__device__ __forceinline__ int status_set(const int* status) {
+    return *reinterpret_cast<const volatile int*>(status);
+}
+
+// Order key of a term: (x, z, phase, sign); ps = phase << 1 | sign.
+__device__ __forceinline__ u32 ps_of(u32 f) { return ((f & 1u) << 1) | ((f >> 1) & 1u); }
+
+template <int AS>
+struct Key {
+    u64 x[AS], z[AS];
+    u32 ps;
+};
+
+template <int AS>
+__device__ __forceinline__ int kcmp(const Key<AS>& a, const Key<AS>& b) {
+#pragma unroll
+    for (int k = 0; k < AS; ++k)
+        if (a.x[k] != b.x[k]) return a.x[k] < b.x[k] ? -1 : 1;
+#pragma unroll
+    for (int k = 0; k < AS; ++k)
+        if (a.z[k] != b.z[k]) return a.z[k] < b.z[k] ? -1 : 1;
+    if (a.ps != b.ps) return a.ps < b.ps ? -1 : 1;
+    return 0;
+}
+
+template <int AS>
+__device__ __forceinline__ Key<AS> gkey(const Buf& B, i64 i) {
+    Key<AS> k;
+#pragma unroll
+    for (int w = 0; w < AS; ++w) {
+        k.x[w] = B.x[w * B.cap + i];
+        k.z[w] = B.z[w * B.cap + i];
+    }
+    k.ps = ps_of(B.f[i]);
+    return k;
+}
+
+template <int AS>
+__device__ __forceinline__ bool anticommutes(const u64* x, const u64* z, const GateP<AS>& g) {
+    u64 par = 0;
+#pragma unroll
+    for (int k = 0; k < AS; ++k) par ^= anti_word(x[k], z[k], g.px[k], g.pz[k]);
+    return (__popcll(par) & 1) != 0;
+}
+
+// Look-back over two 31-bit counters packed as c1 << 31 | c0 (flags in bits
+// 62-63).  In/out values use the form c1 << 32 | c0.
+__device__ __forceinline__ u64 lookback2(u64* lb, u32 tile, u64 v, int* status) {
+    const u64 enc = ((v >> 32) << 31) | (v & 0xffffffffull);
+    auto dec = [](u64 e) { return ((e >> 31) & kC31) << 32 | (e & kC31); };
+    if (tile == 0) {
+        st_volatile64(lb, kF2Pre | enc);
+        return 0;
+    }
+    st_volatile64(lb + tile, kF2Agg | enc);
+    u64 excl = 0;
+    i64 t = (i64)tile - 1;
+    u32 spins = 0;
+    while (t >= 0) {
+        const u64 w = ld_volatile64(lb + t);
+        const u64 fl = w >> 62;
+        if (fl == 0) {
+            if (++spins > kSpinLimit) {
+                raise_status(status, PL_ERR_TIMEOUT);
+                break;
+            }
+            if (spins > 64) __nanosleep(64);
+            continue;
+        }
+        excl += dec(w & ~(3ull << 62));
+        if (fl == 2) break;
+        --t;
+    }
+    const u64 inc = excl + v;
+    st_volatile64(lb + tile, kF2Pre | (((inc >> 32) << 31) | (inc & 0xffffffffull)));
+    return excl;
+}
+
+// ---------------------------------------------------------------------------
+// A: expansion into two runs.
+// ---------------------------------------------------------------------------
+template <int AS>
+__global__ void __launch_bounds__(kPT)
+    k_expand(Buf old, const i64* d_m, GateP<AS> g, int mode, double neg_s, Buf r0, Buf r1,
+             i64* d_k, u64* lb, u32* ctr, int* status, i64 cap_out, int gate, int* d_fail) {
+    __shared__ u32 s_tile;
+    __shared__ u64 s_warp[kPT / 32];
+    __shared__ u64 s_base;
+    if (status_set(status)) return;
+    const i64 m = *d_m;
+    const u32 ntiles = (u32)((m + kExpTile - 1) / kExpTile);
+    if (ntiles == 0) {
+        if (blockIdx.x == 0 && threadIdx.x == 0) d_k[0] = d_k[1] = 0;
+        return;
+    }
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    for (;;) {
+        if (tid == 0) s_tile = atomicAdd(ctr, 1u);
+        __syncthreads();
+        const u32 tile = s_tile;
+        __syncthreads();
+        if (tile >= ntiles) break;
+        const i64 wbase = (i64)tile * kExpTile + warp * (kExpItems * 32);
+        u32 amask = 0, cmask = 0, c0 = 0, c1 = 0;
+        u32 off0[kExpItems], off1[kExpItems];
+#pragma unroll
+        for (int t = 0; t < kExpItems; ++t) {
+            const i64 j = wbase + t * 32 + lane;
+            bool a = false, cl = false;
+            if (j < m) {
+                u64 x[AS], z[AS];
+#pragma unroll
+                for (int k = 0; k < AS; ++k) {
+                    x[k] = old.x[k * old.cap + j];
+                    z[k] = old.z[k * old.cap + j];
+                }
+                a = anticommutes<AS>(x, z, g);
+                const u64 w = g.cls_x ? x[g.cw] : z[g.cw];
+                cl = (w & g.cmask) != 0;
+            }
+            const u32 b0 = __ballot_sync(0xffffffffu, a && !cl);
+            const u32 b1 = __ballot_sync(0xffffffffu, a && cl);
+            off0[t] = c0 + __popc(b0 & lanemask_lt());
+            off1[t] = c1 + __popc(b1 & lanemask_lt());
+            c0 += __popc(b0);
+            c1 += __popc(b1);
+            if (a) amask |= 1u << t;
+            if (cl) cmask |= 1u << t;
+        }
+        if (lane == 0) s_warp[warp] = ((u64)c1 << 32) | c0;
+        __syncthreads();
+        u64 wpre = 0, tot = 0;
+#pragma unroll
+        for (int w = 0; w < kPT / 32; ++w) {
+            const u64 v = s_warp[w];
+            if (w < warp) wpre += v;
+            tot += v;
+        }
+        if (tid == 0) s_base = lookback2(lb, tile, tot, status);
+        __syncthreads();
+        const u64 base = s_base + wpre;
+        const i64 base0 = (u32)base, base1 = (u32)(base >> 32);
+#pragma unroll
+        for (int t = 0; t < kExpItems; ++t) {
+            if (!((amask >> t) & 1u)) continue;
+            const i64 j = wbase + t * 32 + lane;
+            u64 x[AS], z[AS];
+#pragma unroll
+            for (int k = 0; k < AS; ++k) {
+                x[k] = old.x[k * old.cap + j];
+                z[k] = old.z[k * old.cap + j];
+            }
+            const u32 f = old.f[j];
+            PhaseAcc acc;
+#pragma unroll
+            for (int k = 0; k < AS; ++k) acc.step(x[k], z[k], g.px[k], g.pz[k]);
+            const u32 fin = mode == kHalfPos ? ((f + 2u) & 3u) : f;
+            const u32 nf = acc.phase(fin, g.psf);
+            const double nv = mode == kGeneral ? dmul(neg_s, old.v[j]) : old.v[j];
+            const bool cl = (cmask >> t) & 1u;
+            i64 pos = cl ? base1 + off1[t] : base0 + off0[t];
+            // Twin fix-up: the phase-0/phase-1 twins of one string are adjacent
+            // in both runs; their children swap order when the phase shift is odd.
+            if ((f & 1u) == 0 && j + 1 < m) {
+                bool same = true;
+#pragma unroll
+                for (int k = 0; k < AS; ++k)
+                    same = same && old.x[k * old.cap + j + 1] == x[k] &&
+                           old.z[k * old.cap + j + 1] == z[k];
+                if (same && (nf & 1u)) pos += 1;
+            } else if ((f & 1u) == 1 && j > 0) {
+                bool same = true;
+#pragma unroll
+                for (int k = 0; k < AS; ++k)
+                    same = same && old.x[k * old.cap + j - 1] == x[k] &&
+                           old.z[k * old.cap + j - 1] == z[k];
+                if (same && !(nf & 1u)) pos -= 1;
+            }
+            const Buf& R = cl ? r1 : r0;
+            if (pos < 0 || pos >= R.cap) {
+                raise_status(status, PL_ERR_INTERNAL);
+                continue;
+            }
+#pragma unroll
+            for (int k = 0; k < AS; ++k) {
+                R.x[k * R.cap + pos] = x[k] ^ g.px[k];
+                R.z[k * R.cap + pos] = z[k] ^ g.pz[k];
+            }
+            R.f[pos] = (u8)nf;
+            R.v[pos] = nv;
+        }
+        if (tile == ntiles - 1 && tid == 0) {
+            const u64 fin = s_base + tot;
+            const i64 k0 = (u32)fin, k1 = (u32)(fin >> 32);
+            d_k[0] = k0;
+            d_k[1] = k1;
+            if (m + k0 + k1 > cap_out) {
+                raise_status(status, PL_ERR_CAPACITY);
+                atomicExch(d_fail, gate);
+            }
+        }
+        __syncthreads();
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Merge-path partition: split points of each tile's diagonal range.
+// ---------------------------------------------------------------------------
+template <int AS>
+__device__ __forceinline__ i64 merge_split(const Buf& A, i64 na, const Buf& B, i64 nb, i64 d) {
+    i64 lo = d > nb ? d - nb : 0, hi = d < na ? d : na;
+    while (lo < hi) {
+        const i64 mid = (lo + hi) >> 1;
+        if (kcmp<AS>(gkey<AS>(A, mid), gkey<AS>(B, d - 1 - mid)) <= 0) lo = mid + 1;
+        else hi = mid;
+    }
+    return lo;
+}
+
+// For tile t: lo split at max(t*T - halo, 0), hi split at min(t*T + T + halo, total).
+template <int AS>
+__global__ void __launch_bounds__(256) k_partition(Buf A, const i64* pa, Buf B, const i64* pb,
+                                                   const i64* pb2, int T, int halo, u32* lo_s,
+                                                   u32* hi_s, u32 max_tiles, const int* status) {
+    if (status_set(status)) return;
+    const i64 na = *pa, nb = *pb + (pb2 ? *pb2 : 0);
+    const i64 total = na + nb;
+    const u32 ntiles = (u32)((total + T - 1) / T);
+    for (u32 t = blockIdx.x * blockDim.x + threadIdx.x; t < ntiles && t < max_tiles;
+         t += gridDim.x * blockDim.x) {
+        const i64 D = (i64)t * T;
+        const i64 s0 = D - halo > 0 ? D - halo : 0;
+        const i64 s1 = D + T + halo < total ? D + T + halo : total;
+        lo_s[t] = (u32)merge_split<AS>(A, na, B, nb, s0);
+        hi_s[t] = (u32)merge_split<AS>(A, na, B, nb, s1);
+    }
+}
+
+// Shared-memory SoA tile of terms.
+template <int AS>
+struct STile {
+    u64* x;  // [AS][cap]
+    u64* z;
+    double* v;
+    u8* f;   // order key bits: bit0 phase, bit1 sign, bit2 removed
+    u16* order;
+    int cap;
+    __device__ __forceinline__ Key<AS> key(int i) const {
+        Key<AS> k;
+#pragma unroll
+        for (int w = 0; w < AS; ++w) {
+            k.x[w] = x[w * cap + i];
+            k.z[w] = z[w * cap + i];
+        }
+        k.ps = ps_of(f[i] & 3u);
+        return k;
+    }
+};
+
+template <int AS>
+__device__ STile<AS> carve_tile(unsigned char* smem, int cap) {
+    STile<AS> S;
+    S.cap = cap;
+    S.x = reinterpret_cast<u64*>(smem);
+    S.z = S.x + AS * cap;
+    S.v = reinterpret_cast<double*>(S.z + AS * cap);
+    S.f = reinterpret_cast<u8*>(S.v + cap);
+    S.order = reinterpret_cast<u16*>(S.f + ((cap + 15) & ~15));
+    return S;
+}
+
+template <int AS>
+constexpr size_t tile_smem_bytes(int cap) {
+    return (size_t)cap * (16 * AS + 8) + (size_t)((cap + 15) & ~15) + (size_t)cap * 2 + 64;
+}
+
+// Merge [0, na) and [na, na + nb) of the tile into S.order (ties: first part).
+template <int AS>
+__device__ void block_merge(const STile<AS>& S, int na, int nb) {
+    const int L = na + nb;
+    const int per = (L + kPT - 1) / kPT;
+    const int d = min((int)threadIdx.x * per, L);
+    const int e = min(d + per, L);
+    int lo = d > nb ? d - nb : 0, hi = d < na ? d : na;
+    while (lo < hi) {
+        const int mid = (lo + hi) >> 1;
+        if (kcmp<AS>(S.key(mid), S.key(na + d - 1 - mid)) <= 0) lo = mid + 1;
+        else hi = mid;
+    }
+    int a = lo, b = d - lo;
+    for (int q = d; q < e; ++q) {
+        bool take_a;
+        if (a >= na) take_a = false;
+        else if (b >= nb) take_a = true;
+        else take_a = kcmp<AS>(S.key(a), S.key(na + b)) <= 0;
+        S.order[q] = (u16)(take_a ? a++ : na + b++);
+    }
+}
+
+template <int AS>
+__device__ __forceinline__ void tile_load(const STile<AS>& S, int dst, const Buf& B, i64 src) {
+#pragma unroll
+    for (int w = 0; w < AS; ++w) {
+        S.x[w * S.cap + dst] = B.x[w * B.cap + src];
+        S.z[w * S.cap + dst] = B.z[w * B.cap + src];
+    }
+    S.v[dst] = B.v[src];
+    S.f[dst] = B.f[src] & 3u;
+}
+
+// ---------------------------------------------------------------------------
+// B: merge the two runs into one sorted child list.
+// ---------------------------------------------------------------------------
+template <int AS>
+__global__ void __launch_bounds__(kPT)
+    k_merge_runs(Buf r0, Buf r1, const i64* d_k, const u32* lo_s, const u32* hi_s, Buf out,
+                 u32* ctr, int* status) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    __shared__ u32 s_tile;
+    if (status_set(status)) return;
+    constexpr int T = ptile<AS>();
+    const STile<AS> S = carve_tile<AS>(smem, T);
+    const i64 na = d_k[0], nb = d_k[1], total = na + nb;
+    const u32 ntiles = (u32)((total + T - 1) / T);
+    for (;;) {
+        if (threadIdx.x == 0) s_tile = atomicAdd(ctr, 1u);
+        __syncthreads();
+        const u32 tile = s_tile;
+        __syncthreads();
+        if (tile >= ntiles) break;
+        const i64 D = (i64)tile * T;
+        const i64 D1 = D + T < total ? D + T : total;
+        const i64 a0 = lo_s[tile], a1 = hi_s[tile];
+        const i64 b0 = D - a0, b1 = D1 - a1;
+        const int la = (int)(a1 - a0), lb = (int)(b1 - b0);
+        if (la < 0 || lb < 0 || la + lb > T) {
+            raise_status(status, PL_ERR_INTERNAL);
+            __syncthreads();
+            continue;
+        }
+        for (int i = threadIdx.x; i < la + lb; i += kPT) {
+            if (i < la) tile_load<AS>(S, i, r0, a0 + i);
+            else tile_load<AS>(S, i, r1, b0 + (i - la));
+        }
+        __syncthreads();
+        block_merge<AS>(S, la, lb);
+        __syncthreads();
+        for (int q = threadIdx.x; q < la + lb; q += kPT) {
+            const int e = S.order[q];
+            const i64 o = D + q;
+            if (o >= out.cap) {
+                raise_status(status, PL_ERR_INTERNAL);
+                break;
+            }
+#pragma unroll
+            for (int w = 0; w < AS; ++w) {
+                out.x[w * out.cap + o] = S.x[w * S.cap + e];
+                out.z[w * out.cap + o] = S.z[w * S.cap + e];
+            }
+            out.f[o] = S.f[e];
+            out.v[o] = S.v[e];
+        }
+        __syncthreads();
+    }
+}
+
+// ---------------------------------------------------------------------------
+// C: merge old terms with the children, reduce, filter, compact.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ u32 lookback1(u32* lb, u32 tile, u32 cnt, int* status) {
+    constexpr u32 kAgg = 1u << 30, kPre = 2u << 30, kMask = (1u << 30) - 1;
+    if (tile == 0) {
+        st_volatile(lb, kPre | cnt);
+        return 0;
+    }
+    st_volatile(lb + tile, kAgg | cnt);
+    u32 excl = 0;
+    i64 t = (i64)tile - 1;
+    u32 spins = 0;
+    while (t >= 0) {
+        const u32 w = ld_volatile(lb + t);
+        const u32 fl = w >> 30;
+        if (fl == 0) {
+            if (++spins > kSpinLimit) {
+                raise_status(status, PL_ERR_TIMEOUT);
+                break;
+            }
+            if (spins > 64) __nanosleep(64);
+            continue;
+        }
+        excl += w & kMask;
+        if (fl == 2) break;
+        --t;
+    }
+    st_volatile(lb + tile, kPre | ((excl + cnt) & kMask));
+    return excl;
+}
+
+template <int AS>
+__global__ void __launch_bounds__(kPT)
+    k_merge_reduce(Buf old, const i64* d_m, Buf nw, const i64* d_k, const u32* lo_s,
+                   const u32* hi_s, GateP<AS> g, int mode, double c, Buf out, i64* d_out,
+                   u64 max_weight, double cutoff, u32* lb, u32* ctr, int* status, int gate,
+                   int* d_fail) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    __shared__ u32 s_tile, s_excl;
+    __shared__ u32 s_warp[kPT / 32];
+    if (status_set(status)) return;
+    constexpr int IT = PItems<AS>::v;
+    constexpr int T = ptile<AS>();
+    const STile<AS> S = carve_tile<AS>(smem, T + 2);
+    const i64 na = *d_m, nb = d_k[0] + d_k[1], total = na + nb;
+    const u32 ntiles = (u32)((total + T - 1) / T);
+    if (ntiles == 0) {
+        if (blockIdx.x == 0 && threadIdx.x == 0) *d_out = 0;
+        return;
+    }
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    for (;;) {
+        if (tid == 0) s_tile = atomicAdd(ctr, 1u);
+        __syncthreads();
+        const u32 tile = s_tile;
+        __syncthreads();
+        if (tile >= ntiles) break;
+        const i64 D = (i64)tile * T;
+        const i64 s0 = D > 0 ? D - 1 : 0;
+        const i64 s1 = D + T + 1 < total ? D + T + 1 : total;
+        const i64 a0 = lo_s[tile], a1 = hi_s[tile];
+        const i64 b0 = s0 - a0, b1 = s1 - a1;
+        const int la = (int)(a1 - a0), lbn = (int)(b1 - b0);
+        const bool bad = la < 0 || lbn < 0 || la + lbn > T + 2;
+        if (!bad) {
+            for (int i = tid; i < la + lbn; i += kPT) {
+                if (i < la) {
+                    tile_load<AS>(S, i, old, a0 + i);
+                    u64 x[AS], z[AS];
+#pragma unroll
+                    for (int w = 0; w < AS; ++w) {
+                        x[w] = S.x[w * S.cap + i];
+                        z[w] = S.z[w * S.cap + i];
+                    }
+                    if (anticommutes<AS>(x, z, g)) {
+                        if (mode == kGeneral) S.v[i] = dmul(S.v[i], c);
+                        else S.f[i] |= 4u;  // +-pi/2: the old term moved to its child
+                    }
+                } else {
+                    tile_load<AS>(S, i, nw, b0 + (i - la));
+                }
+            }
+        }
+        __syncthreads();
+        if (!bad) block_merge<AS>(S, la, lbn);
+        __syncthreads();
+        // output positions of this tile: global [D, min(D+T, total))
+        const i64 dend = D + T < total ? D + T : total;
+        const int q0 = (int)(D - s0);
+        const int L = la + lbn;
+        bool keep[IT];
+        double res[IT];
+        int head_e[IT];
+        u32 nkeep = 0;
+#pragma unroll
+        for (int it = 0; it < IT; ++it) {
+            keep[it] = false;
+            res[it] = 0.0;
+            head_e[it] = 0;
+            const int q = q0 + tid * IT + it;
+            if (bad || D + tid * IT + it >= dend) continue;
+            const int e = S.order[q];
+            const Key<AS> ke = S.key(e);
+            bool head = (q == 0);
+            if (!head) {
+                const Key<AS> kp = S.key(S.order[q - 1]);
+                head = false;
+#pragma unroll
+                for (int w = 0; w < AS; ++w)
+                    head = head || kp.x[w] != ke.x[w] || kp.z[w] != ke.z[w];
+                head = head || ((kp.ps ^ ke.ps) & 2u);
+            }
+            if (!head) continue;
+            double sp = 0.0, sm = 0.0;
+            bool has = false;
+            int members = 0;
+            for (int r = q; r < L; ++r) {
+                const int er = S.order[r];
+                if (r > q) {
+                    const Key<AS> kr = S.key(er);
+                    bool same = ((kr.ps ^ ke.ps) & 2u) == 0;
+#pragma unroll
+                    for (int w = 0; w < AS; ++w)
+                        same = same && kr.x[w] == ke.x[w] && kr.z[w] == ke.z[w];
+                    if (!same) break;
+                }
+                if (++members > 2) {
+                    raise_status(status, PL_ERR_INTERNAL);
+                    break;
+                }
+                const u32 fr = S.f[er];
+                if (fr & 4u) continue;
+                has = true;
+                if (fr & 2u) sm = dadd(sm, S.v[er]);
+                else sp = dadd(sp, S.v[er]);
+            }
+            if (!has) continue;
+            const double rv = dadd(sp, -sm);
+            bool k = rv != 0.0;
+            if (k && cutoff > 0.0) k = fabs(rv) >= cutoff;
+            if (k && max_weight != ~0ull) {
+                u64 wsum = 0;
+#pragma unroll
+                for (int w = 0; w < AS; ++w) wsum += (u64)__popcll(ke.x[w] | ke.z[w]);
+                k = wsum <= max_weight;
+            }
+            keep[it] = k;
+            res[it] = rv;
+            head_e[it] = e;
+            nkeep += k ? 1u : 0u;
+        }
+        // block exclusive scan of per-thread keep counts
+        u32 inc = nkeep;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const u32 t = __shfl_up_sync(0xffffffffu, inc, o);
+            if (lane >= o) inc += t;
+        }
+        if (lane == 31) s_warp[warp] = inc;
+        __syncthreads();
+        u32 wpre = 0, tot = 0;
+#pragma unroll
+        for (int w = 0; w < kPT / 32; ++w) {
+            const u32 cw = s_warp[w];
+            if (w < warp) wpre += cw;
+            tot += cw;
+        }
+        if (tid == 0) s_excl = lookback1(lb, tile, tot, status);
+        __syncthreads();
+        i64 o = (i64)s_excl + wpre + (inc - nkeep);
+#pragma unroll
+        for (int it = 0; it < IT; ++it) {
+            if (!keep[it]) continue;
+            if (o >= out.cap) {
+                raise_status(status, PL_ERR_CAPACITY);
+                atomicExch(d_fail, gate);
+                break;
+            }
+            const int e = head_e[it];
+#pragma unroll
+            for (int w = 0; w < AS; ++w) {
+                out.x[w * out.cap + o] = S.x[w * S.cap + e];
+                out.z[w * out.cap + o] = S.z[w * S.cap + e];
+            }
+            out.f[o] = (u8)(S.f[e] & 1u);
+            out.v[o] = res[it];
+            ++o;
+        }
+        if (tile == ntiles - 1 && tid == 0) *d_out = (i64)s_excl + tot;
+        __syncthreads();
+    }
+}
+
+// ---------------------------------------------------------------------------
+// In-place and general-path kernels.
+// ---------------------------------------------------------------------------
+// theta ~ pi: anticommuting terms change sign.  canonical: negate the value
+// (canonicalize would fold the sign); otherwise flip the sign bit exactly as
+// evolve does (PauliSumOperations.h:124-130).
+template <int AS>
+__global__ void __launch_bounds__(256) k_negate(Buf b, const i64* d_n, GateP<AS> g, int fold,
+                                                const int* status) {
+    if (status_set(status)) return;
+    const i64 n = *d_n;
+    for (i64 i = (i64)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+         i += (i64)gridDim.x * blockDim.x) {
+        u64 x[AS], z[AS];
+#pragma unroll
+        for (int k = 0; k < AS; ++k) {
+            x[k] = b.x[k * b.cap + i];
+            z[k] = b.z[k * b.cap + i];
+        }
+        if (!anticommutes<AS>(x, z, g)) continue;
+        if (fold) b.v[i] = -b.v[i];
+        else b.f[i] ^= 2u;
+    }
+}
+
+// theta ~ +-pi/2 without a following canonicalize: anticommuting Q becomes
+// Q*ps in place, with the extra sign flip at +pi/2 (PauliSumOperations.h:131-147).
+template <int AS>
+__global__ void __launch_bounds__(256) k_halfpi_inplace(Buf b, const i64* d_n, GateP<AS> g,
+                                                        int pos, const int* status) {
+    if (status_set(status)) return;
+    const i64 n = *d_n;
+    for (i64 i = (i64)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+         i += (i64)gridDim.x * blockDim.x) {
+        u64 x[AS], z[AS];
+#pragma unroll
+        for (int k = 0; k < AS; ++k) {
+            x[k] = b.x[k * b.cap + i];
+            z[k] = b.z[k * b.cap + i];
+        }
+        if (!anticommutes<AS>(x, z, g)) continue;
+        PhaseAcc acc;
+#pragma unroll
+        for (int k = 0; k < AS; ++k) {
+            acc.step(x[k], z[k], g.px[k], g.pz[k]);
+            b.x[k * b.cap + i] = x[k] ^ g.px[k];
+            b.z[k * b.cap + i] = z[k] ^ g.pz[k];
+        }
+        const u32 f = b.f[i];
+        b.f[i] = (u8)acc.phase(pos ? (f ^ 2u) : f, g.psf);
+    }
+}
+
+// General branch materialised: out[0, m) = old terms (anticommuting ones
+// scaled by cos), out[m + r] = child r (Q*ps, -sin * value) in old order --
+// exactly the array the reference's `+=` sorts (PauliSumCore.h:210-237).
+template <int AS>
+__global__ void __launch_bounds__(kPT)
+    k_materialize(Buf old, i64 m, GateP<AS> g, double c, double neg_s, Buf out, i64* d_total,
+                  u64* lb, u32* ctr, int* status) {
+    __shared__ u32 s_tile;
+    __shared__ u64 s_warp[kPT / 32];
+    __shared__ u64 s_base;
+    const u32 ntiles = (u32)((m + kExpTile - 1) / kExpTile);
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    for (;;) {
+        if (tid == 0) s_tile = atomicAdd(ctr, 1u);
+        __syncthreads();
+        const u32 tile = s_tile;
+        __syncthreads();
+        if (tile >= ntiles) break;
+        const i64 wbase = (i64)tile * kExpTile + warp * (kExpItems * 32);
+        u32 amask = 0, cnt = 0;
+        u32 off[kExpItems];
+#pragma unroll
+        for (int t = 0; t < kExpItems; ++t) {
+            const i64 j = wbase + t * 32 + lane;
+            bool a = false;
+            if (j < m) {
+                u64 x[AS], z[AS];
+#pragma unroll
+                for (int k = 0; k < AS; ++k) {
+                    x[k] = old.x[k * old.cap + j];
+                    z[k] = old.z[k * old.cap + j];
+                    out.x[k * out.cap + j] = x[k];
+                    out.z[k * out.cap + j] = z[k];
+                }
+                a = anticommutes<AS>(x, z, g);
+                out.f[j] = old.f[j];
+                out.v[j] = a ? dmul(old.v[j], c) : old.v[j];
+            }
+            const u32 bal = __ballot_sync(0xffffffffu, a);
+            off[t] = cnt + __popc(bal & lanemask_lt());
+            cnt += __popc(bal);
+            if (a) amask |= 1u << t;
+        }
+        if (lane == 0) s_warp[warp] = cnt;
+        __syncthreads();
+        u64 wpre = 0, tot = 0;
+#pragma unroll
+        for (int w = 0; w < kPT / 32; ++w) {
+            const u64 v = s_warp[w];
+            if (w < warp) wpre += v;
+            tot += v;
+        }
+        if (tid == 0) s_base = lookback2(lb, tile, tot, status);
+        __syncthreads();
+        const i64 base = (i64)(u32)(s_base + wpre);
+#pragma unroll
+        for (int t = 0; t < kExpItems; ++t) {
+            if (!((amask >> t) & 1u)) continue;
+            const i64 j = wbase + t * 32 + lane;
+            const i64 pos = m + base + off[t];
+            if (pos >= out.cap) {
+                raise_status(status, PL_ERR_CAPACITY);
+                continue;
+            }
+            PhaseAcc acc;
+#pragma unroll
+            for (int k = 0; k < AS; ++k) {
+                const u64 x = old.x[k * old.cap + j], z = old.z[k * old.cap + j];
+                acc.step(x, z, g.px[k], g.pz[k]);
+                out.x[k * out.cap + pos] = x ^ g.px[k];
+                out.z[k * out.cap + pos] = z ^ g.pz[k];
+            }
+            out.f[pos] = (u8)acc.phase(old.f[j], g.psf);
+            out.v[pos] = dmul(neg_s, old.v[j]);
+        }
+        if (tile == ntiles - 1 && tid == 0) *d_total = m + (i64)(u32)(s_base + tot);
+        __syncthreads();
+    }
+}
+
+// Order-preserving filters cutoff / truncate_weight (PauliSumUtils.h:378-393).
+template <int AS>
+__global__ void __launch_bounds__(kPT) k_filter(Buf in, i64 n, Buf out, double eps,
+                                                u64 max_weight, i64* d_out, u32* lb, u32* ctr,
+                                                int* status) {
+    __shared__ u32 s_tile, s_excl;
+    __shared__ u32 s_warp[kPT / 32];
+    const u32 ntiles = (u32)((n + kExpTile - 1) / kExpTile);
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    for (;;) {
+        if (tid == 0) s_tile = atomicAdd(ctr, 1u);
+        __syncthreads();
+        const u32 tile = s_tile;
+        __syncthreads();
+        if (tile >= ntiles) break;
+        const i64 wbase = (i64)tile * kExpTile + warp * (kExpItems * 32);
+        u32 kmask = 0, cnt = 0;
+        u32 off[kExpItems];
+#pragma unroll
+        for (int t = 0; t < kExpItems; ++t) {
+            const i64 j = wbase + t * 32 + lane;
+            bool k = false;
+            if (j < n) {
+                k = true;
+                if (eps > 0.0) k = fabs(in.v[j]) >= eps;
+                if (k && max_weight != ~0ull) {
+                    u64 w = 0;
+#pragma unroll
+                    for (int q = 0; q < AS; ++q)
+                        w += (u64)__popcll(in.x[q * in.cap + j] | in.z[q * in.cap + j]);
+                    k = w <= max_weight;
+                }
+            }
+            const u32 bal = __ballot_sync(0xffffffffu, k);
+            off[t] = cnt + __popc(bal & lanemask_lt());
+            cnt += __popc(bal);
+            if (k) kmask |= 1u << t;
+        }
+        if (lane == 0) s_warp[warp] = cnt;
+        __syncthreads();
+        u32 wpre = 0, tot = 0;
+#pragma unroll
+        for (int w = 0; w < kPT / 32; ++w) {
+            const u32 v = s_warp[w];
+            if (w < warp) wpre += v;
+            tot += v;
+        }
+        if (tid == 0) s_excl = lookback1(lb, tile, tot, status);
+        __syncthreads();
+#pragma unroll
+        for (int t = 0; t < kExpItems; ++t) {
+            if (!((kmask >> t) & 1u)) continue;
+            const i64 j = wbase + t * 32 + lane;
+            const i64 o = (i64)s_excl + wpre + off[t];
+#pragma unroll
+            for (int q = 0; q < AS; ++q) {
+                out.x[q * out.cap + o] = in.x[q * in.cap + j];
+                out.z[q * out.cap + o] = in.z[q * in.cap + j];
+            }
+            out.f[o] = in.f[j];
+            out.v[o] = in.v[j];
+        }
+        if (tile == ntiles - 1 && tid == 0) *d_out = (i64)s_excl + tot;
+        __syncthreads();
+    }
+}
+
+template <int AS>
+__global__ void __launch_bounds__(256) k_cnot_state(Buf b, const i64* d_n, int wc, u64 mc,
+                                                    int wt, u64 mt, const int* status) {
+    if (status_set(status)) return;
+    const i64 n = *d_n;
+    for (i64 i = (i64)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+         i += (i64)gridDim.x * blockDim.x) {
+        const u64 xc = (b.x[wc * b.cap + i] & mc) != 0, zc = (b.z[wc * b.cap + i] & mc) != 0;
+        const u64 xt = (b.x[wt * b.cap + i] & mt) != 0, zt = (b.z[wt * b.cap + i] & mt) != 0;
+        b.f[i] ^= (u8)((xc & zt & (1ull ^ xt ^ zc)) << 1);
+        b.x[wt * b.cap + i] ^= (0ull - xc) & mt;
+        b.z[wc * b.cap + i] ^= (0ull - zt) & mc;
+    }
+}
+
+// isCloseOne (PauliSumOperations.h:19-21).
+bool close_one(double v) { return std::fabs(v - 1.0) <= 1e-14; }
+
+}  // namespace
+}  // namespace pl
+
+// ===========================================================================
+// Host state
+// ===========================================================================
+using namespace pl;
+
+struct pl_state {
+    int as = 1;
+    cudaStream_t st = nullptr;
+    i64 cap = 0;
+    void* mem = nullptr;
+    Buf S[2], R0, R1, N;
+    int cur = 0;
+    i64* d_size = nullptr;  // [2]: sizes of S[0], S[1]
+    i64* d_k = nullptr;     // [2]: run sizes
+    i64* d_tmp = nullptr;   // scratch count
+    int* d_status = nullptr;
+    int* d_fail = nullptr;
+    u64* lbA = nullptr;
+    u32* lbC = nullptr;
+    u32* ctr = nullptr;     // [8]
+    u32 *spB_lo = nullptr, *spB_hi = nullptr, *spC_lo = nullptr, *spC_hi = nullptr;
+    u32 max_tiles = 0;
+    size_t zero_bytes = 0;  // bytes from lbA to the end of the counters (one memset per gate)
+    DevArena ws;            // collate workspace
+    // 0: anything; 1: distinct (x,z,phase) keys; 2: canonical and sorted
+    int cls = 0;
+};
+
+namespace pl {
+namespace {
+
+inline size_t a256(size_t b) { return (b + 255) & ~size_t(255); }
+
+size_t buf_bytes(int as, i64 cap) {
+    return 2 * a256(8 * (size_t)as * cap) + a256(cap) + a256(8 * (size_t)cap);
+}
+
+Buf carve_buf(unsigned char*& p, int as, i64 cap) {
+    Buf b;
+    b.cap = cap;
+    b.x = (u64*)p;
+    p += a256(8 * (size_t)as * cap);
+    b.z = (u64*)p;
+    p += a256(8 * (size_t)as * cap);
+    b.v = (double*)p;
+    p += a256(8 * (size_t)cap);
+    b.f = (u8*)p;
+    p += a256(cap);
+    return b;
+}
+
+// Allocate all buffers for capacity cap (contents undefined).
+int state_alloc(pl_state* s, i64 cap, void** mem_out, Buf* S, Buf& R0, Buf& R1, Buf& N,
+                size_t* small_off) {
+    const u32 max_tiles = (u32)((2 * cap) / 256 + 4);
+    size_t total = 5 * buf_bytes(s->as, cap);
+    const size_t small = a256(8 * (size_t)max_tiles) + a256(4 * (size_t)max_tiles) +
+                         a256(4 * 16) + 4 * a256(4 * (size_t)max_tiles) + a256(8 * 8) + a256(64);
+    total += small;
+    void* mem = nullptr;
+    if (cudaMalloc(&mem, total) != cudaSuccess) {
+        cudaGetLastError();
+        return record_status(PL_ERR_OOM, "pl_state buffers");
+    }
+    unsigned char* p = (unsigned char*)mem;
+    S[0] = carve_buf(p, s->as, cap);
+    S[1] = carve_buf(p, s->as, cap);
+    R0 = carve_buf(p, s->as, cap);
+    R1 = carve_buf(p, s->as, cap);
+    N = carve_buf(p, s->as, cap);
+    *small_off = (size_t)(p - (unsigned char*)mem);
+    *mem_out = mem;
+    return PL_OK;
+}
+
+void wire_small(pl_state* s, unsigned char* p, u32 max_tiles) {
+    s->max_tiles = max_tiles;
+    unsigned char* z0 = p;
+    s->lbA = (u64*)p;
+    p += a256(8 * (size_t)max_tiles);
+    s->lbC = (u32*)p;
+    p += a256(4 * (size_t)max_tiles);
+    s->ctr = (u32*)p;
+    p += a256(4 * 16);
+    s->zero_bytes = (size_t)(p - z0);
+    s->spB_lo = (u32*)p;
+    p += a256(4 * (size_t)max_tiles);
+    s->spB_hi = (u32*)p;
+    p += a256(4 * (size_t)max_tiles);
+    s->spC_lo = (u32*)p;
+    p += a256(4 * (size_t)max_tiles);
+    s->spC_hi = (u32*)p;
+    p += a256(4 * (size_t)max_tiles);
+    s->d_size = (i64*)p;
+    s->d_k = s->d_size + 2;
+    s->d_tmp = s->d_size + 4;
+    p += a256(8 * 8);
+    s->d_status = (int*)p;
+    s->d_fail = s->d_status + 1;
+}
+
+// (Re)build all buffers with capacity >= need, keeping the current state.
+int state_grow(pl_state* s, i64 need) {
+    i64 cap = std::max<i64>(need, std::max<i64>(2 * s->cap, 1 << 16));
+    i64 n = 0;
+    if (s->mem) {
+        PL_CUDA_TRY(cudaMemcpyAsync(&n, s->d_size + s->cur, sizeof(i64), cudaMemcpyDeviceToHost,
+                                    s->st));
+        PL_CUDA_TRY(cudaStreamSynchronize(s->st));
+    }
+    void* mem = nullptr;
+    Buf S[2], R0, R1, N;
+    size_t off = 0;
+    const int rc = state_alloc(s, cap, &mem, S, R0, R1, N, &off);
+    if (rc) return rc;
+    int status = 0, fail = 0;
+    if (s->mem) {
+        const Buf& o = s->S[s->cur];
+        if (n > 0) {
+            PL_CUDA_TRY(cudaMemcpy2DAsync(S[0].x, 8 * cap, o.x, 8 * o.cap, 8 * n, s->as,
+                                          cudaMemcpyDeviceToDevice, s->st));
+            PL_CUDA_TRY(cudaMemcpy2DAsync(S[0].z, 8 * cap, o.z, 8 * o.cap, 8 * n, s->as,
+                                          cudaMemcpyDeviceToDevice, s->st));
+            PL_CUDA_TRY(cudaMemcpyAsync(S[0].f, o.f, n, cudaMemcpyDeviceToDevice, s->st));
+            PL_CUDA_TRY(cudaMemcpyAsync(S[0].v, o.v, 8 * n, cudaMemcpyDeviceToDevice, s->st));
+        }
+        PL_CUDA_TRY(cudaMemcpyAsync(&status, s->d_status, sizeof(int), cudaMemcpyDeviceToHost,
+                                    s->st));
+        PL_CUDA_TRY(cudaStreamSynchronize(s->st));
+        cudaFree(s->mem);
+    }
+    s->mem = mem;
+    s->cap = cap;
+    s->S[0] = S[0];
+    s->S[1] = S[1];
+    s->R0 = R0;
+    s->R1 = R1;
+    s->N = N;
+    s->cur = 0;
+    wire_small(s, (unsigned char*)mem + off, (u32)((2 * cap) / 256 + 4));
+    i64 sizes[8] = {n, 0, 0, 0, 0, 0, 0, 0};
+    int st2[2] = {status == PL_ERR_CAPACITY ? 0 : status, fail};
+    PL_CUDA_TRY(cudaMemcpyAsync(s->d_size, sizes, sizeof(sizes), cudaMemcpyHostToDevice, s->st));
+    PL_CUDA_TRY(cudaMemcpyAsync(s->d_status, st2, sizeof(st2), cudaMemcpyHostToDevice, s->st));
+    PL_CUDA_TRY(cudaStreamSynchronize(s->st));
+    return PL_OK;
+}
+
+int read_size(pl_state* s, i64* n) {
+    PL_CUDA_TRY(cudaMemcpyAsync(n, s->d_size + s->cur, sizeof(i64), cudaMemcpyDeviceToHost, s->st));
+    PL_CUDA_TRY(cudaStreamSynchronize(s->st));
+    return PL_OK;
+}
+
+int read_status(pl_state* s, int* status, int* fail) {
+    int v[2] = {0, 0};
+    PL_CUDA_TRY(cudaMemcpyAsync(v, s->d_status, sizeof(v), cudaMemcpyDeviceToHost, s->st));
+    PL_CUDA_TRY(cudaStreamSynchronize(s->st));
+    *status = v[0];
+    *fail = v[1];
+    return PL_OK;
+}
+
+int clear_status(pl_state* s) {
+    PL_CUDA_TRY(cudaMemsetAsync(s->d_status, 0, 2 * sizeof(int), s->st));
+    return PL_OK;
+}
+
+SoAView view_of(const Buf& b, i64 n) { return SoAView{b.x, b.z, b.f, b.v, n, b.cap}; }
+SoAOut out_of(const Buf& b) { return SoAOut{b.x, b.z, b.f, b.v, b.cap}; }
+
+// Collate S[cur] (n terms, host-known) into S[other].
+int state_collate(pl_state* s, i64 n, const CollateArgs& a) {
+    if (n > s->cap) return record_status(PL_ERR_INTERNAL, "state_collate size");
+    const size_t need = collate_ws_bytes(s->as, n);
+    int rc = s->ws.ensure(need);
+    if (rc) return rc;
+    const int other = 1 - s->cur;
+    i64 cnt = 0;
+    rc = collate_soa(s->as, view_of(s->S[s->cur], n), out_of(s->S[other]), a, &cnt, s->ws.ptr,
+                     s->ws.bytes, s->st);
+    if (rc) return rc;
+    PL_CUDA_TRY(cudaMemcpyAsync(s->d_size + other, &cnt, sizeof(i64), cudaMemcpyHostToDevice,
+                                s->st));
+    PL_CUDA_TRY(cudaStreamSynchronize(s->st));
+    s->cur = other;
+    return PL_OK;
+}
+
+struct Rot {
+    std::vector<u64> px, pz;
+    u32 pf;
+    double theta;
+};
+
+template <int AS>
+GateP<AS> make_gate(const Rot& r, bool* single) {
+    GateP<AS> g;
+    int bits = 0, cw = 0;
+    u64 cm = 0;
+    int cls_x = 1;
+    for (int k = 0; k < AS; ++k) {
+        g.px[k] = r.px[k];
+        g.pz[k] = r.pz[k];
+    }
+    // the class bit: the generator's first set x bit, else its first z bit
+    for (int k = 0; k < AS && !cm; ++k)
+        if (r.px[k]) {
+            cw = k;
+            cm = r.px[k] & (~r.px[k] + 1);
+            cls_x = 1;
+        }
+    for (int k = 0; k < AS && !cm; ++k)
+        if (r.pz[k]) {
+            cw = k;
+            cm = r.pz[k] & (~r.pz[k] + 1);
+            cls_x = 0;
+        }
+    for (int k = 0; k < AS; ++k) bits += __builtin_popcountll(r.px[k] | r.pz[k]);
+    g.psf = (r.pf ^ 1u) & 3u;
+    g.cw = cw;
+    g.cmask = cm;
+    g.cls_x = cls_x;
+    *single = bits == 1;
+    return g;
+}
+
+int classify(double theta, double* c, double* sn) {
+    *c = std::cos(theta);
+    *sn = std::sin(theta);
+    if (close_one(*c)) return kSkip;
+    if (close_one(-*c)) return kNegate;
+    if (close_one(*sn)) return kHalfPos;
+    if (close_one(-*sn)) return kHalfNeg;
+    return kGeneral;
+}
+
+int grid_persistent(int per_sm) { return sm_count() * per_sm; }
+
+template <int AS>
+int set_smem_attrs() {
+    static thread_local bool done[kMaxAS + 1] = {};
+    if (done[AS]) return PL_OK;
+    constexpr int T = ptile<AS>();
+    PL_CUDA_TRY(cudaFuncSetAttribute(k_merge_runs<AS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)tile_smem_bytes<AS>(T)));
+    PL_CUDA_TRY(cudaFuncSetAttribute(k_merge_reduce<AS>,
+                                     cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)tile_smem_bytes<AS>(T + 2)));
+    done[AS] = true;
+    return PL_OK;
+}
+
+// One fast-path rotation on a canonical state: S[cur] -> S[1-cur].
+template <int AS>
+int fast_rotation(pl_state* s, const GateP<AS>& g, int mode, double c, double sn,
+                  const pl_truncation& tr, int gate_index) {
+    PL_CUDA_TRY(cudaMemsetAsync(s->lbA, 0, s->zero_bytes, s->st));
+    const int in = s->cur, outb = 1 - s->cur;
+    constexpr int T = ptile<AS>();
+    k_expand<AS><<<grid_persistent(4), kPT, 0, s->st>>>(
+        s->S[in], s->d_size + in, g, mode, -sn, s->R0, s->R1, s->d_k, s->lbA, s->ctr + 0,
+        s->d_status, s->cap, gate_index, s->d_fail);
+    const int pgrid = std::max(1, (int)((s->max_tiles + 255) / 256));
+    k_partition<AS><<<pgrid, 256, 0, s->st>>>(s->R0, s->d_k, s->R1, s->d_k + 1, nullptr, T, 0,
+                                              s->spB_lo, s->spB_hi, s->max_tiles, s->d_status);
+    k_merge_runs<AS><<<grid_persistent(2), kPT, tile_smem_bytes<AS>(T), s->st>>>(
+        s->R0, s->R1, s->d_k, s->spB_lo, s->spB_hi, s->N, s->ctr + 1, s->d_status);
+    k_partition<AS><<<pgrid, 256, 0, s->st>>>(s->S[in], s->d_size + in, s->N, s->d_k, s->d_k + 1,
+                                              T, 1, s->spC_lo, s->spC_hi, s->max_tiles,
+                                              s->d_status);
+    const u64 mw = tr.max_weight;
+    const double cut = tr.coefficient_cutoff > 0.0 ? tr.coefficient_cutoff : 0.0;
+    k_merge_reduce<AS><<<grid_persistent(2), kPT, tile_smem_bytes<AS>(T + 2), s->st>>>(
+        s->S[in], s->d_size + in, s->N, s->d_k, s->spC_lo, s->spC_hi, g, mode, c, s->S[outb],
+        s->d_size + outb, mw, cut, s->lbC, s->ctr + 2, s->d_status, gate_index, s->d_fail);
+    PL_CUDA_TRY(cudaGetLastError());
+    s->cur = outb;
+    return PL_OK;
+}
+
+// General-path rotation (any state, any generator) with or without the
+// following apply_truncation.
+template <int AS>
+int general_rotation(pl_state* s, const Rot& r, bool truncate, const pl_truncation& tr) {
+    bool single = false;
+    const GateP<AS> g = make_gate<AS>(r, &single);
+    double c, sn;
+    const int mode = classify(r.theta, &c, &sn);
+    i64 n = 0;
+    int rc = read_size(s, &n);
+    if (rc) return rc;
+    const int grid = grid_for(n, 256, sm_count() * 8);
+    if (mode == kNegate) {
+        k_negate<AS><<<grid, 256, 0, s->st>>>(s->S[s->cur], s->d_size + s->cur, g, 0,
+                                              s->d_status);
+        if (s->cls == 2) s->cls = 1;
+    } else if (mode == kHalfPos || mode == kHalfNeg) {
+        k_halfpi_inplace<AS><<<grid, 256, 0, s->st>>>(s->S[s->cur], s->d_size + s->cur, g,
+                                                      mode == kHalfPos, s->d_status);
+        if (s->cls == 2) s->cls = 1;
+    } else if (mode == kGeneral) {
+        // old + children can need up to 2n slots
+        if (2 * n > s->cap) {
+            rc = state_grow(s, 2 * n);
+            if (rc) return rc;
+        }
+        PL_CUDA_TRY(cudaMemsetAsync(s->lbA, 0, s->zero_bytes, s->st));
+        const int other = 1 - s->cur;
+        k_materialize<AS><<<grid_persistent(4), kPT, 0, s->st>>>(
+            s->S[s->cur], n, g, c, -sn, s->S[other], s->d_tmp, s->lbA, s->ctr + 0, s->d_status);
+        i64 total = 0;
+        PL_CUDA_TRY(cudaMemcpyAsync(&total, s->d_tmp, sizeof(i64), cudaMemcpyDeviceToHost, s->st));
+        int st[2];
+        PL_CUDA_TRY(cudaMemcpyAsync(st, s->d_status, sizeof(st), cudaMemcpyDeviceToHost, s->st));
+        PL_CUDA_TRY(cudaStreamSynchronize(s->st));
+        if (n == 0) total = 0;
+        if (st[0]) return record_status(st[0], "evolve: materialise");
+        s->cur = other;
+        CollateArgs a;
+        if (truncate) {
+            a.mode = kProp;
+            a.cutoff = tr.coefficient_cutoff > 0.0 ? tr.coefficient_cutoff : 0.0;
+            a.max_weight = tr.max_weight;
+        } else {
+            a.mode = kCombine;
+        }
+        rc = state_collate(s, total, a);
+        if (rc) return rc;
+        s->cls = truncate ? 2 : 0;
+        return PL_OK;
+    }
+    PL_CUDA_TRY(cudaGetLastError());
+    if (!truncate) return PL_OK;
+    // apply_truncation after a fast-path branch
+    rc = read_size(s, &n);
+    if (rc) return rc;
+    CollateArgs a;
+    a.mode = kCanon;
+    a.cutoff = tr.coefficient_cutoff > 0.0 ? tr.coefficient_cutoff : 0.0;
+    a.max_weight = tr.max_weight;
+    rc = state_collate(s, n, a);
+    if (rc) return rc;
+    s->cls = 2;
+    return PL_OK;
+}
+
+// Make a state of class 1 (distinct keys) canonical: sort by (x, z, phase),
+// folding signs (values then carry the sign; see the header comment).
+int state_canonical_sort(pl_state* s) {
+    i64 n = 0;
+    int rc = read_size(s, &n);
+    if (rc) return rc;
+    CollateArgs a;
+    a.mode = kCanon;
+    rc = state_collate(s, n, a);
+    if (rc) return rc;
+    s->cls = 2;
+    return PL_OK;
+}
+
+struct Op {
+    int kind;  // 0 rotation, 1 CNOT
+    int a, b;
+};
+
+template <int AS>
+int run_ops(pl_state* s, const std::vector<Rot>& rots, const std::vector<Op>& ops,
+            const pl_truncation& tr) {
+    if (tr.max_terms != ~0ull)
+        return record_status(PL_ERR_UNSUPPORTED, "max_terms truncation (trim) is not built");
+    int rc = set_smem_attrs<AS>();
+    if (rc) return rc;
+    // per-rotation device parameters
+    std::vector<GateP<AS>> gates(rots.size());
+    std::vector<int> modes(rots.size()), singles(rots.size());
+    std::vector<double> cs(rots.size()), sns(rots.size());
+    for (size_t r = 0; r < rots.size(); ++r) {
+        bool single = false;
+        gates[r] = make_gate<AS>(rots[r], &single);
+        singles[r] = single;
+        modes[r] = classify(rots[r].theta, &cs[r], &sns[r]);
+    }
+    constexpr int kWindow = 192;
+    std::vector<int> in_buf(ops.size(), 0);
+    size_t i = 0, since_sync = 0;
+    bool pending = false;  // fast-path work not yet checked
+    // Check queued work; on a capacity overflow, grow and rewind to the
+    // failing gate (its input buffer is untouched).  Returns false on error.
+    auto checkpoint = [&](bool* rewound) -> int {
+        *rewound = false;
+        int st = 0, fail = 0;
+        int r = read_status(s, &st, &fail);
+        if (r) return r;
+        since_sync = 0;
+        pending = false;
+        if (st == 0) return PL_OK;
+        if (st != PL_ERR_CAPACITY) return record_status(st, "propagate: device check");
+        s->cur = in_buf[fail];
+        s->cls = 2;
+        i64 m = 0, k[2] = {0, 0};
+        PL_CUDA_TRY(cudaMemcpyAsync(&m, s->d_size + s->cur, sizeof(i64), cudaMemcpyDeviceToHost,
+                                    s->st));
+        PL_CUDA_TRY(cudaMemcpyAsync(k, s->d_k, sizeof(k), cudaMemcpyDeviceToHost, s->st));
+        PL_CUDA_TRY(cudaStreamSynchronize(s->st));
+        r = clear_status(s);
+        if (r) return r;
+        r = state_grow(s, 2 * std::max<i64>(m + k[0] + k[1], 2 * m));
+        if (r) return r;
+        i = (size_t)fail;
+        *rewound = true;
+        return PL_OK;
+    };
+    while (i < ops.size()) {
+        const Op& op = ops[i];
+        bool rewound = false;
+        if (op.kind == 1) {
+            if (s->cls == 2) s->cls = 1;
+            in_buf[i] = s->cur;
+            k_cnot_state<AS><<<grid_persistent(8), 256, 0, s->st>>>(
+                s->S[s->cur], s->d_size + s->cur, op.a / 64, 1ull << (op.a % 64), op.b / 64,
+                1ull << (op.b % 64), s->d_status);
+            pending = true;
+            ++i;
+            ++since_sync;
+        } else {
+            const int r = op.a;
+            const bool fast_ok = singles[r] && (s->cls == 2 || s->cls == 1);
+            if (fast_ok && s->cls == 1 && modes[r] != kSkip) {
+                // the state must be canonical (sorted) before the merge path
+                rc = checkpoint(&rewound);
+                if (rc) return rc;
+                if (rewound) continue;
+                rc = state_canonical_sort(s);
+                if (rc) return rc;
+            }
+            if (fast_ok && s->cls == 2) {
+                in_buf[i] = s->cur;
+                if (modes[r] == kNegate) {
+                    k_negate<AS><<<grid_persistent(8), 256, 0, s->st>>>(
+                        s->S[s->cur], s->d_size + s->cur, gates[r], 1, s->d_status);
+                } else if (modes[r] != kSkip) {
+                    rc = fast_rotation<AS>(s, gates[r], modes[r], cs[r], sns[r], tr, (int)i);
+                    if (rc) return rc;
+                }
+                pending = true;
+                ++i;
+                ++since_sync;
+            } else if (modes[r] == kSkip && s->cls == 2) {
+                ++i;
+            } else {
+                // general path (synchronous)
+                rc = checkpoint(&rewound);
+                if (rc) return rc;
+                if (rewound) continue;
+                rc = general_rotation<AS>(s, rots[r], true, tr);
+                if (rc) return rc;
+                ++i;
+            }
+        }
+        if (pending && (since_sync >= (size_t)kWindow || i == ops.size())) {
+            rc = checkpoint(&rewound);
+            if (rc) return rc;
+        }
+    }
+    return PL_OK;
+}
+
+int check_state(pl_state* s) {
+    if (!s) return record_status(PL_ERR_INVALID_ARG, "pl_state is NULL");
+    return PL_OK;
+}
+
+std::vector<Rot> host_rotations(int as, const u64* rx, const u64* rz, const u8* rf,
+                                const double* th, i64 n_rot) {
+    std::vector<Rot> v((size_t)n_rot);
+    for (i64 r = 0; r < n_rot; ++r) {
+        v[r].px.resize(as);
+        v[r].pz.resize(as);
+        for (int k = 0; k < as; ++k) {
+            v[r].px[k] = rx[(size_t)k * n_rot + r];
+            v[r].pz[k] = rz[(size_t)k * n_rot + r];
+        }
+        v[r].pf = rf ? rf[r] : 0;
+        v[r].theta = th[r];
+    }
+    return v;
+}
+
+}  // namespace
+}  // namespace pl
+
+// ===========================================================================
+// C ABI
+// ===========================================================================
+extern "C" int pl_state_create(pl_state** out, int array_size, int64_t capacity_hint,
+                               cudaStream_t stream) {
+    if (!out || array_size < 1 || array_size > kMaxAS || capacity_hint < 0)
+        return record_status(PL_ERR_INVALID_ARG, "pl_state_create");
+    pl_state* s = new pl_state();
+    s->as = array_size;
+    s->st = stream;
+    const int rc = state_grow(s, std::max<int64_t>(capacity_hint, 1 << 16));
+    if (rc) {
+        delete s;
+        return rc;
+    }
+    *out = s;
+    return record_status(PL_OK, nullptr);
+}
+
+extern "C" int pl_state_destroy(pl_state* s) {
+    if (!s) return record_status(PL_OK, nullptr);
+    cudaStreamSynchronize(s->st);
+    if (s->mem) cudaFree(s->mem);
+    delete s;
+    return record_status(PL_OK, nullptr);
+}
+
+extern "C" int pl_state_upload(pl_state* s, const uint64_t* x, const uint64_t* z,
+                               const uint8_t* flags, const double* val, int64_t n) {
+    int rc = check_state(s);
+    if (rc) return rc;
+    if (n < 0 || (n > 0 && (!x || !z || !flags || !val)) || n >= (1ll << 30))
+        return record_status(PL_ERR_INVALID_ARG, "pl_state_upload");
+    if (n > s->cap) {
+        rc = state_grow(s, 2 * n);
+        if (rc) return rc;
+    }
+    const Buf& b = s->S[s->cur];
+    if (n > 0) {
+        PL_CUDA_TRY(cudaMemcpy2DAsync(b.x, 8 * b.cap, x, 8 * n, 8 * n, s->as,
+                                      cudaMemcpyHostToDevice, s->st));
+        PL_CUDA_TRY(cudaMemcpy2DAsync(b.z, 8 * b.cap, z, 8 * n, 8 * n, s->as,
+                                      cudaMemcpyHostToDevice, s->st));
+        PL_CUDA_TRY(cudaMemcpyAsync(b.f, flags, n, cudaMemcpyHostToDevice, s->st));
+        PL_CUDA_TRY(cudaMemcpyAsync(b.v, val, 8 * n, cudaMemcpyHostToDevice, s->st));
+    }
+    i64 nn = n;
+    PL_CUDA_TRY(cudaMemcpyAsync(s->d_size + s->cur, &nn, sizeof(i64), cudaMemcpyHostToDevice,
+                                s->st));
+    PL_CUDA_TRY(cudaMemsetAsync(s->d_status, 0, 2 * sizeof(int), s->st));
+    PL_CUDA_TRY(cudaStreamSynchronize(s->st));
+    s->cls = 0;
+    return record_status(PL_OK, nullptr);
+}
+
+extern "C" int pl_state_size(pl_state* s, int64_t* n) {
+    int rc = check_state(s);
+    if (rc) return rc;
+    if (!n) return record_status(PL_ERR_INVALID_ARG, "pl_state_size");
+    i64 v = 0;
+    rc = read_size(s, &v);
+    if (rc) return rc;
+    *n = v;
+    return record_status(PL_OK, nullptr);
+}
+
+extern "C" int pl_state_download(pl_state* s, uint64_t* x, uint64_t* z, uint8_t* flags,
+                                 double* val, int64_t capacity, int64_t* n_out) {
+    int rc = check_state(s);
+    if (rc) return rc;
+    if (!n_out) return record_status(PL_ERR_INVALID_ARG, "pl_state_download");
+    i64 n = 0;
+    rc = read_size(s, &n);
+    if (rc) return rc;
+    *n_out = n;
+    if (!x) return record_status(PL_OK, nullptr);
+    if (n > capacity || !z || !flags || !val)
+        return record_status(PL_ERR_CAPACITY, "pl_state_download: host buffer too small");
+    const Buf& b = s->S[s->cur];
+    if (n > 0) {
+        PL_CUDA_TRY(cudaMemcpy2DAsync(x, 8 * n, b.x, 8 * b.cap, 8 * n, s->as,
+                                      cudaMemcpyDeviceToHost, s->st));
+        PL_CUDA_TRY(cudaMemcpy2DAsync(z, 8 * n, b.z, 8 * b.cap, 8 * n, s->as,
+                                      cudaMemcpyDeviceToHost, s->st));
+        PL_CUDA_TRY(cudaMemcpyAsync(flags, b.f, n, cudaMemcpyDeviceToHost, s->st));
+        PL_CUDA_TRY(cudaMemcpyAsync(val, b.v, 8 * n, cudaMemcpyDeviceToHost, s->st));
+    }
+    PL_CUDA_TRY(cudaStreamSynchronize(s->st));
+    return record_status(PL_OK, nullptr);
+}
+
+extern "C" int pl_state_evolve(pl_state* s, const uint64_t* rot_x, const uint64_t* rot_z,
+                               const uint8_t* rot_flags, const double* rot_theta,
+                               int64_t n_rot) {
+    int rc = check_state(s);
+    if (rc) return rc;
+    if (n_rot < 0 || (n_rot > 0 && (!rot_x || !rot_z || !rot_theta)))
+        return record_status(PL_ERR_INVALID_ARG, "pl_state_evolve");
+    const auto rots = host_rotations(s->as, (const u64*)rot_x, (const u64*)rot_z, rot_flags,
+                                     rot_theta, n_rot);
+    pl_truncation tr{~0ull, 0.0, ~0ull};
+    PL_DISPATCH_AS(s->as, for (const Rot& r : rots) {
+        double c, sn;
+        if (classify(r.theta, &c, &sn) == kSkip) continue;
+        rc = general_rotation<AS>(s, r, false, tr);
+        if (rc) return rc;
+    });
+    int st = 0, fail = 0;
+    rc = read_status(s, &st, &fail);
+    if (rc) return rc;
+    if (st) return record_status(st, "pl_state_evolve");
+    return record_status(PL_OK, nullptr);
+}
+
+static int collate_state_api(pl_state* s, int mode, double cutoff, uint64_t max_weight) {
+    int rc = check_state(s);
+    if (rc) return rc;
+    i64 n = 0;
+    rc = read_size(s, &n);
+    if (rc) return rc;
+    CollateArgs a;
+    a.mode = mode;
+    a.cutoff = cutoff;
+    a.max_weight = max_weight;
+    rc = state_collate(s, n, a);
+    if (rc) return rc;
+    s->cls = mode == kCombine ? 0 : 2;
+    return record_status(PL_OK, nullptr);
+}
+
+extern "C" int pl_state_canonicalize(pl_state* s) {
+    return collate_state_api(s, kCanon, 0.0, ~0ull);
+}
+extern "C" int pl_state_sort_and_combine(pl_state* s) {
+    return collate_state_api(s, kCombine, 0.0, ~0ull);
+}
+extern "C" int pl_state_apply_truncation(pl_state* s, const pl_truncation* o) {
+    if (!o) return record_status(PL_ERR_INVALID_ARG, "pl_state_apply_truncation");
+    if (o->max_terms != ~0ull)
+        return record_status(PL_ERR_UNSUPPORTED, "max_terms truncation (trim) is not built");
+    return collate_state_api(s, kCanon, o->coefficient_cutoff > 0 ? o->coefficient_cutoff : 0.0,
+                             o->max_weight);
+}
+
+static int filter_state(pl_state* s, double eps, uint64_t max_weight) {
+    int rc = check_state(s);
+    if (rc) return rc;
+    i64 n = 0;
+    rc = read_size(s, &n);
+    if (rc) return rc;
+    const int other = 1 - s->cur;
+    PL_CUDA_TRY(cudaMemsetAsync(s->lbA, 0, s->zero_bytes, s->st));
+    PL_DISPATCH_AS(s->as, k_filter<AS><<<grid_persistent(4), kPT, 0, s->st>>>(
+                              s->S[s->cur], n, s->S[other], eps, max_weight, s->d_size + other,
+                              s->lbC, s->ctr + 3, s->d_status));
+    PL_CUDA_TRY(cudaGetLastError());
+    if (n == 0) {
+        i64 z = 0;
+        PL_CUDA_TRY(cudaMemcpyAsync(s->d_size + other, &z, sizeof(i64), cudaMemcpyHostToDevice,
+                                    s->st));
+    }
+    int st = 0, fail = 0;
+    rc = read_status(s, &st, &fail);
+    if (rc) return rc;
+    if (st) return record_status(st, "filter");
+    s->cur = other;
+    return record_status(PL_OK, nullptr);
+}
+
+extern "C" int pl_state_cutoff(pl_state* s, double eps) {
+    return filter_state(s, eps > 0 ? eps : -1.0, ~0ull);
+}
+extern "C" int pl_state_truncate_weight(pl_state* s, uint64_t max_weight) {
+    return filter_state(s, 0.0, max_weight);
+}
+
+extern "C" int pl_state_apply_cnot(pl_state* s, int control, int target) {
+    int rc = check_state(s);
+    if (rc) return rc;
+    if (control < 0 || target < 0 || control >= 64 * s->as || target >= 64 * s->as ||
+        control == target)
+        return record_status(PL_ERR_INVALID_ARG, "pl_state_apply_cnot");
+    PL_DISPATCH_AS(s->as, k_cnot_state<AS><<<grid_persistent(8), 256, 0, s->st>>>(
+                              s->S[s->cur], s->d_size + s->cur, control / 64,
+                              1ull << (control % 64), target / 64, 1ull << (target % 64),
+                              s->d_status));
+    PL_CUDA_TRY(cudaGetLastError());
+    if (s->cls == 2) s->cls = 1;
+    return record_status(PL_OK, nullptr);
+}
+
+extern "C" int pl_state_zero_state_expectation(pl_state* s, double* result) {
+    int rc = check_state(s);
+    if (rc) return rc;
+    if (!result) return record_status(PL_ERR_INVALID_ARG, "pl_state_zero_state_expectation");
+    i64 n = 0;
+    rc = read_size(s, &n);
+    if (rc) return rc;
+    const Buf& b = s->S[s->cur];
+    rc = pl_zero_state_expectation(s->as, (const uint64_t*)b.x, b.f, b.v, n, b.cap,
+                                   (double*)s->d_tmp, s->st);
+    if (rc) return rc;
+    PL_CUDA_TRY(cudaMemcpyAsync(result, s->d_tmp, sizeof(double), cudaMemcpyDeviceToHost, s->st));
+    PL_CUDA_TRY(cudaStreamSynchronize(s->st));
+    return record_status(PL_OK, nullptr);
+}
+
+extern "C" int pl_propagate(pl_state* s, const uint64_t* rot_x, const uint64_t* rot_z,
+                            const uint8_t* rot_flags, const double* rot_theta, int64_t n_rot,
+                            const int32_t* ops, int64_t n_ops, const pl_truncation* opts) {
+    int rc = check_state(s);
+    if (rc) return rc;
+    if (!opts || n_rot < 0 || (n_rot > 0 && (!rot_x || !rot_z || !rot_theta)) || n_ops < 0 ||
+        (ops && n_ops > 0 && !ops))
+        return record_status(PL_ERR_INVALID_ARG, "pl_propagate");
+    const auto rots = host_rotations(s->as, (const u64*)rot_x, (const u64*)rot_z, rot_flags,
+                                     rot_theta, n_rot);
+    // Heisenberg order: walk the circuit backwards.
+    std::vector<Op> list;
+    if (ops) {
+        list.reserve((size_t)n_ops);
+        for (i64 l = n_ops; l-- > 0;) {
+            const int kind = ops[3 * l], a = ops[3 * l + 1], b = ops[3 * l + 2];
+            if (kind == PL_OP_ROTATION) {
+                if (a < 0 || a >= n_rot)
+                    return record_status(PL_ERR_INVALID_ARG, "pl_propagate: rotation index");
+            } else if (kind == PL_OP_CNOT) {
+                if (a < 0 || b < 0 || a >= 64 * s->as || b >= 64 * s->as || a == b)
+                    return record_status(PL_ERR_INVALID_ARG, "pl_propagate: CNOT qubits");
+            } else {
+                return record_status(PL_ERR_INVALID_ARG, "pl_propagate: op kind");
+            }
+            list.push_back(Op{kind == PL_OP_CNOT ? 1 : 0, a, b});
+        }
+    } else {
+        for (i64 l = n_rot; l-- > 0;) list.push_back(Op{0, (int)l, 0});
+    }
+    PL_DISPATCH_AS(s->as, rc = run_ops<AS>(s, rots, list, *opts));
+    if (rc) return rc;
+    int st = 0, fail = 0;
+    rc = read_status(s, &st, &fail);
+    if (rc) return rc;
+    if (st) return record_status(st, "pl_propagate");
+    return record_status(PL_OK, nullptr);
+}

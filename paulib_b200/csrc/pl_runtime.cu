@@ -1,0 +1,76 @@
+// pl_runtime.cu -- status reporting and per-device bookkeeping.
+//
+// The reference reports CUDA failures by throwing std::runtime_error
+// (include/gpu/GpuPauliSum.h:25-30) and traps on a bad array size
+// (src/gpu/gpu_mul.cu:122-131).  Here every entry point returns a status
+// code; the most recent status and a message are kept per host thread so
+// the void drop-ins can be checked with pl_get_last_error().
+
+#include <cstdio>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "pl_collate.cuh"
+#include "pl_common.cuh"
+
+namespace {
+thread_local int g_last_status = PL_OK;
+thread_local std::string g_last_msg;
+}  // namespace
+
+namespace pl {
+
+int record_status(int code, const char* what) {
+    g_last_status = code;
+    if (code == PL_OK) {
+        g_last_msg.clear();
+    } else {
+        g_last_msg = std::string(pl_status_string(code)) + (what ? std::string(": ") + what : "");
+    }
+    return code;
+}
+
+int record_cuda(cudaError_t e) {
+    const char* s = cudaGetErrorString(e);
+    cudaGetLastError();  // clear a sticky launch error where possible
+    g_last_status = e == cudaErrorMemoryAllocation ? PL_ERR_OOM : PL_ERR_CUDA;
+    g_last_msg = std::string("CUDA: ") + (s ? s : "unknown error");
+    return g_last_status;
+}
+
+int sm_count() {
+    static std::mutex mu;
+    static std::vector<int> cache;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    std::lock_guard<std::mutex> lock(mu);
+    if ((int)cache.size() <= dev) cache.resize(dev + 1, 0);
+    if (cache[dev] == 0) {
+        int v = 0;
+        if (cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || v <= 0)
+            v = 148;
+        cache[dev] = v;
+    }
+    return cache[dev];
+}
+
+}  // namespace pl
+
+extern "C" const char* pl_status_string(int status) {
+    switch (status) {
+        case PL_OK: return "ok";
+        case PL_ERR_INVALID_ARG: return "invalid argument";
+        case PL_ERR_OOM: return "out of device memory";
+        case PL_ERR_TIMEOUT: return "device wait timed out";
+        case PL_ERR_CUDA: return "CUDA error";
+        case PL_ERR_CAPACITY: return "output capacity exceeded";
+        case PL_ERR_UNSUPPORTED: return "unsupported";
+        case PL_ERR_INTERNAL: return "internal consistency check failed";
+        default: return "unknown status";
+    }
+}
+
+extern "C" int pl_get_last_error(void) { return g_last_status; }
+extern "C" const char* pl_last_error_message(void) { return g_last_msg.c_str(); }
+extern "C" int pl_version(void) { return 1; }

@@ -1,0 +1,385 @@
+// pl_terms.cu -- per-term and per-pair kernels: outer product, commutator,
+// apply_CNOT, zero_state_expectation.
+//
+//   outer product     PauliSum::multiply(rhs), PauliSumOperations.h:256-306;
+//                     reference GPU kernel src/gpu/gpu_mul.cu:50-97
+//   commutator        commutator_impl, PauliSumOperations.h:316-346;
+//                     reference GPU kernel src/gpu/gpu_commutator.cu:25-87
+//   apply_CNOT        PauliSumClifford.h:213-239
+//   zero_state_exp.   PauliSumUtils.h:163-177
+
+#include <algorithm>
+
+#include "pl_common.cuh"
+
+namespace pl {
+namespace {
+
+// ---------------------------------------------------------------------------
+// Outer product: out[i*n + j] = lhs[j] * rhs[i].  One CTA row per rhs term
+// (held in registers), lhs streamed with coalesced loads (it stays in L2),
+// output written with streaming stores -- the kernel is HBM-write bound.
+// ---------------------------------------------------------------------------
+template <int AS>
+__global__ void __launch_bounds__(256)
+    k_multiply(const u64* __restrict__ ax, const u64* __restrict__ az, const u8* __restrict__ af,
+               const double* __restrict__ av, u64 n, const u64* __restrict__ bx,
+               const u64* __restrict__ bz, const u8* __restrict__ bf,
+               const double* __restrict__ bv, u64 m, u64* __restrict__ ox, u64* __restrict__ oz,
+               u8* __restrict__ of, double* __restrict__ ov) {
+    const u64 total = n * m;
+    for (u64 i = blockIdx.y; i < m; i += gridDim.y) {
+        u64 rx[AS], rz[AS];
+#pragma unroll
+        for (int k = 0; k < AS; ++k) {
+            rx[k] = __ldg(bx + k * m + i);
+            rz[k] = __ldg(bz + k * m + i);
+        }
+        const u32 rf = __ldg(bf + i);
+        const double rv = __ldg(bv + i);
+        const u64 row = i * n;
+        for (u64 j = (u64)blockIdx.x * blockDim.x + threadIdx.x; j < n;
+             j += (u64)gridDim.x * blockDim.x) {
+            PhaseAcc acc;
+#pragma unroll
+            for (int k = 0; k < AS; ++k) {
+                const u64 lx = __ldg(ax + k * n + j), lz = __ldg(az + k * n + j);
+                __stcs(ox + k * total + row + j, lx ^ rx[k]);
+                __stcs(oz + k * total + row + j, lz ^ rz[k]);
+                acc.step(lx, lz, rx[k], rz[k]);
+            }
+            __stcs(of + row + j, (u8)acc.phase(__ldg(af + j), rf));
+            __stcs(ov + row + j, dmul(__ldg(av + j), rv));
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Commutator with deterministic emission order.
+// Pair p = i*m + j (i over lhs, j over rhs), the order of the single-threaded
+// CPU commutator_impl.  A tile is 8192 consecutive pairs; each warp tests 32
+// consecutive pairs per step (coalesced rhs loads, broadcast lhs loads),
+// records the anticommuting ones in shared memory in pair order, and a
+// decoupled look-back over tiles turns tile counts into output slots.
+// ---------------------------------------------------------------------------
+constexpr int kCThreads = 256;
+constexpr int kCItems = 32;
+constexpr int kCWarpSpan = kCItems * 32;
+constexpr u64 kCTile = (u64)kCThreads * kCItems;
+constexpr u64 kFlag64Agg = 1ull << 62;
+constexpr u64 kFlag64Pre = 2ull << 62;
+constexpr u64 kCount64Mask = (1ull << 62) - 1;
+
+__device__ __forceinline__ u64 lookback64(u64* lb, u32 tile, u64 cnt, u64 init, int* status) {
+    if (tile == 0) {
+        st_volatile64(lb, kFlag64Pre | ((init + cnt) & kCount64Mask));
+        return init;
+    }
+    st_volatile64(lb + tile, kFlag64Agg | cnt);
+    u64 excl = 0;
+    i64 t = (i64)tile - 1;
+    u32 spins = 0;
+    while (t >= 0) {
+        const u64 w = ld_volatile64(lb + t);
+        const u64 fl = w >> 62;
+        if (fl == 0) {
+            if (++spins > kSpinLimit) {
+                raise_status(status, PL_ERR_TIMEOUT);
+                break;
+            }
+            if (spins > 64) __nanosleep(64);
+            continue;
+        }
+        excl += w & kCount64Mask;
+        if (fl == 2) break;
+        --t;
+    }
+    st_volatile64(lb + tile, kFlag64Pre | ((excl + cnt) & kCount64Mask));
+    return excl;
+}
+
+template <int AS>
+__global__ void __launch_bounds__(kCThreads)
+    k_commutator(const u64* __restrict__ ax, const u64* __restrict__ az,
+                 const u8* __restrict__ af, const double* __restrict__ av, u64 n,
+                 const u64* __restrict__ bx, const u64* __restrict__ bz,
+                 const u8* __restrict__ bf, const double* __restrict__ bv, u64 m, int mul_i,
+                 u64* __restrict__ ox, u64* __restrict__ oz, u8* __restrict__ of,
+                 double* __restrict__ ov, i64 capacity, unsigned long long* d_count, u64 npairs,
+                 u64* lb, u32* tile_ctr, int* status) {
+    __shared__ u16 s_emit[kCThreads / 32][kCWarpSpan];
+    __shared__ u32 s_wcount[kCThreads / 32];
+    __shared__ u32 s_tile;
+    __shared__ u64 s_base;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    if (tid == 0) s_tile = atomicAdd(tile_ctr, 1u);
+    __syncthreads();
+    const u32 tile = s_tile;
+    const u64 wbase = (u64)tile * kCTile + (u64)warp * kCWarpSpan;
+    const u64 p0 = wbase + lane;
+    u64 i = p0 / m, j = p0 - (p0 / m) * m;
+    u32 cnt = 0;
+    for (int t = 0; t < kCItems; ++t) {
+        const u64 p = wbase + (u64)t * 32 + lane;
+        bool anti = false;
+        if (p < npairs) {
+            u64 par = 0;
+#pragma unroll
+            for (int k = 0; k < AS; ++k)
+                par ^= anti_word(__ldg(ax + k * n + i), __ldg(az + k * n + i),
+                                 __ldg(bx + k * m + j), __ldg(bz + k * m + j));
+            anti = (__popcll(par) & 1) != 0;
+        }
+        const u32 bal = __ballot_sync(0xffffffffu, anti);
+        if (anti) s_emit[warp][cnt + __popc(bal & lanemask_lt())] = (u16)(t * 32 + lane);
+        cnt += __popc(bal);
+        j += 32;
+        while (j >= m && i < n) {
+            j -= m;
+            ++i;
+        }
+    }
+    if (lane == 0) s_wcount[warp] = cnt;
+    __syncthreads();
+    if (tid == 0) {
+        u64 tot = 0;
+        for (int w = 0; w < kCThreads / 32; ++w) tot += s_wcount[w];
+        const u64 init = tile == 0 ? (u64)*d_count : 0ull;
+        s_base = lookback64(lb, tile, tot, init, status);
+        if (tile == gridDim.x - 1) *d_count = (unsigned long long)(s_base + tot);
+    }
+    __syncthreads();
+    u64 wpre = 0;
+    for (int w = 0; w < warp; ++w) wpre += s_wcount[w];
+    const u64 base = s_base + wpre;
+    for (u32 e = lane; e < cnt; e += 32) {
+        const u64 p = wbase + s_emit[warp][e];
+        const u64 ii = p / m, jj = p - ii * m;
+        const i64 slot = (i64)(base + e);
+        if (slot >= capacity) {
+            raise_status(status, PL_ERR_CAPACITY);
+            continue;
+        }
+        PhaseAcc acc;
+#pragma unroll
+        for (int k = 0; k < AS; ++k) {
+            const u64 lx = __ldg(ax + k * n + ii), lz = __ldg(az + k * n + ii);
+            const u64 rx = __ldg(bx + k * m + jj), rz = __ldg(bz + k * m + jj);
+            ox[(i64)k * capacity + slot] = lx ^ rx;
+            oz[(i64)k * capacity + slot] = lz ^ rz;
+            acc.step(lx, lz, rx, rz);
+        }
+        of[slot] = (u8)((acc.phase(__ldg(af + ii), __ldg(bf + jj)) + (u32)mul_i) & 3u);
+        ov[slot] = dmul(dmul(2.0, __ldg(av + ii)), __ldg(bv + jj));
+    }
+}
+
+// ---------------------------------------------------------------------------
+// apply_CNOT: flags ^= (xc & zt & (1 ^ xt ^ zc)) << 1; x_t ^= x_c; z_c ^= z_t.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(256) k_cnot(u64* x, u64* z, u8* f, u64 n, u64 stride, int wc,
+                                              u64 mc, int wt, u64 mt) {
+    for (u64 i = (u64)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+         i += (u64)gridDim.x * blockDim.x) {
+        u64* xc_p = x + (u64)wc * stride + i;
+        u64* zc_p = z + (u64)wc * stride + i;
+        u64* xt_p = x + (u64)wt * stride + i;
+        u64* zt_p = z + (u64)wt * stride + i;
+        const u64 xc = (*xc_p & mc) != 0, zc = (*zc_p & mc) != 0;
+        const u64 xt = (*xt_p & mt) != 0, zt = (*zt_p & mt) != 0;
+        f[i] ^= (u8)((xc & zt & (1ull ^ xt ^ zc)) << 1);
+        *xt_p ^= (0ull - xc) & mt;
+        *zc_p ^= (0ull - zt) & mc;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// zero_state_expectation: one CTA, each thread sums a strided subsequence
+// in order, then a fixed binary tree -- deterministic for a given n.
+// ---------------------------------------------------------------------------
+template <int AS>
+__global__ void __launch_bounds__(1024) k_zero_state(const u64* __restrict__ x,
+                                                     const u8* __restrict__ f,
+                                                     const double* __restrict__ v, u64 n,
+                                                     u64 stride, double* out) {
+    __shared__ double s[1024];
+    double acc = 0.0;
+    for (u64 i = threadIdx.x; i < n; i += blockDim.x) {
+        u64 any = 0;
+#pragma unroll
+        for (int k = 0; k < AS; ++k) any |= __ldg(x + k * stride + i);
+        const u32 fl = __ldg(f + i);
+        if (any == 0 && (fl & 1u) == 0) {
+            const double val = __ldg(v + i);
+            acc = dadd(acc, (fl & 2u) ? -val : val);
+        }
+    }
+    s[threadIdx.x] = acc;
+    __syncthreads();
+    for (int st = blockDim.x / 2; st > 0; st >>= 1) {
+        if ((int)threadIdx.x < st) s[threadIdx.x] = dadd(s[threadIdx.x], s[threadIdx.x + st]);
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) *out = s[0];
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// Host entry points (internal).
+// ---------------------------------------------------------------------------
+int multiply_impl(int as, const u64* ax, const u64* az, const u8* af, const double* av, i64 n,
+                  const u64* bx, const u64* bz, const u8* bf, const double* bv, i64 m, u64* ox,
+                  u64* oz, u8* of, double* ov, cudaStream_t st) {
+    if (as < 1 || as > kMaxAS || n < 0 || m < 0 || (n > 0 && m > (1ll << 40) / n))
+        return record_status(PL_ERR_INVALID_ARG, "multiply: bad array_size or size");
+    if (n == 0 || m == 0) return record_status(PL_OK, nullptr);
+    if (!ax || !az || !af || !av || !bx || !bz || !bf || !bv || !ox || !oz || !of || !ov)
+        return record_status(PL_ERR_INVALID_ARG, "multiply: null pointer");
+    const dim3 grid((unsigned)grid_for(n, 256, 2048), (unsigned)std::min<i64>(m, 65535));
+    PL_DISPATCH_AS(as, k_multiply<AS><<<grid, 256, 0, st>>>(ax, az, af, av, (u64)n, bx, bz, bf,
+                                                           bv, (u64)m, ox, oz, of, ov));
+    PL_CUDA_TRY(cudaGetLastError());
+    return record_status(PL_OK, nullptr);
+}
+
+// Scratch for the commutator's tile look-back: one u64 per 8192 pairs plus
+// a tile counter and a status word.
+size_t commutator_scratch_bytes(u64 npairs) {
+    const u64 tiles = (npairs + kCTile - 1) / kCTile;
+    return (size_t)tiles * 8 + 256;
+}
+
+int commutator_launch(int as, int mul_i, const u64* ax, const u64* az, const u8* af,
+                      const double* av, i64 n, const u64* bx, const u64* bz, const u8* bf,
+                      const double* bv, i64 m, u64* ox, u64* oz, u8* of, double* ov,
+                      i64 capacity, unsigned long long* d_count, void* scratch,
+                      int* d_status, cudaStream_t st) {
+    const u64 npairs = (u64)n * (u64)m;
+    const u64 tiles = (npairs + kCTile - 1) / kCTile;
+    unsigned char* s = (unsigned char*)scratch;
+    u64* lb = (u64*)(s + 256);
+    u32* tile_ctr = (u32*)s;
+    PL_CUDA_TRY(cudaMemsetAsync(scratch, 0, commutator_scratch_bytes(npairs), st));
+    PL_DISPATCH_AS(as, k_commutator<AS><<<(unsigned)tiles, kCThreads, 0, st>>>(
+                           ax, az, af, av, (u64)n, bx, bz, bf, bv, (u64)m, mul_i, ox, oz, of, ov,
+                           capacity, d_count, npairs, lb, tile_ctr, d_status));
+    PL_CUDA_TRY(cudaGetLastError());
+    return PL_OK;
+}
+
+int commutator_impl(int as, int mul_i, const u64* ax, const u64* az, const u8* af,
+                    const double* av, i64 n, const u64* bx, const u64* bz, const u8* bf,
+                    const double* bv, i64 m, u64* ox, u64* oz, u8* of, double* ov, i64 capacity,
+                    unsigned long long* d_count, cudaStream_t st) {
+    if (as < 1 || as > kMaxAS || n < 0 || m < 0 || capacity < 0 || !d_count ||
+        (n > 0 && m > (1ll << 40) / n))
+        return record_status(PL_ERR_INVALID_ARG, "commutator: bad array_size or size");
+    if (n == 0 || m == 0) return record_status(PL_OK, nullptr);
+    if (!ax || !az || !af || !av || !bx || !bz || !bf || !bv || !ox || !oz || !of || !ov)
+        return record_status(PL_ERR_INVALID_ARG, "commutator: null pointer");
+    // Stream-ordered scratch: safe when several streams call concurrently.
+    const size_t bytes = commutator_scratch_bytes((u64)n * (u64)m) + 256;
+    void* scratch = nullptr;
+    PL_CUDA_TRY(cudaMallocAsync(&scratch, bytes, st));
+    int* d_status = (int*)((unsigned char*)scratch + bytes - 256);
+    PL_CUDA_TRY(cudaMemsetAsync(d_status, 0, sizeof(int), st));
+    int rc = commutator_launch(as, mul_i, ax, az, af, av, n, bx, bz, bf, bv, m, ox, oz, of, ov,
+                               capacity, d_count, scratch, d_status, st);
+    int dstat = 0;
+    if (rc == PL_OK) {
+        // The capacity/timeout check needs the device status: read it back
+        // stream-ordered, then release the scratch.
+        cudaError_t e = cudaMemcpyAsync(&dstat, d_status, sizeof(int), cudaMemcpyDeviceToHost, st);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+        if (e != cudaSuccess) rc = record_cuda(e);
+    }
+    cudaFreeAsync(scratch, st);
+    if (rc != PL_OK) return rc;
+    if (dstat != 0) return record_status(dstat, "commutator: device-side check");
+    return record_status(PL_OK, nullptr);
+}
+
+}  // namespace pl
+
+// ---------------------------------------------------------------------------
+// C ABI
+// ---------------------------------------------------------------------------
+using namespace pl;
+
+extern "C" void launch_gpu_mul_soa(int array_size, const uint64_t* lhs_x, const uint64_t* lhs_z,
+                                   const uint8_t* lhs_flags, const double* lhs_val,
+                                   const uint64_t* rhs_x, const uint64_t* rhs_z,
+                                   const uint8_t* rhs_flags, const double* rhs_val,
+                                   uint64_t* out_x, uint64_t* out_z, uint8_t* out_flags,
+                                   double* out_val, int n, int m, cudaStream_t stream) {
+    multiply_impl(array_size, (const u64*)lhs_x, (const u64*)lhs_z, lhs_flags, lhs_val, n,
+                  (const u64*)rhs_x, (const u64*)rhs_z, rhs_flags, rhs_val, m, (u64*)out_x,
+                  (u64*)out_z, out_flags, out_val, stream);
+}
+
+extern "C" int pl_multiply(int array_size, const uint64_t* lhs_x, const uint64_t* lhs_z,
+                           const uint8_t* lhs_flags, const double* lhs_val, int64_t n,
+                           const uint64_t* rhs_x, const uint64_t* rhs_z,
+                           const uint8_t* rhs_flags, const double* rhs_val, int64_t m,
+                           uint64_t* out_x, uint64_t* out_z, uint8_t* out_flags, double* out_val,
+                           cudaStream_t stream) {
+    return multiply_impl(array_size, (const u64*)lhs_x, (const u64*)lhs_z, lhs_flags, lhs_val, n,
+                         (const u64*)rhs_x, (const u64*)rhs_z, rhs_flags, rhs_val, m,
+                         (u64*)out_x, (u64*)out_z, out_flags, out_val, stream);
+}
+
+extern "C" void launch_gpu_commutator_soa(int array_size, int multiply_by_i,
+                                          const uint64_t* lhs_x, const uint64_t* lhs_z,
+                                          const uint8_t* lhs_flags, const double* lhs_val,
+                                          const uint64_t* rhs_x, const uint64_t* rhs_z,
+                                          const uint8_t* rhs_flags, const double* rhs_val,
+                                          uint64_t* out_x, uint64_t* out_z, uint8_t* out_flags,
+                                          double* out_val, unsigned long long* d_count, int n,
+                                          int m, long long capacity, cudaStream_t stream) {
+    commutator_impl(array_size, multiply_by_i ? 1 : 0, (const u64*)lhs_x, (const u64*)lhs_z,
+                    lhs_flags, lhs_val, n, (const u64*)rhs_x, (const u64*)rhs_z, rhs_flags,
+                    rhs_val, m, (u64*)out_x, (u64*)out_z, out_flags, out_val, capacity, d_count,
+                    stream);
+}
+
+extern "C" int pl_commutator(int array_size, int multiply_by_i, const uint64_t* lhs_x,
+                             const uint64_t* lhs_z, const uint8_t* lhs_flags,
+                             const double* lhs_val, int64_t n, const uint64_t* rhs_x,
+                             const uint64_t* rhs_z, const uint8_t* rhs_flags,
+                             const double* rhs_val, int64_t m, uint64_t* out_x, uint64_t* out_z,
+                             uint8_t* out_flags, double* out_val, int64_t capacity,
+                             unsigned long long* d_count, cudaStream_t stream) {
+    return commutator_impl(array_size, multiply_by_i ? 1 : 0, (const u64*)lhs_x,
+                           (const u64*)lhs_z, lhs_flags, lhs_val, n, (const u64*)rhs_x,
+                           (const u64*)rhs_z, rhs_flags, rhs_val, m, (u64*)out_x, (u64*)out_z,
+                           out_flags, out_val, capacity, d_count, stream);
+}
+
+extern "C" int pl_apply_cnot(int array_size, uint64_t* x, uint64_t* z, uint8_t* flags, int64_t n,
+                             int64_t stride, int control, int target, cudaStream_t stream) {
+    if (array_size < 1 || array_size > kMaxAS || n < 0 || stride < n || control < 0 ||
+        target < 0 || control >= 64 * array_size || target >= 64 * array_size ||
+        control == target)
+        return record_status(PL_ERR_INVALID_ARG, "pl_apply_cnot: bad argument");
+    if (n == 0) return record_status(PL_OK, nullptr);
+    if (!x || !z || !flags) return record_status(PL_ERR_INVALID_ARG, "pl_apply_cnot: null");
+    k_cnot<<<grid_for(n, 256, sm_count() * 8), 256, 0, stream>>>(
+        (u64*)x, (u64*)z, flags, (u64)n, (u64)stride, control / 64, 1ull << (control % 64),
+        target / 64, 1ull << (target % 64));
+    PL_CUDA_TRY(cudaGetLastError());
+    return record_status(PL_OK, nullptr);
+}
+
+extern "C" int pl_zero_state_expectation(int array_size, const uint64_t* x, const uint8_t* flags,
+                                         const double* val, int64_t n, int64_t stride,
+                                         double* d_result, cudaStream_t stream) {
+    if (array_size < 1 || array_size > kMaxAS || n < 0 || stride < n || !d_result)
+        return record_status(PL_ERR_INVALID_ARG, "pl_zero_state_expectation: bad argument");
+    if (n > 0 && (!x || !flags || !val))
+        return record_status(PL_ERR_INVALID_ARG, "pl_zero_state_expectation: null");
+    PL_DISPATCH_AS(array_size, k_zero_state<AS><<<1, 1024, 0, stream>>>(
+                                   (const u64*)x, flags, val, (u64)n, (u64)stride, d_result));
+    PL_CUDA_TRY(cudaGetLastError());
+    return record_status(PL_OK, nullptr);
+}

@@ -1,0 +1,153 @@
+"""Device-resident Pauli sum and propagation through the C ABI (pl_state_*).
+
+Mirrors the reference's PauliSum methods that the propagation loop uses
+(evolve, canonicalize, sort_and_combine, cutoff, truncate_weight,
+apply_CNOT, zero_state_expectation; PauliSumOperations.h / PauliSumUtils.h)
+and the driver (propagate / propagate_expectation, PauliPropagation.h:54-71).
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import _abi
+
+U64_MAX = (1 << 64) - 1
+
+
+def _ptr(a: np.ndarray):
+    return a.ctypes.data_as(C.c_void_p) if a is not None and a.size else None
+
+
+def truncation(max_weight=None, cutoff=0.0, max_terms=None) -> _abi.Truncation:
+    return _abi.Truncation(U64_MAX if max_weight is None else int(max_weight),
+                           float(cutoff or 0.0), U64_MAX if max_terms is None else int(max_terms))
+
+
+class State:
+    """A Pauli sum kept on the GPU between gates (``pl_state``)."""
+
+    def __init__(self, array_size: int, capacity_hint: int = 1 << 16, stream=None):
+        self.array_size = int(array_size)
+        self._lib = _abi.lib()
+        h = C.c_void_p()
+        s = stream if stream is not None else _default_stream()
+        _abi.check(self._lib.pl_state_create(C.byref(h), self.array_size, int(capacity_hint), s),
+                   "pl_state_create")
+        self._h = h
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._lib.pl_state_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    # -- data ------------------------------------------------------------
+    def upload(self, x, z, flags, val):
+        x = np.ascontiguousarray(x, np.uint64).reshape(self.array_size, -1)
+        z = np.ascontiguousarray(z, np.uint64).reshape(self.array_size, -1)
+        f = np.ascontiguousarray(flags, np.uint8)
+        v = np.ascontiguousarray(val, np.float64)
+        _abi.check(self._lib.pl_state_upload(self._h, _ptr(x), _ptr(z), _ptr(f), _ptr(v),
+                                             v.shape[0]), "pl_state_upload")
+        return self
+
+    def size(self) -> int:
+        n = C.c_int64()
+        _abi.check(self._lib.pl_state_size(self._h, C.byref(n)), "pl_state_size")
+        return n.value
+
+    def download(self):
+        n = self.size()
+        x = np.zeros((self.array_size, n), np.uint64)
+        z = np.zeros((self.array_size, n), np.uint64)
+        f = np.zeros(n, np.uint8)
+        v = np.zeros(n, np.float64)
+        got = C.c_int64()
+        if n:
+            _abi.check(self._lib.pl_state_download(self._h, _ptr(x), _ptr(z), _ptr(f), _ptr(v),
+                                                   n, C.byref(got)), "pl_state_download")
+        return x, z, f, v
+
+    # -- operations --------------------------------------------------------
+    def evolve(self, rx, rz, rf, theta):
+        rx = np.ascontiguousarray(rx, np.uint64).reshape(self.array_size, -1)
+        rz = np.ascontiguousarray(rz, np.uint64).reshape(self.array_size, -1)
+        rf = np.ascontiguousarray(rf, np.uint8)
+        th = np.ascontiguousarray(theta, np.float64)
+        _abi.check(self._lib.pl_state_evolve(self._h, _ptr(rx), _ptr(rz), _ptr(rf), _ptr(th),
+                                             th.shape[0]), "pl_state_evolve")
+
+    def apply_truncation(self, max_weight=None, cutoff=0.0, max_terms=None):
+        t = truncation(max_weight, cutoff, max_terms)
+        _abi.check(self._lib.pl_state_apply_truncation(self._h, C.byref(t)),
+                   "pl_state_apply_truncation")
+
+    def canonicalize(self):
+        _abi.check(self._lib.pl_state_canonicalize(self._h), "pl_state_canonicalize")
+
+    def sort_and_combine(self):
+        _abi.check(self._lib.pl_state_sort_and_combine(self._h), "pl_state_sort_and_combine")
+
+    def cutoff(self, eps):
+        _abi.check(self._lib.pl_state_cutoff(self._h, float(eps)), "pl_state_cutoff")
+
+    def truncate_weight(self, w):
+        _abi.check(self._lib.pl_state_truncate_weight(self._h, int(w)), "pl_state_truncate_weight")
+
+    def apply_cnot(self, c, t):
+        _abi.check(self._lib.pl_state_apply_cnot(self._h, int(c), int(t)), "pl_state_apply_cnot")
+
+    def zero_state_expectation(self) -> float:
+        r = C.c_double()
+        _abi.check(self._lib.pl_state_zero_state_expectation(self._h, C.byref(r)),
+                   "pl_state_zero_state_expectation")
+        return r.value
+
+    def propagate(self, rx, rz, rf, theta, ops=None, max_weight=None, cutoff=0.0,
+                  max_terms=None):
+        rx = np.ascontiguousarray(rx, np.uint64).reshape(self.array_size, -1)
+        rz = np.ascontiguousarray(rz, np.uint64).reshape(self.array_size, -1)
+        rf = np.ascontiguousarray(rf, np.uint8)
+        th = np.ascontiguousarray(theta, np.float64)
+        t = truncation(max_weight, cutoff, max_terms)
+        if ops is None:
+            o, n_ops = None, 0
+        else:
+            o = np.ascontiguousarray(ops, np.int32).reshape(-1, 3)
+            n_ops = o.shape[0]
+        _abi.check(self._lib.pl_propagate(self._h, _ptr(rx), _ptr(rz), _ptr(rf), _ptr(th),
+                                          th.shape[0], _ptr(o) if o is not None else None, n_ops,
+                                          C.byref(t)), "pl_propagate")
+
+
+def _default_stream():
+    try:
+        import torch
+        if torch.cuda.is_available():
+            return int(torch.cuda.current_stream().cuda_stream)
+    except Exception:
+        pass
+    return None
+
+
+def propagate_expectation_planes(obs, circ, max_weight=None, cutoff=0.0, max_terms=None,
+                                 capacity_hint: int = 1 << 16) -> float:
+    """<0|U^dagger O U|0> for a workloads.Circuit (rotations + CNOTs)."""
+    with State(obs.x.shape[0], capacity_hint) as st:
+        st.upload(obs.x, obs.z, obs.flags, obs.val)
+        r = circ.rotations
+        st.propagate(r.x, r.z, r.flags, r.val, circ.ops, max_weight, cutoff, max_terms)
+        return st.zero_state_expectation()
