@@ -207,12 +207,37 @@ PL_API int pl_state_truncate_weight(pl_state* state, uint64_t max_weight);
 PL_API int pl_state_apply_cnot(pl_state* state, int control, int target);
 PL_API int pl_state_zero_state_expectation(pl_state* state, double* result);
 
+/* lhs := lhs * rhs, the outer product in the reference's i*n + j order
+ * (PauliSum::multiply, PauliSumOperations.h:256-306).  lhs and rhs may be
+ * the same state. */
+PL_API int pl_state_multiply(pl_state* lhs, pl_state* rhs);
+/* lhs := canonicalize(lhs * rhs) without materialising the products
+ * (`a *= b; a.canonicalize()`). */
+PL_API int pl_state_multiply_canonicalize(pl_state* lhs, pl_state* rhs);
+/* out := [a, b] (multiply_by_i = 0) or i[a, b] (= 1), uncombined, in the
+ * reference's single-threaded CPU order (commutator / i_commutator,
+ * PauliSumOperations.h:316-356). */
+PL_API int pl_state_commutator(pl_state* out, pl_state* a, pl_state* b, int multiply_by_i);
+
 /* propagate (PauliPropagation.h:54-63): ops walked in reverse; a rotation
  * is evolve + apply_truncation, a CNOT is apply_CNOT.  ops == NULL means
  * "every rotation in order", the reference's rotation-only circuit. */
 PL_API int pl_propagate(pl_state* state, const uint64_t* rot_x, const uint64_t* rot_z,
                  const uint8_t* rot_flags, const double* rot_theta, int64_t n_rot,
                  const int32_t* ops, int64_t n_ops, const pl_truncation* opts);
+
+/* ---- measurement hooks ------------------------------------------------ */
+
+/* Reset the library's counters.  With enable_timing != 0, every onesweep
+ * digit pass of the collate engine is bracketed by CUDA events recorded on
+ * its launching stream. */
+PL_API int pl_profile_reset(int enable_timing);
+/* Kernel launches issued by the library since the last reset, and (when
+ * timing) the number, total device time and algorithmic bytes (read +
+ * write of keys and payloads) of the timed digit passes.  Synchronises the
+ * streams the timed passes ran on. */
+PL_API int pl_profile_read(uint64_t* launches, uint64_t* timed_launches, double* timed_ms,
+                           uint64_t* timed_bytes);
 
 #ifdef __cplusplus
 }

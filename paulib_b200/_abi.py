@@ -40,6 +40,8 @@ EXPORTS = (
     "pl_state_size", "pl_state_evolve", "pl_state_apply_truncation", "pl_state_canonicalize",
     "pl_state_sort_and_combine", "pl_state_cutoff", "pl_state_truncate_weight",
     "pl_state_apply_cnot", "pl_state_zero_state_expectation", "pl_propagate",
+    "pl_profile_reset", "pl_profile_read", "pl_state_multiply",
+    "pl_state_multiply_canonicalize", "pl_state_commutator",
 )
 
 
@@ -106,6 +108,12 @@ def lib():
         "pl_state_apply_cnot": (I32, [VP, I32, I32]),
         "pl_state_zero_state_expectation": (I32, [VP, C.POINTER(C.c_double)]),
         "pl_propagate": (I32, [VP, VP, VP, VP, VP, I64, VP, I64, C.POINTER(Truncation)]),
+        "pl_profile_reset": (I32, [I32]),
+        "pl_state_multiply": (I32, [VP, VP]),
+        "pl_state_multiply_canonicalize": (I32, [VP, VP]),
+        "pl_state_commutator": (I32, [VP, VP, VP, I32]),
+        "pl_profile_read": (I32, [C.POINTER(C.c_uint64), C.POINTER(C.c_uint64),
+                                  C.POINTER(C.c_double), C.POINTER(C.c_uint64)]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name, None)
@@ -183,3 +191,16 @@ def stream_ptr(stream=None) -> int:
 def workspace(nbytes: int, device="cuda"):
     torch = _torch()
     return torch.empty(max(int(nbytes), 256), dtype=torch.uint8, device=device)
+
+
+def profile_reset(timing: bool = False):
+    check(lib().pl_profile_reset(int(bool(timing))), "pl_profile_reset")
+
+
+def profile_read():
+    """(launches, timed_launches, timed_ms, timed_bytes) since the last reset."""
+    a, b, d = C.c_uint64(), C.c_uint64(), C.c_uint64()
+    ms = C.c_double()
+    check(lib().pl_profile_read(C.byref(a), C.byref(b), C.byref(ms), C.byref(d)),
+          "pl_profile_read")
+    return a.value, b.value, ms.value, d.value

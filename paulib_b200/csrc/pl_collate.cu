@@ -131,6 +131,7 @@ struct ProdSrc {
     const u8 *af, *bf;
     const double *av, *bv;
     u32 n, m;
+    i64 sa, sb;  // plane strides of the operands
     __device__ __forceinline__ void split(u32 p, u32& i, u32& j) const {
         i = p / n;
         j = p - i * n;
@@ -141,8 +142,8 @@ struct ProdSrc {
         PhaseAcc acc;
 #pragma unroll
         for (int k = 0; k < AS; ++k) {
-            const u64 a_x = __ldg(ax + (i64)k * n + j), a_z = __ldg(az + (i64)k * n + j);
-            const u64 b_x = __ldg(bx + (i64)k * m + i), b_z = __ldg(bz + (i64)k * m + i);
+            const u64 a_x = __ldg(ax + (i64)k * sa + j), a_z = __ldg(az + (i64)k * sa + j);
+            const u64 b_x = __ldg(bx + (i64)k * sb + i), b_z = __ldg(bz + (i64)k * sb + i);
             xw[k] = a_x ^ b_x;
             zw[k] = a_z ^ b_z;
             acc.step(a_x, a_z, b_x, b_z);
@@ -763,7 +764,7 @@ int run_collate(const Src& src, u32 n, int mode, const KeyLayout& L, const PassP
     PL_CUDA_TRY(cudaMemsetAsync(B.d_status, 0, sizeof(int), st));
     PL_CUDA_TRY(cudaMemsetAsync(B.d_count, 0, sizeof(i64), st));
     const int gblocks = grid_for(n, 256, nsm * 8);
-    k_pack<AS, Src><<<gblocks, 256, 0, st>>>(src, n, mode, L, P, B.ka, B.pa, B.planes, B.hist);
+    k_pack<AS, Src><<<gblocks, 256, 0, st>>>(src, n, mode, L, P, B.ka, B.pa, B.planes, B.hist), pl::note_launch();
     u64 *kin = B.ka, *kout = B.kb;
     u32 *vin = B.pa, *vout = B.pb;
     for (int c = 0; c < L.nchunks; ++c) {
@@ -771,13 +772,24 @@ int run_collate(const Src& src, u32 n, int mode, const KeyLayout& L, const PassP
         if (np == 0) continue;
         if (c > 0)
             k_gather_chunk<<<gblocks, 256, 0, st>>>(B.planes + (size_t)c * n, vin, n, P, c, kin,
-                                                    B.hist, B.d_status);
-        k_scan_buckets<<<np, kRadix, 0, st>>>(B.hist, p0);
+                                                    B.hist, B.d_status), pl::note_launch();
+        k_scan_buckets<<<np, kRadix, 0, st>>>(B.hist, p0), pl::note_launch();
         for (int p = p0; p < p0 + np; ++p) {
             PL_CUDA_TRY(cudaMemsetAsync(B.lb, 0, sizeof(u32) * (size_t)tiles * kRadix, st));
+            cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+            if (timing_enabled()) {
+                PL_CUDA_TRY(cudaEventCreate(&ev0));
+                PL_CUDA_TRY(cudaEventCreate(&ev1));
+                PL_CUDA_TRY(cudaEventRecord(ev0, st));
+            }
             k_radix_pass<<<tiles, kThreads, kRadixDynSmem, st>>>(
                 kin, vin, kout, vout, n, P.shift[p], P.bits[p], B.hist + (size_t)p * kRadix, B.lb,
-                B.counters + 8 + p, B.d_status);
+                B.counters + 8 + p, B.d_status), pl::note_launch();
+            if (ev1) {
+                PL_CUDA_TRY(cudaEventRecord(ev1, st));
+                // algorithmic bytes: read and write one u64 key + one u32 payload per term
+                timed_push(ev0, ev1, 24ull * n);
+            }
             std::swap(kin, kout);
             std::swap(vin, vout);
         }
@@ -785,14 +797,14 @@ int run_collate(const Src& src, u32 n, int mode, const KeyLayout& L, const PassP
     PL_CUDA_TRY(cudaMemsetAsync(B.lb_seg, 0, sizeof(u32) * tiles, st));
     SegCtx C{kin, vin, B.planes, n, L.nchunks, L.seg_mask0, mode};
     k_segments<Src><<<tiles, kThreads, 0, st>>>(src, C, B.seg_start, B.seg_sum, B.long_list,
-                                                B.counters, B.lb_seg, B.d_status);
+                                                B.counters, B.lb_seg, B.d_status), pl::note_launch();
     k_long_segments<Src><<<nsm * 4, kThreads, 0, st>>>(src, vin, B.seg_start, B.long_list,
-                                                       B.counters, mode, B.seg_sum);
+                                                       B.counters, mode, B.seg_sum), pl::note_launch();
     // Emit over the segment count; the grid covers the worst case (n).
     PL_CUDA_TRY(cudaMemsetAsync(B.lb_emit, 0, sizeof(u32) * tiles, st));
     k_emit<AS, Src><<<tiles, kThreads, 0, st>>>(src, vin, B.seg_start, B.seg_sum, B.counters,
                                                 B.lb_emit, mode, a.cutoff, a.max_weight, out,
-                                                B.d_count, B.d_status);
+                                                B.d_count, B.d_status), pl::note_launch();
     PL_CUDA_TRY(cudaGetLastError());
     i64 cnt = 0;
     int dstat = 0;
@@ -848,7 +860,7 @@ int collate_soa(int as, const SoAView& in, const SoAOut& out, const CollateArgs&
         PL_CUDA_TRY(cudaMemcpyAsync(B.andm, init_and.data(), 8 * kMaxFields,
                                     cudaMemcpyHostToDevice, st));
         k_masks<AS><<<grid_for(n, 256, sm_count() * 4), 256, 0, st>>>(src, n, a.mode, B.orm,
-                                                                     B.andm);
+                                                                     B.andm), pl::note_launch();
         u64 hor[kMaxFields], hand[kMaxFields];
         PL_CUDA_TRY(cudaMemcpyAsync(hor, B.orm, 8 * kMaxFields, cudaMemcpyDeviceToHost, st));
         PL_CUDA_TRY(cudaMemcpyAsync(hand, B.andm, 8 * kMaxFields, cudaMemcpyDeviceToHost, st));
@@ -890,13 +902,13 @@ int multiply_collate(int as, const SoAView& lhs, const SoAView& rhs, const SoAOu
         u64 hor[2][kMaxFields], hand[2][kMaxFields];
         const SoAView* ops[2] = {&lhs, &rhs};
         for (int w = 0; w < 2; ++w) {
-            SoASrc<AS> s{ops[w]->x, ops[w]->z, ops[w]->f, ops[w]->v, ops[w]->n};
+            SoASrc<AS> s{ops[w]->x, ops[w]->z, ops[w]->f, ops[w]->v, ops[w]->stride};
             PL_CUDA_TRY(cudaMemcpyAsync(B.orm, init_or.data(), 8 * kMaxFields,
                                         cudaMemcpyHostToDevice, st));
             PL_CUDA_TRY(cudaMemcpyAsync(B.andm, init_and.data(), 8 * kMaxFields,
                                         cudaMemcpyHostToDevice, st));
             k_masks<AS><<<grid_for(ops[w]->n, 256, sm_count() * 4), 256, 0, st>>>(
-                s, (u32)ops[w]->n, a.mode, B.orm, B.andm);
+                s, (u32)ops[w]->n, a.mode, B.orm, B.andm), pl::note_launch();
             PL_CUDA_TRY(cudaMemcpyAsync(hor[w], B.orm, 8 * kMaxFields, cudaMemcpyDeviceToHost, st));
             PL_CUDA_TRY(
                 cudaMemcpyAsync(hand[w], B.andm, 8 * kMaxFields, cudaMemcpyDeviceToHost, st));
@@ -912,8 +924,8 @@ int multiply_collate(int as, const SoAView& lhs, const SoAView& rhs, const SoAOu
         KeyLayout L;
         PassPlan P;
         build_layout(AS, a.mode, por, pand, L, P);
-        ProdSrc<AS> src{lhs.x, lhs.z, rhs.x, rhs.z, lhs.f, rhs.f, lhs.v, rhs.v, (u32)lhs.n,
-                        (u32)rhs.n};
+        ProdSrc<AS> src{lhs.x, lhs.z, rhs.x,    rhs.z,      lhs.f,     rhs.f,
+                        lhs.v, rhs.v, (u32)lhs.n, (u32)rhs.n, lhs.stride, rhs.stride};
         rc = run_collate<AS>(src, n, a.mode, L, P, a, out, out_count, B, st);
     });
     return rc;

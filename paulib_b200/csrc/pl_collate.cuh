@@ -59,4 +59,13 @@ int multiply_collate(int as, const SoAView& lhs, const SoAView& rhs, const SoAOu
                      const CollateArgs& a, i64* out_count, void* ws, size_t ws_bytes,
                      cudaStream_t stream);
 
+// Outer product and commutator launchers (pl_terms.cu); s* are plane strides.
+int multiply_impl(int as, const u64* ax, const u64* az, const u8* af, const double* av, i64 n,
+                  i64 sa, const u64* bx, const u64* bz, const u8* bf, const double* bv, i64 m,
+                  i64 sb, u64* ox, u64* oz, u8* of, double* ov, i64 so, cudaStream_t st);
+int commutator_impl(int as, int mul_i, const u64* ax, const u64* az, const u8* af,
+                    const double* av, i64 n, i64 sa, const u64* bx, const u64* bz, const u8* bf,
+                    const double* bv, i64 m, i64 sb, u64* ox, u64* oz, u8* of, double* ov,
+                    i64 capacity, unsigned long long* d_count, cudaStream_t st);
+
 }  // namespace pl

@@ -119,4 +119,8 @@ int sm_count();
 namespace pl {
 int record_cuda(cudaError_t e);
 int record_status(int code, const char* what);
+// Measurement hooks (pl_profile_*): launch counter and event-timed passes.
+void note_launch();
+bool timing_enabled();
+void timed_push(cudaEvent_t start, cudaEvent_t stop, unsigned long long bytes);
 }  // namespace pl

@@ -1119,20 +1119,20 @@ int fast_rotation(pl_state* s, const GateP<AS>& g, int mode, double c, double sn
     constexpr int T = ptile<AS>();
     k_expand<AS><<<grid_persistent(4), kPT, 0, s->st>>>(
         s->S[in], s->d_size + in, g, mode, -sn, s->R0, s->R1, s->d_k, s->lbA, s->ctr + 0,
-        s->d_status, s->cap, gate_index, s->d_fail);
+        s->d_status, s->cap, gate_index, s->d_fail), pl::note_launch();
     const int pgrid = std::max(1, (int)((s->max_tiles + 255) / 256));
     k_partition<AS><<<pgrid, 256, 0, s->st>>>(s->R0, s->d_k, s->R1, s->d_k + 1, nullptr, T, 0,
-                                              s->spB_lo, s->spB_hi, s->max_tiles, s->d_status);
+                                              s->spB_lo, s->spB_hi, s->max_tiles, s->d_status), pl::note_launch();
     k_merge_runs<AS><<<grid_persistent(2), kPT, tile_smem_bytes<AS>(T), s->st>>>(
-        s->R0, s->R1, s->d_k, s->spB_lo, s->spB_hi, s->N, s->ctr + 1, s->d_status);
+        s->R0, s->R1, s->d_k, s->spB_lo, s->spB_hi, s->N, s->ctr + 1, s->d_status), pl::note_launch();
     k_partition<AS><<<pgrid, 256, 0, s->st>>>(s->S[in], s->d_size + in, s->N, s->d_k, s->d_k + 1,
                                               T, 1, s->spC_lo, s->spC_hi, s->max_tiles,
-                                              s->d_status);
+                                              s->d_status), pl::note_launch();
     const u64 mw = tr.max_weight;
     const double cut = tr.coefficient_cutoff > 0.0 ? tr.coefficient_cutoff : 0.0;
     k_merge_reduce<AS><<<grid_persistent(2), kPT, tile_smem_bytes<AS>(T + 2), s->st>>>(
         s->S[in], s->d_size + in, s->N, s->d_k, s->spC_lo, s->spC_hi, g, mode, c, s->S[outb],
-        s->d_size + outb, mw, cut, s->lbC, s->ctr + 2, s->d_status, gate_index, s->d_fail);
+        s->d_size + outb, mw, cut, s->lbC, s->ctr + 2, s->d_status, gate_index, s->d_fail), pl::note_launch();
     PL_CUDA_TRY(cudaGetLastError());
     s->cur = outb;
     return PL_OK;
@@ -1152,11 +1152,11 @@ int general_rotation(pl_state* s, const Rot& r, bool truncate, const pl_truncati
     const int grid = grid_for(n, 256, sm_count() * 8);
     if (mode == kNegate) {
         k_negate<AS><<<grid, 256, 0, s->st>>>(s->S[s->cur], s->d_size + s->cur, g, 0,
-                                              s->d_status);
+                                              s->d_status), pl::note_launch();
         if (s->cls == 2) s->cls = 1;
     } else if (mode == kHalfPos || mode == kHalfNeg) {
         k_halfpi_inplace<AS><<<grid, 256, 0, s->st>>>(s->S[s->cur], s->d_size + s->cur, g,
-                                                      mode == kHalfPos, s->d_status);
+                                                      mode == kHalfPos, s->d_status), pl::note_launch();
         if (s->cls == 2) s->cls = 1;
     } else if (mode == kGeneral) {
         // old + children can need up to 2n slots
@@ -1167,7 +1167,7 @@ int general_rotation(pl_state* s, const Rot& r, bool truncate, const pl_truncati
         PL_CUDA_TRY(cudaMemsetAsync(s->lbA, 0, s->zero_bytes, s->st));
         const int other = 1 - s->cur;
         k_materialize<AS><<<grid_persistent(4), kPT, 0, s->st>>>(
-            s->S[s->cur], n, g, c, -sn, s->S[other], s->d_tmp, s->lbA, s->ctr + 0, s->d_status);
+            s->S[s->cur], n, g, c, -sn, s->S[other], s->d_tmp, s->lbA, s->ctr + 0, s->d_status), pl::note_launch();
         i64 total = 0;
         PL_CUDA_TRY(cudaMemcpyAsync(&total, s->d_tmp, sizeof(i64), cudaMemcpyDeviceToHost, s->st));
         int st[2];
@@ -1278,7 +1278,7 @@ int run_ops(pl_state* s, const std::vector<Rot>& rots, const std::vector<Op>& op
             in_buf[i] = s->cur;
             k_cnot_state<AS><<<grid_persistent(8), 256, 0, s->st>>>(
                 s->S[s->cur], s->d_size + s->cur, op.a / 64, 1ull << (op.a % 64), op.b / 64,
-                1ull << (op.b % 64), s->d_status);
+                1ull << (op.b % 64), s->d_status), pl::note_launch();
             pending = true;
             ++i;
             ++since_sync;
@@ -1297,7 +1297,7 @@ int run_ops(pl_state* s, const std::vector<Rot>& rots, const std::vector<Op>& op
                 in_buf[i] = s->cur;
                 if (modes[r] == kNegate) {
                     k_negate<AS><<<grid_persistent(8), 256, 0, s->st>>>(
-                        s->S[s->cur], s->d_size + s->cur, gates[r], 1, s->d_status);
+                        s->S[s->cur], s->d_size + s->cur, gates[r], 1, s->d_status), pl::note_launch();
                 } else if (modes[r] != kSkip) {
                     rc = fast_rotation<AS>(s, gates[r], modes[r], cs[r], sns[r], tr, (int)i);
                     if (rc) return rc;
@@ -1503,7 +1503,7 @@ static int filter_state(pl_state* s, double eps, uint64_t max_weight) {
     PL_CUDA_TRY(cudaMemsetAsync(s->lbA, 0, s->zero_bytes, s->st));
     PL_DISPATCH_AS(s->as, k_filter<AS><<<grid_persistent(4), kPT, 0, s->st>>>(
                               s->S[s->cur], n, s->S[other], eps, max_weight, s->d_size + other,
-                              s->lbC, s->ctr + 3, s->d_status));
+                              s->lbC, s->ctr + 3, s->d_status), pl::note_launch());
     PL_CUDA_TRY(cudaGetLastError());
     if (n == 0) {
         i64 z = 0;
@@ -1534,7 +1534,7 @@ extern "C" int pl_state_apply_cnot(pl_state* s, int control, int target) {
     PL_DISPATCH_AS(s->as, k_cnot_state<AS><<<grid_persistent(8), 256, 0, s->st>>>(
                               s->S[s->cur], s->d_size + s->cur, control / 64,
                               1ull << (control % 64), target / 64, 1ull << (target % 64),
-                              s->d_status));
+                              s->d_status), pl::note_launch());
     PL_CUDA_TRY(cudaGetLastError());
     if (s->cls == 2) s->cls = 1;
     return record_status(PL_OK, nullptr);
@@ -1593,4 +1593,118 @@ extern "C" int pl_propagate(pl_state* s, const uint64_t* rot_x, const uint64_t* 
     if (rc) return rc;
     if (st) return record_status(st, "pl_propagate");
     return record_status(PL_OK, nullptr);
+}
+
+// ---------------------------------------------------------------------------
+// Algebra on device-resident states.
+// ---------------------------------------------------------------------------
+extern "C" int pl_state_multiply(pl_state* lhs, pl_state* rhs) {
+    int rc = check_state(lhs);
+    if (rc) return rc;
+    rc = check_state(rhs);
+    if (rc) return rc;
+    if (lhs->as != rhs->as) return record_status(PL_ERR_INVALID_ARG, "pl_state_multiply: AS");
+    i64 n = 0, m = 0;
+    rc = read_size(lhs, &n);
+    if (rc) return rc;
+    rc = read_size(rhs, &m);
+    if (rc) return rc;
+    if (n > 0 && m > ((1ll << 30) - 1) / n)
+        return record_status(PL_ERR_INVALID_ARG, "pl_state_multiply: n*m must be < 2^30");
+    if (rhs->st != lhs->st) PL_CUDA_TRY(cudaStreamSynchronize(rhs->st));
+    if (n * m > lhs->cap) {
+        rc = state_grow(lhs, n * m);
+        if (rc) return rc;
+    }
+    const Buf& a = lhs->S[lhs->cur];
+    const Buf& b = rhs->S[rhs->cur];
+    const int other = 1 - lhs->cur;
+    const Buf& o = lhs->S[other];
+    rc = multiply_impl(lhs->as, a.x, a.z, a.f, a.v, n, a.cap, b.x, b.z, b.f, b.v, m, b.cap, o.x,
+                       o.z, o.f, o.v, o.cap, lhs->st);
+    if (rc) return rc;
+    const i64 nm = n * m;
+    PL_CUDA_TRY(cudaMemcpyAsync(lhs->d_size + other, &nm, sizeof(i64), cudaMemcpyHostToDevice,
+                                lhs->st));
+    PL_CUDA_TRY(cudaStreamSynchronize(lhs->st));
+    lhs->cur = other;
+    lhs->cls = 0;
+    return record_status(PL_OK, nullptr);
+}
+
+extern "C" int pl_state_multiply_canonicalize(pl_state* lhs, pl_state* rhs) {
+    int rc = check_state(lhs);
+    if (rc) return rc;
+    rc = check_state(rhs);
+    if (rc) return rc;
+    if (lhs->as != rhs->as)
+        return record_status(PL_ERR_INVALID_ARG, "pl_state_multiply_canonicalize: AS");
+    i64 n = 0, m = 0;
+    rc = read_size(lhs, &n);
+    if (rc) return rc;
+    rc = read_size(rhs, &m);
+    if (rc) return rc;
+    if (rhs->st != lhs->st) PL_CUDA_TRY(cudaStreamSynchronize(rhs->st));
+    rc = lhs->ws.ensure(multiply_collate_ws_bytes(lhs->as, n, m));
+    if (rc) return rc;
+    for (int attempt = 0; attempt < 2; ++attempt) {
+        const Buf& a = lhs->S[lhs->cur];
+        const Buf& b = rhs->S[rhs->cur];
+        const int other = 1 - lhs->cur;
+        CollateArgs args;
+        args.mode = kCanon;
+        i64 cnt = 0;
+        rc = multiply_collate(lhs->as, view_of(a, n), view_of(b, m), out_of(lhs->S[other]), args,
+                              &cnt, lhs->ws.ptr, lhs->ws.bytes, lhs->st);
+        if (rc == PL_ERR_CAPACITY && attempt == 0) {
+            rc = state_grow(lhs, cnt);
+            if (rc) return rc;
+            continue;
+        }
+        if (rc) return rc;
+        PL_CUDA_TRY(cudaMemcpyAsync(lhs->d_size + other, &cnt, sizeof(i64),
+                                    cudaMemcpyHostToDevice, lhs->st));
+        PL_CUDA_TRY(cudaStreamSynchronize(lhs->st));
+        lhs->cur = other;
+        lhs->cls = 2;
+        return record_status(PL_OK, nullptr);
+    }
+    return record_status(PL_ERR_INTERNAL, "pl_state_multiply_canonicalize");
+}
+
+extern "C" int pl_state_commutator(pl_state* out, pl_state* a, pl_state* b, int multiply_by_i) {
+    int rc = check_state(out);
+    if (rc) return rc;
+    if ((rc = check_state(a)) || (rc = check_state(b))) return rc;
+    if (out == a || out == b || a->as != b->as || out->as != a->as)
+        return record_status(PL_ERR_INVALID_ARG, "pl_state_commutator: operands");
+    i64 n = 0, m = 0;
+    if ((rc = read_size(a, &n)) || (rc = read_size(b, &m))) return rc;
+    if (a->st != out->st) PL_CUDA_TRY(cudaStreamSynchronize(a->st));
+    if (b->st != out->st) PL_CUDA_TRY(cudaStreamSynchronize(b->st));
+    for (int attempt = 0; attempt < 2; ++attempt) {
+        const Buf& A = a->S[a->cur];
+        const Buf& B = b->S[b->cur];
+        Buf& O = out->S[out->cur];
+        PL_CUDA_TRY(cudaMemsetAsync(out->d_tmp, 0, sizeof(i64), out->st));
+        rc = commutator_impl(out->as, multiply_by_i ? 1 : 0, A.x, A.z, A.f, A.v, n, A.cap, B.x,
+                             B.z, B.f, B.v, m, B.cap, O.x, O.z, O.f, O.v, O.cap,
+                             (unsigned long long*)out->d_tmp, out->st);
+        i64 cnt = 0;
+        PL_CUDA_TRY(cudaMemcpyAsync(&cnt, out->d_tmp, sizeof(i64), cudaMemcpyDeviceToHost,
+                                    out->st));
+        PL_CUDA_TRY(cudaStreamSynchronize(out->st));
+        if (rc == PL_ERR_CAPACITY && attempt == 0) {
+            rc = state_grow(out, cnt);
+            if (rc) return rc;
+            continue;
+        }
+        if (rc) return rc;
+        PL_CUDA_TRY(cudaMemcpyAsync(out->d_size + out->cur, &cnt, sizeof(i64),
+                                    cudaMemcpyHostToDevice, out->st));
+        PL_CUDA_TRY(cudaStreamSynchronize(out->st));
+        out->cls = 0;
+        return record_status(PL_OK, nullptr);
+    }
+    return record_status(PL_ERR_INTERNAL, "pl_state_commutator");
 }

@@ -6,6 +6,7 @@
 // code; the most recent status and a message are kept per host thread so
 // the void drop-ins can be checked with pl_get_last_error().
 
+#include <atomic>
 #include <cstdio>
 #include <mutex>
 #include <string>
@@ -17,6 +18,15 @@
 namespace {
 thread_local int g_last_status = PL_OK;
 thread_local std::string g_last_msg;
+
+std::atomic<unsigned long long> g_launches{0};
+std::atomic<bool> g_timing{false};
+struct Timed {
+    cudaEvent_t start, stop;
+    unsigned long long bytes;
+};
+std::mutex g_timed_mu;
+std::vector<Timed> g_timed;
 }  // namespace
 
 namespace pl {
@@ -37,6 +47,13 @@ int record_cuda(cudaError_t e) {
     g_last_status = e == cudaErrorMemoryAllocation ? PL_ERR_OOM : PL_ERR_CUDA;
     g_last_msg = std::string("CUDA: ") + (s ? s : "unknown error");
     return g_last_status;
+}
+
+void note_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
+bool timing_enabled() { return g_timing.load(std::memory_order_relaxed); }
+void timed_push(cudaEvent_t start, cudaEvent_t stop, unsigned long long bytes) {
+    std::lock_guard<std::mutex> lock(g_timed_mu);
+    g_timed.push_back(Timed{start, stop, bytes});
 }
 
 int sm_count() {
@@ -74,3 +91,41 @@ extern "C" const char* pl_status_string(int status) {
 extern "C" int pl_get_last_error(void) { return g_last_status; }
 extern "C" const char* pl_last_error_message(void) { return g_last_msg.c_str(); }
 extern "C" int pl_version(void) { return 1; }
+
+extern "C" int pl_profile_reset(int enable_timing) {
+    {
+        std::lock_guard<std::mutex> lock(g_timed_mu);
+        for (auto& t : g_timed) {
+            cudaEventSynchronize(t.stop);
+            cudaEventDestroy(t.start);
+            cudaEventDestroy(t.stop);
+        }
+        g_timed.clear();
+    }
+    g_launches.store(0);
+    g_timing.store(enable_timing != 0);
+    return pl::record_status(PL_OK, nullptr);
+}
+
+extern "C" int pl_profile_read(uint64_t* launches, uint64_t* timed_launches, double* timed_ms,
+                               uint64_t* timed_bytes) {
+    double ms = 0.0;
+    unsigned long long bytes = 0, count = 0;
+    {
+        std::lock_guard<std::mutex> lock(g_timed_mu);
+        for (auto& t : g_timed) {
+            float e = 0.f;
+            if (cudaEventSynchronize(t.stop) != cudaSuccess ||
+                cudaEventElapsedTime(&e, t.start, t.stop) != cudaSuccess)
+                return pl::record_cuda(cudaGetLastError());
+            ms += e;
+            bytes += t.bytes;
+            ++count;
+        }
+    }
+    if (launches) *launches = g_launches.load();
+    if (timed_launches) *timed_launches = count;
+    if (timed_ms) *timed_ms = ms;
+    if (timed_bytes) *timed_bytes = bytes;
+    return pl::record_status(PL_OK, nullptr);
+}

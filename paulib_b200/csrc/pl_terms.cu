@@ -23,17 +23,16 @@ namespace {
 template <int AS>
 __global__ void __launch_bounds__(256)
     k_multiply(const u64* __restrict__ ax, const u64* __restrict__ az, const u8* __restrict__ af,
-               const double* __restrict__ av, u64 n, const u64* __restrict__ bx,
+               const double* __restrict__ av, u64 n, u64 sa, const u64* __restrict__ bx,
                const u64* __restrict__ bz, const u8* __restrict__ bf,
-               const double* __restrict__ bv, u64 m, u64* __restrict__ ox, u64* __restrict__ oz,
-               u8* __restrict__ of, double* __restrict__ ov) {
-    const u64 total = n * m;
+               const double* __restrict__ bv, u64 m, u64 sb, u64* __restrict__ ox,
+               u64* __restrict__ oz, u8* __restrict__ of, double* __restrict__ ov, u64 so) {
     for (u64 i = blockIdx.y; i < m; i += gridDim.y) {
         u64 rx[AS], rz[AS];
 #pragma unroll
         for (int k = 0; k < AS; ++k) {
-            rx[k] = __ldg(bx + k * m + i);
-            rz[k] = __ldg(bz + k * m + i);
+            rx[k] = __ldg(bx + k * sb + i);
+            rz[k] = __ldg(bz + k * sb + i);
         }
         const u32 rf = __ldg(bf + i);
         const double rv = __ldg(bv + i);
@@ -43,9 +42,9 @@ __global__ void __launch_bounds__(256)
             PhaseAcc acc;
 #pragma unroll
             for (int k = 0; k < AS; ++k) {
-                const u64 lx = __ldg(ax + k * n + j), lz = __ldg(az + k * n + j);
-                __stcs(ox + k * total + row + j, lx ^ rx[k]);
-                __stcs(oz + k * total + row + j, lz ^ rz[k]);
+                const u64 lx = __ldg(ax + k * sa + j), lz = __ldg(az + k * sa + j);
+                __stcs(ox + k * so + row + j, lx ^ rx[k]);
+                __stcs(oz + k * so + row + j, lz ^ rz[k]);
                 acc.step(lx, lz, rx[k], rz[k]);
             }
             __stcs(of + row + j, (u8)acc.phase(__ldg(af + j), rf));
@@ -101,9 +100,10 @@ __device__ __forceinline__ u64 lookback64(u64* lb, u32 tile, u64 cnt, u64 init, 
 template <int AS>
 __global__ void __launch_bounds__(kCThreads)
     k_commutator(const u64* __restrict__ ax, const u64* __restrict__ az,
-                 const u8* __restrict__ af, const double* __restrict__ av, u64 n,
+                 const u8* __restrict__ af, const double* __restrict__ av, u64 n, u64 sa,
                  const u64* __restrict__ bx, const u64* __restrict__ bz,
-                 const u8* __restrict__ bf, const double* __restrict__ bv, u64 m, int mul_i,
+                 const u8* __restrict__ bf, const double* __restrict__ bv, u64 m, u64 sb,
+                 int mul_i,
                  u64* __restrict__ ox, u64* __restrict__ oz, u8* __restrict__ of,
                  double* __restrict__ ov, i64 capacity, unsigned long long* d_count, u64 npairs,
                  u64* lb, u32* tile_ctr, int* status) {
@@ -126,8 +126,8 @@ __global__ void __launch_bounds__(kCThreads)
             u64 par = 0;
 #pragma unroll
             for (int k = 0; k < AS; ++k)
-                par ^= anti_word(__ldg(ax + k * n + i), __ldg(az + k * n + i),
-                                 __ldg(bx + k * m + j), __ldg(bz + k * m + j));
+                par ^= anti_word(__ldg(ax + k * sa + i), __ldg(az + k * sa + i),
+                                 __ldg(bx + k * sb + j), __ldg(bz + k * sb + j));
             anti = (__popcll(par) & 1) != 0;
         }
         const u32 bal = __ballot_sync(0xffffffffu, anti);
@@ -163,8 +163,8 @@ __global__ void __launch_bounds__(kCThreads)
         PhaseAcc acc;
 #pragma unroll
         for (int k = 0; k < AS; ++k) {
-            const u64 lx = __ldg(ax + k * n + ii), lz = __ldg(az + k * n + ii);
-            const u64 rx = __ldg(bx + k * m + jj), rz = __ldg(bz + k * m + jj);
+            const u64 lx = __ldg(ax + k * sa + ii), lz = __ldg(az + k * sa + ii);
+            const u64 rx = __ldg(bx + k * sb + jj), rz = __ldg(bz + k * sb + jj);
             ox[(i64)k * capacity + slot] = lx ^ rx;
             oz[(i64)k * capacity + slot] = lz ^ rz;
             acc.step(lx, lz, rx, rz);
@@ -229,16 +229,17 @@ __global__ void __launch_bounds__(1024) k_zero_state(const u64* __restrict__ x,
 // Host entry points (internal).
 // ---------------------------------------------------------------------------
 int multiply_impl(int as, const u64* ax, const u64* az, const u8* af, const double* av, i64 n,
-                  const u64* bx, const u64* bz, const u8* bf, const double* bv, i64 m, u64* ox,
-                  u64* oz, u8* of, double* ov, cudaStream_t st) {
+                  i64 sa, const u64* bx, const u64* bz, const u8* bf, const double* bv, i64 m,
+                  i64 sb, u64* ox, u64* oz, u8* of, double* ov, i64 so, cudaStream_t st) {
     if (as < 1 || as > kMaxAS || n < 0 || m < 0 || (n > 0 && m > (1ll << 40) / n))
         return record_status(PL_ERR_INVALID_ARG, "multiply: bad array_size or size");
     if (n == 0 || m == 0) return record_status(PL_OK, nullptr);
     if (!ax || !az || !af || !av || !bx || !bz || !bf || !bv || !ox || !oz || !of || !ov)
         return record_status(PL_ERR_INVALID_ARG, "multiply: null pointer");
     const dim3 grid((unsigned)grid_for(n, 256, 2048), (unsigned)std::min<i64>(m, 65535));
-    PL_DISPATCH_AS(as, k_multiply<AS><<<grid, 256, 0, st>>>(ax, az, af, av, (u64)n, bx, bz, bf,
-                                                           bv, (u64)m, ox, oz, of, ov));
+    PL_DISPATCH_AS(as, k_multiply<AS><<<grid, 256, 0, st>>>(ax, az, af, av, (u64)n, (u64)sa, bx,
+                                                           bz, bf, bv, (u64)m, (u64)sb, ox, oz,
+                                                           of, ov, (u64)so), pl::note_launch());
     PL_CUDA_TRY(cudaGetLastError());
     return record_status(PL_OK, nullptr);
 }
@@ -251,9 +252,9 @@ size_t commutator_scratch_bytes(u64 npairs) {
 }
 
 int commutator_launch(int as, int mul_i, const u64* ax, const u64* az, const u8* af,
-                      const double* av, i64 n, const u64* bx, const u64* bz, const u8* bf,
-                      const double* bv, i64 m, u64* ox, u64* oz, u8* of, double* ov,
-                      i64 capacity, unsigned long long* d_count, void* scratch,
+                      const double* av, i64 n, i64 sa, const u64* bx, const u64* bz,
+                      const u8* bf, const double* bv, i64 m, i64 sb, u64* ox, u64* oz, u8* of,
+                      double* ov, i64 capacity, unsigned long long* d_count, void* scratch,
                       int* d_status, cudaStream_t st) {
     const u64 npairs = (u64)n * (u64)m;
     const u64 tiles = (npairs + kCTile - 1) / kCTile;
@@ -262,16 +263,17 @@ int commutator_launch(int as, int mul_i, const u64* ax, const u64* az, const u8*
     u32* tile_ctr = (u32*)s;
     PL_CUDA_TRY(cudaMemsetAsync(scratch, 0, commutator_scratch_bytes(npairs), st));
     PL_DISPATCH_AS(as, k_commutator<AS><<<(unsigned)tiles, kCThreads, 0, st>>>(
-                           ax, az, af, av, (u64)n, bx, bz, bf, bv, (u64)m, mul_i, ox, oz, of, ov,
-                           capacity, d_count, npairs, lb, tile_ctr, d_status));
+                           ax, az, af, av, (u64)n, (u64)sa, bx, bz, bf, bv, (u64)m, (u64)sb,
+                           mul_i, ox, oz, of, ov, capacity, d_count, npairs, lb, tile_ctr,
+                           d_status), pl::note_launch());
     PL_CUDA_TRY(cudaGetLastError());
     return PL_OK;
 }
 
 int commutator_impl(int as, int mul_i, const u64* ax, const u64* az, const u8* af,
-                    const double* av, i64 n, const u64* bx, const u64* bz, const u8* bf,
-                    const double* bv, i64 m, u64* ox, u64* oz, u8* of, double* ov, i64 capacity,
-                    unsigned long long* d_count, cudaStream_t st) {
+                    const double* av, i64 n, i64 sa, const u64* bx, const u64* bz, const u8* bf,
+                    const double* bv, i64 m, i64 sb, u64* ox, u64* oz, u8* of, double* ov,
+                    i64 capacity, unsigned long long* d_count, cudaStream_t st) {
     if (as < 1 || as > kMaxAS || n < 0 || m < 0 || capacity < 0 || !d_count ||
         (n > 0 && m > (1ll << 40) / n))
         return record_status(PL_ERR_INVALID_ARG, "commutator: bad array_size or size");
@@ -284,8 +286,8 @@ int commutator_impl(int as, int mul_i, const u64* ax, const u64* az, const u8* a
     PL_CUDA_TRY(cudaMallocAsync(&scratch, bytes, st));
     int* d_status = (int*)((unsigned char*)scratch + bytes - 256);
     PL_CUDA_TRY(cudaMemsetAsync(d_status, 0, sizeof(int), st));
-    int rc = commutator_launch(as, mul_i, ax, az, af, av, n, bx, bz, bf, bv, m, ox, oz, of, ov,
-                               capacity, d_count, scratch, d_status, st);
+    int rc = commutator_launch(as, mul_i, ax, az, af, av, n, sa, bx, bz, bf, bv, m, sb, ox, oz,
+                               of, ov, capacity, d_count, scratch, d_status, st);
     int dstat = 0;
     if (rc == PL_OK) {
         // The capacity/timeout check needs the device status: read it back
@@ -313,9 +315,9 @@ extern "C" void launch_gpu_mul_soa(int array_size, const uint64_t* lhs_x, const 
                                    const uint8_t* rhs_flags, const double* rhs_val,
                                    uint64_t* out_x, uint64_t* out_z, uint8_t* out_flags,
                                    double* out_val, int n, int m, cudaStream_t stream) {
-    multiply_impl(array_size, (const u64*)lhs_x, (const u64*)lhs_z, lhs_flags, lhs_val, n,
-                  (const u64*)rhs_x, (const u64*)rhs_z, rhs_flags, rhs_val, m, (u64*)out_x,
-                  (u64*)out_z, out_flags, out_val, stream);
+    multiply_impl(array_size, (const u64*)lhs_x, (const u64*)lhs_z, lhs_flags, lhs_val, n, n,
+                  (const u64*)rhs_x, (const u64*)rhs_z, rhs_flags, rhs_val, m, m, (u64*)out_x,
+                  (u64*)out_z, out_flags, out_val, (i64)n * m, stream);
 }
 
 extern "C" int pl_multiply(int array_size, const uint64_t* lhs_x, const uint64_t* lhs_z,
@@ -325,8 +327,8 @@ extern "C" int pl_multiply(int array_size, const uint64_t* lhs_x, const uint64_t
                            uint64_t* out_x, uint64_t* out_z, uint8_t* out_flags, double* out_val,
                            cudaStream_t stream) {
     return multiply_impl(array_size, (const u64*)lhs_x, (const u64*)lhs_z, lhs_flags, lhs_val, n,
-                         (const u64*)rhs_x, (const u64*)rhs_z, rhs_flags, rhs_val, m,
-                         (u64*)out_x, (u64*)out_z, out_flags, out_val, stream);
+                         n, (const u64*)rhs_x, (const u64*)rhs_z, rhs_flags, rhs_val, m, m,
+                         (u64*)out_x, (u64*)out_z, out_flags, out_val, n * m, stream);
 }
 
 extern "C" void launch_gpu_commutator_soa(int array_size, int multiply_by_i,
@@ -338,9 +340,9 @@ extern "C" void launch_gpu_commutator_soa(int array_size, int multiply_by_i,
                                           double* out_val, unsigned long long* d_count, int n,
                                           int m, long long capacity, cudaStream_t stream) {
     commutator_impl(array_size, multiply_by_i ? 1 : 0, (const u64*)lhs_x, (const u64*)lhs_z,
-                    lhs_flags, lhs_val, n, (const u64*)rhs_x, (const u64*)rhs_z, rhs_flags,
-                    rhs_val, m, (u64*)out_x, (u64*)out_z, out_flags, out_val, capacity, d_count,
-                    stream);
+                    lhs_flags, lhs_val, n, n, (const u64*)rhs_x, (const u64*)rhs_z, rhs_flags,
+                    rhs_val, m, m, (u64*)out_x, (u64*)out_z, out_flags, out_val, capacity,
+                    d_count, stream);
 }
 
 extern "C" int pl_commutator(int array_size, int multiply_by_i, const uint64_t* lhs_x,
@@ -351,9 +353,9 @@ extern "C" int pl_commutator(int array_size, int multiply_by_i, const uint64_t* 
                              uint8_t* out_flags, double* out_val, int64_t capacity,
                              unsigned long long* d_count, cudaStream_t stream) {
     return commutator_impl(array_size, multiply_by_i ? 1 : 0, (const u64*)lhs_x,
-                           (const u64*)lhs_z, lhs_flags, lhs_val, n, (const u64*)rhs_x,
-                           (const u64*)rhs_z, rhs_flags, rhs_val, m, (u64*)out_x, (u64*)out_z,
-                           out_flags, out_val, capacity, d_count, stream);
+                           (const u64*)lhs_z, lhs_flags, lhs_val, n, n, (const u64*)rhs_x,
+                           (const u64*)rhs_z, rhs_flags, rhs_val, m, m, (u64*)out_x,
+                           (u64*)out_z, out_flags, out_val, capacity, d_count, stream);
 }
 
 extern "C" int pl_apply_cnot(int array_size, uint64_t* x, uint64_t* z, uint8_t* flags, int64_t n,
@@ -366,7 +368,7 @@ extern "C" int pl_apply_cnot(int array_size, uint64_t* x, uint64_t* z, uint8_t* 
     if (!x || !z || !flags) return record_status(PL_ERR_INVALID_ARG, "pl_apply_cnot: null");
     k_cnot<<<grid_for(n, 256, sm_count() * 8), 256, 0, stream>>>(
         (u64*)x, (u64*)z, flags, (u64)n, (u64)stride, control / 64, 1ull << (control % 64),
-        target / 64, 1ull << (target % 64));
+        target / 64, 1ull << (target % 64)), pl::note_launch();
     PL_CUDA_TRY(cudaGetLastError());
     return record_status(PL_OK, nullptr);
 }
@@ -379,7 +381,7 @@ extern "C" int pl_zero_state_expectation(int array_size, const uint64_t* x, cons
     if (n > 0 && (!x || !flags || !val))
         return record_status(PL_ERR_INVALID_ARG, "pl_zero_state_expectation: null");
     PL_DISPATCH_AS(array_size, k_zero_state<AS><<<1, 1024, 0, stream>>>(
-                                   (const u64*)x, flags, val, (u64)n, (u64)stride, d_result));
+                                   (const u64*)x, flags, val, (u64)n, (u64)stride, d_result), pl::note_launch());
     PL_CUDA_TRY(cudaGetLastError());
     return record_status(PL_OK, nullptr);
 }
