@@ -220,6 +220,8 @@ def run_product_collate(args, rank, local, ws):
         torch.cuda.synchronize()
     barrier(ws)
     launches, timed_n, timed_ms, timed_bytes = _abi.profile_read()
+    kernels = {k: {"launches": c, "ms_per_step": t / args.steps}
+               for k, (c, t, _) in _abi.profile_report().items()}
     _abi.profile_reset(timing=False)
     step_ms = [e0.elapsed_time(e1) for e0, e1 in evs]
     t_ms = max_over_ranks(sum(step_ms), ws)
@@ -308,6 +310,7 @@ def run_product_collate(args, rank, local, ws):
         "pipeline_roofline": {"bytes_model": "B_canon(n_in, n_out, b=41)",
                               "bytes_per_step": pipe_bytes, "achieved": pipe_gbs,
                               "peak": peak, "frac": pipe_gbs / peak, "unit": "GB/s"},
+        "kernels": kernels,
         "clocks": clk.summary(),
     }
     if ws == 1 and rank == 0 and not args.no_cpu_baseline:

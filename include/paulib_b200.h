@@ -228,9 +228,9 @@ PL_API int pl_propagate(pl_state* state, const uint64_t* rot_x, const uint64_t* 
 
 /* ---- measurement hooks ------------------------------------------------ */
 
-/* Reset the library's counters.  With enable_timing != 0, every onesweep
- * digit pass of the collate engine is bracketed by CUDA events recorded on
- * its launching stream. */
+/* Reset the library's counters.  With enable_timing != 0, every kernel of
+ * the collate engine is bracketed by CUDA events recorded on its launching
+ * stream (the onesweep digit passes are also summed by pl_profile_read). */
 PL_API int pl_profile_reset(int enable_timing);
 /* Kernel launches issued by the library since the last reset, and (when
  * timing) the number, total device time and algorithmic bytes (read +
@@ -238,6 +238,9 @@ PL_API int pl_profile_reset(int enable_timing);
  * streams the timed passes ran on. */
 PL_API int pl_profile_read(uint64_t* launches, uint64_t* timed_launches, double* timed_ms,
                            uint64_t* timed_bytes);
+/* Per-kernel totals of every timed launch, one "name count total_ms bytes"
+ * line per kernel, into buf (NUL-terminated). */
+PL_API int pl_profile_report(char* buf, size_t cap);
 
 #ifdef __cplusplus
 }

@@ -41,7 +41,7 @@ EXPORTS = (
     "pl_state_sort_and_combine", "pl_state_cutoff", "pl_state_truncate_weight",
     "pl_state_apply_cnot", "pl_state_zero_state_expectation", "pl_propagate",
     "pl_profile_reset", "pl_profile_read", "pl_state_multiply",
-    "pl_state_multiply_canonicalize", "pl_state_commutator",
+    "pl_state_multiply_canonicalize", "pl_state_commutator", "pl_profile_report",
 )
 
 
@@ -109,6 +109,7 @@ def lib():
         "pl_state_zero_state_expectation": (I32, [VP, C.POINTER(C.c_double)]),
         "pl_propagate": (I32, [VP, VP, VP, VP, VP, I64, VP, I64, C.POINTER(Truncation)]),
         "pl_profile_reset": (I32, [I32]),
+        "pl_profile_report": (I32, [C.c_char_p, C.c_size_t]),
         "pl_state_multiply": (I32, [VP, VP]),
         "pl_state_multiply_canonicalize": (I32, [VP, VP]),
         "pl_state_commutator": (I32, [VP, VP, VP, I32]),
@@ -204,3 +205,14 @@ def profile_read():
     check(lib().pl_profile_read(C.byref(a), C.byref(b), C.byref(ms), C.byref(d)),
           "pl_profile_read")
     return a.value, b.value, ms.value, d.value
+
+
+def profile_report() -> dict:
+    """{kernel name: (launches, total_ms, bytes)} of the timed launches."""
+    buf = C.create_string_buffer(1 << 16)
+    check(lib().pl_profile_report(buf, len(buf)), "pl_profile_report")
+    out = {}
+    for ln in buf.value.decode().splitlines():
+        name, cnt, ms, nbytes = ln.split()
+        out[name] = (int(cnt), float(ms), int(nbytes))
+    return out

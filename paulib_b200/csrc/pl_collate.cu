@@ -41,7 +41,9 @@ namespace {
 
 constexpr int kThreads = 256;
 constexpr int kItems = 16;
-constexpr int kTile = kThreads * kItems;  // 4096 keys per tile
+constexpr int kTile = kThreads * kItems;    // 4096 terms per segment / emit tile
+constexpr int kRItems = 8;
+constexpr int kRTile = kThreads * kRItems;  // 2048 keys per radix tile
 constexpr int kRadix = 256;
 constexpr int kWarps = kThreads / 32;
 constexpr u32 kIdxMask = 0x7fffffffu;
@@ -65,6 +67,7 @@ struct KeyLayout {
     int total_bits;
     int nchunks;
     u64 seg_mask0;  // chunk-0 mask for segment equality (drops the sign bit in kProp)
+    u64 cbits[kMaxFields];  // values of the bits that do not vary
 };
 
 struct PassPlan {
@@ -102,6 +105,33 @@ __device__ __forceinline__ u64 pack_chunk(const KeyLayout& L, const u64* xw, con
     return r;
 }
 
+// Inverse of pack_chunk for single-chunk layouts: the full key of a term
+// from its packed key and the constant bits.
+template <int AS>
+__device__ __forceinline__ void unpack_key(const KeyLayout& L, u64 packed, u64* xw, u64* zw,
+                                           u32& fv) {
+#pragma unroll
+    for (int f = 0; f < 2 * AS + 1; ++f) {
+        const int w = L.width[f];
+        u64 word = L.cbits[f];
+        if (w) {
+            const u64 m = w >= 64 ? ~0ull : ((1ull << w) - 1ull);
+            const u64 v = (packed >> L.off[f]) & m;
+            word = (word & ~(m << L.lo[f])) | (v << L.lo[f]);
+        }
+        if (f < AS) xw[f] = word;
+        else if (f < 2 * AS) zw[f - AS] = word;
+        else fv = (u32)word;
+    }
+}
+
+// Output flags byte from the flags key field.
+__device__ __forceinline__ u32 out_flags(u32 fv, int mode) {
+    if (mode == kCombine) return fv & 3u;
+    if (mode == kCanon) return fv & 1u;
+    return (fv >> 1) & 1u;  // kProp: field is phase << 1 | sign
+}
+
 // ---------------------------------------------------------------------------
 // Term sources: where keys and values of the (virtual) input come from.
 // ---------------------------------------------------------------------------
@@ -123,6 +153,27 @@ struct SoASrc {
     __device__ __forceinline__ double value(u32 i) const { return __ldg(v + i); }
 };
 
+// Division by a loop-invariant u32 d via a 32-bit magic multiplier
+// (round-up method): q = (t + ((p - t) >> 1)) >> s with t = umulhi(p, m).
+struct FastDiv {
+    u32 d, m, s;
+    static FastDiv make(u32 d) {
+        FastDiv f{d, 0, 0};
+        if (d > 1) {
+            int l = 0;
+            while ((1ull << l) < d) ++l;
+            f.m = (u32)((((unsigned __int128)1 << 32) * ((1ull << l) - d)) / d + 1);
+            f.s = (u32)(l - 1);
+        }
+        return f;
+    }
+    __device__ __forceinline__ u32 div(u32 p) const {
+        if (d == 1) return p;
+        const u32 t = __umulhi(p, m);
+        return (t + ((p - t) >> 1)) >> s;
+    }
+};
+
 // Products of the outer product PauliSum::multiply (PauliSumOperations.h:
 // 256-306): index p = i*n + j is lhs[j] * rhs[i], value lhs_j * rhs_i.
 template <int AS>
@@ -132,8 +183,9 @@ struct ProdSrc {
     const double *av, *bv;
     u32 n, m;
     i64 sa, sb;  // plane strides of the operands
+    FastDiv dn;  // division by n
     __device__ __forceinline__ void split(u32 p, u32& i, u32& j) const {
-        i = p / n;
+        i = dn.div(p);
         j = p - i * n;
     }
     __device__ __forceinline__ void key(u32 p, u64* xw, u64* zw, u32& fl) const {
@@ -199,8 +251,53 @@ __global__ void __launch_bounds__(256) k_masks(SoASrc<AS> src, u32 n, int mode, 
 // ---------------------------------------------------------------------------
 template <int AS, class Src>
 __global__ void __launch_bounds__(256) k_pack(Src src, u32 n, int mode, KeyLayout L,
-                                              PassPlan P, u64* keys, u32* pay, u64* planes,
-                                              u32* hist) {
+                                              PassPlan P, u32 count_mask, u64* keys, u32* pay,
+                                              u64* planes, u32* hist) {
+    __shared__ u32 sh[8 * kRadix];
+    const int np0 = P.first[1] - P.first[0];
+    for (int i = threadIdx.x; i < np0 * kRadix; i += blockDim.x) sh[i] = 0;
+    __syncthreads();
+    const int lane = threadIdx.x & 31;
+    const u32 wstride = gridDim.x * blockDim.x;
+    for (u32 w0 = (blockIdx.x * blockDim.x + threadIdx.x) & ~31u; w0 < n; w0 += wstride) {
+        const u32 i = w0 + lane;
+        const bool valid = i < n;
+        u64 k0 = 0;
+        if (valid) {
+            u64 xw[AS], zw[AS];
+            u32 fl;
+            src.key(i, xw, zw, fl);
+            const u32 fv = flags_field(fl, mode);
+            k0 = pack_chunk<AS>(L, xw, zw, fv, 0);
+            keys[i] = k0;
+            const u32 sign = (mode == kCombine) ? 0u : ((fl >> 1) & 1u);
+            pay[i] = i | (sign << 31);
+            if (L.nchunks > 1) {
+                planes[i] = k0;
+                for (int c = 1; c < L.nchunks; ++c)
+                    planes[(i64)c * n + i] = pack_chunk<AS>(L, xw, zw, fv, c);
+            }
+        }
+        for (int p = 0; p < np0; ++p) {
+            if (!((count_mask >> p) & 1u)) continue;
+            const u32 d = valid ? ((u32)(k0 >> P.shift[p]) & ((1u << P.bits[p]) - 1u)) : kSentinel;
+            const u32 peers = __match_any_sync(0xffffffffu, d);
+            if (valid && lane == __ffs(peers) - 1) atomicAdd(&sh[p * kRadix + d], __popc(peers));
+        }
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < np0 * kRadix; i += blockDim.x)
+        if (sh[i]) atomicAdd(&hist[i], sh[i]);
+}
+
+// Digit histograms of the operands of a product.  For a digit made only of
+// x / z bits, the product's digit is the XOR of the operands' digits
+// (x = ax ^ bx, z = az ^ bz), so the histogram over all n*m products is the
+// XOR-convolution of the two operand histograms; only digits that include
+// the phase bit must be counted product by product.
+template <int AS>
+__global__ void __launch_bounds__(256) k_operand_hist(SoASrc<AS> src, u32 n, KeyLayout L,
+                                                      PassPlan P, u32 conv_mask, u32* h) {
     __shared__ u32 sh[8 * kRadix];
     const int np0 = P.first[1] - P.first[0];
     for (int i = threadIdx.x; i < np0 * kRadix; i += blockDim.x) sh[i] = 0;
@@ -209,24 +306,28 @@ __global__ void __launch_bounds__(256) k_pack(Src src, u32 n, int mode, KeyLayou
         u64 xw[AS], zw[AS];
         u32 fl;
         src.key(i, xw, zw, fl);
-        const u32 fv = flags_field(fl, mode);
-        const u64 k0 = pack_chunk<AS>(L, xw, zw, fv, 0);
-        keys[i] = k0;
-        const u32 sign = (mode == kCombine) ? 0u : ((fl >> 1) & 1u);
-        pay[i] = i | (sign << 31);
-        if (L.nchunks > 1) {
-            planes[i] = k0;
-            for (int c = 1; c < L.nchunks; ++c)
-                planes[(i64)c * n + i] = pack_chunk<AS>(L, xw, zw, fv, c);
-        }
-        for (int p = 0; p < np0; ++p) {
-            const u32 d = (u32)(k0 >> P.shift[p]) & ((1u << P.bits[p]) - 1u);
-            atomicAdd(&sh[p * kRadix + d], 1u);
-        }
+        const u64 k0 = pack_chunk<AS>(L, xw, zw, 0u, 0);
+        for (int p = 0; p < np0; ++p)
+            if ((conv_mask >> p) & 1u)
+                atomicAdd(&sh[p * kRadix + ((u32)(k0 >> P.shift[p]) & ((1u << P.bits[p]) - 1u))],
+                          1u);
     }
     __syncthreads();
     for (int i = threadIdx.x; i < np0 * kRadix; i += blockDim.x)
-        if (sh[i]) atomicAdd(&hist[i], sh[i]);
+        if (sh[i]) atomicAdd(&h[i], sh[i]);
+}
+
+// hist[p][d] = sum_{d1} hA[p][d1] * hB[p][d1 ^ d] for every pass p in conv_mask.
+__global__ void __launch_bounds__(256) k_xor_conv(const u32* hA, const u32* hB, PassPlan P,
+                                                  u32 conv_mask, u32* hist) {
+    const int p = blockIdx.x;
+    if (!((conv_mask >> p) & 1u)) return;
+    const u32 R = 1u << P.bits[p];
+    const u32 d = threadIdx.x;
+    if (d >= R) return;
+    u32 acc = 0;
+    for (u32 d1 = 0; d1 < R; ++d1) acc += hA[p * kRadix + d1] * hB[p * kRadix + (d1 ^ d)];
+    hist[p * kRadix + d] = acc;
 }
 
 // Chunk c >= 1: bring chunk c of every term into the current order and
@@ -239,17 +340,27 @@ __global__ void __launch_bounds__(256) k_gather_chunk(const u64* __restrict__ pl
     const int p0 = P.first[c], np = P.first[c + 1] - P.first[c];
     for (int i = threadIdx.x; i < np * kRadix; i += blockDim.x) sh[i] = 0;
     __syncthreads();
-    for (u32 i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        const u32 src = pay[i] & kIdxMask;
-        if (src >= n) {
-            raise_status(status, PL_ERR_INTERNAL);
-            continue;
+    const int lane = threadIdx.x & 31;
+    const u32 wstride = gridDim.x * blockDim.x;
+    for (u32 w0 = (blockIdx.x * blockDim.x + threadIdx.x) & ~31u; w0 < n; w0 += wstride) {
+        const u32 i = w0 + lane;
+        bool valid = i < n;
+        u64 k = 0;
+        if (valid) {
+            const u32 src = pay[i] & kIdxMask;
+            if (src >= n) {
+                raise_status(status, PL_ERR_INTERNAL);
+                valid = false;
+            } else {
+                k = __ldg(planes_c + src);
+                keys[i] = k;
+            }
         }
-        const u64 k = __ldg(planes_c + src);
-        keys[i] = k;
         for (int p = 0; p < np; ++p) {
-            const u32 d = (u32)(k >> P.shift[p0 + p]) & ((1u << P.bits[p0 + p]) - 1u);
-            atomicAdd(&sh[p * kRadix + d], 1u);
+            const u32 d = valid ? ((u32)(k >> P.shift[p0 + p]) & ((1u << P.bits[p0 + p]) - 1u))
+                                : kSentinel;
+            const u32 peers = __match_any_sync(0xffffffffu, d);
+            if (valid && lane == __ffs(peers) - 1) atomicAdd(&sh[p * kRadix + d], __popc(peers));
         }
     }
     __syncthreads();
@@ -297,8 +408,9 @@ __device__ __forceinline__ u32 block_excl_scan(u32 v, u32* s_warp, u32& total) {
 }
 
 // Decoupled look-back over per-tile counters (status | count words).
-// Publishes this tile's aggregate, walks predecessors, publishes the
-// inclusive prefix and returns the exclusive prefix.  Bounded.
+// Publishes this tile's aggregate, walks predecessors four at a time (one
+// round trip per window), publishes the inclusive prefix and returns the
+// exclusive prefix.  Bounded.
 __device__ __forceinline__ u32 lookback(u32* lb, u32 tile, u32 stride, u32 cnt, int* status) {
     if (tile == 0) {
         st_volatile(lb, kFlagPre | cnt);
@@ -310,19 +422,30 @@ __device__ __forceinline__ u32 lookback(u32* lb, u32 tile, u32 stride, u32 cnt, 
     i64 t = (i64)tile - 1;
     u32 spins = 0;
     while (t >= 0) {
-        const u32 w = ld_volatile(lb + (size_t)t * stride);
-        const u32 fl = w >> 30;
-        if (fl == 0) {
+        u32 w[4];
+#pragma unroll
+        for (int k = 0; k < 4; ++k)
+            w[k] = t - k >= 0 ? ld_volatile(lb + (size_t)(t - k) * stride) : kFlagPre;
+        int k = 0;
+        bool done = false;
+        for (; k < 4; ++k) {
+            const u32 fl = w[k] >> 30;
+            if (fl == 0) break;
+            excl += w[k] & kCountMask;
+            if (fl == 2) {
+                done = true;
+                break;
+            }
+        }
+        if (done) break;
+        t -= k;
+        if (k == 0) {
             if (++spins > kSpinLimit) {
                 raise_status(status, PL_ERR_TIMEOUT);
                 break;
             }
             if (spins > 64) __nanosleep(64);
-            continue;
         }
-        excl += w & kCountMask;
-        if (fl == 2) break;
-        --t;
     }
     st_volatile(mine, kFlagPre | ((excl + cnt) & kCountMask));
     return excl;
@@ -340,28 +463,32 @@ struct RadixSmem {
     u32 tile;
 };
 
-__global__ void __launch_bounds__(kThreads, 2)
+// LAST: the final pass also fetches each term's coefficient from the source
+// and writes it in sorted order, so the segment sums read contiguous values.
+template <class Src, bool LAST>
+__global__ void __launch_bounds__(kThreads, 4)
     k_radix_pass(const u64* __restrict__ kin, const u32* __restrict__ vin, u64* __restrict__ kout,
                  u32* __restrict__ vout, u32 n, int shift, int bits,
-                 const u32* __restrict__ bstart, u32* lb, u32* tile_ctr, int* status) {
+                 const u32* __restrict__ bstart, u32* lb, u32* tile_ctr, int* status, Src src,
+                 double* __restrict__ val_out) {
     extern __shared__ __align__(16) unsigned char dsm[];
     u64* skeys = reinterpret_cast<u64*>(dsm);
-    u32* svals = reinterpret_cast<u32*>(dsm + sizeof(u64) * kTile);
+    u32* svals = reinterpret_cast<u32*>(dsm + sizeof(u64) * kRTile);
     __shared__ RadixSmem S;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     if (tid == 0) S.tile = atomicAdd(tile_ctr, 1u);
     for (int i = tid; i < kWarps * kRadix; i += kThreads) S.whist[i] = 0;
     __syncthreads();
     const u32 tile = S.tile;
-    const u32 base = tile * (u32)kTile;
+    const u32 base = tile * (u32)kRTile;
     const u32 dmask = (1u << bits) - 1u;
 
-    u64 keys[kItems];
-    u32 vals[kItems];
-    u32 rank[kItems];
-    const u32 wbase = base + (u32)warp * (kItems * 32);
+    u64 keys[kRItems];
+    u32 vals[kRItems];
+    u32 rank[kRItems];
+    const u32 wbase = base + (u32)warp * (kRItems * 32);
 #pragma unroll
-    for (int t = 0; t < kItems; ++t) {
+    for (int t = 0; t < kRItems; ++t) {
         const u32 idx = wbase + t * 32 + lane;
         if (idx < n) {
             keys[t] = kin[idx];
@@ -373,7 +500,7 @@ __global__ void __launch_bounds__(kThreads, 2)
     }
     u32* wh = S.whist + warp * kRadix;
 #pragma unroll
-    for (int t = 0; t < kItems; ++t) {
+    for (int t = 0; t < kRItems; ++t) {
         const bool valid = (wbase + t * 32 + lane) < n;
         const u32 d = valid ? ((u32)(keys[t] >> shift) & dmask) : kSentinel;
         const u32 peers = __match_any_sync(0xffffffffu, d);
@@ -404,7 +531,7 @@ __global__ void __launch_bounds__(kThreads, 2)
     S.gofs[d] = bstart[d] + excl;
     __syncthreads();
 #pragma unroll
-    for (int t = 0; t < kItems; ++t) {
+    for (int t = 0; t < kRItems; ++t) {
         if (wbase + t * 32 + lane < n) {
             const u32 dd = (u32)(keys[t] >> shift) & dmask;
             const u32 pos = S.bloc[dd] + S.whist[warp * kRadix + dd] + rank[t];
@@ -413,21 +540,23 @@ __global__ void __launch_bounds__(kThreads, 2)
         }
     }
     __syncthreads();
-    const u32 tile_n = min((u32)kTile, n - base);
+    const u32 tile_n = min((u32)kRTile, n - base);
     for (u32 p = tid; p < tile_n; p += kThreads) {
         const u64 k = skeys[p];
         const u32 dd = (u32)(k >> shift) & dmask;
         const u32 g = S.gofs[dd] + (p - S.bloc[dd]);
         if (g < n) {
+            const u32 pv = svals[p];
             kout[g] = k;
-            vout[g] = svals[p];
+            vout[g] = pv;
+            if (LAST) val_out[g] = src.value(pv & kIdxMask);
         } else {
             raise_status(status, PL_ERR_INTERNAL);
         }
     }
 }
 
-constexpr size_t kRadixDynSmem = sizeof(u64) * kTile + sizeof(u32) * kTile;
+constexpr size_t kRadixDynSmem = sizeof(u64) * kRTile + sizeof(u32) * kRTile;
 
 // ---------------------------------------------------------------------------
 // 4. Segments: equal-key runs of the sorted order.
@@ -435,6 +564,7 @@ constexpr size_t kRadixDynSmem = sizeof(u64) * kTile + sizeof(u32) * kTile;
 struct SegCtx {
     const u64* keys;     // sorted top chunk
     const u32* pay;      // sorted payloads
+    const double* vals;  // coefficients in sorted order
     const u64* planes;   // chunk planes (nchunks > 1)
     u32 n;
     int nchunks;
@@ -442,12 +572,31 @@ struct SegCtx {
     int mode;
 };
 
-__device__ __forceinline__ bool same_key(const SegCtx& C, u32 a, u32 b) {
-    // a, b: positions in the sorted order
+// Segment fold.  A warp owns 1024 consecutive sorted terms, staged in shared
+// memory; lane L folds its own 32 terms left to right (32 independent
+// chains per warp), and a second, lane-serial phase folds each lane's
+// prefix (the tail of the segment carried in from its left neighbour) onto
+// that carry.  Every segment is therefore summed in exactly the reference's
+// left-to-right order (PauliSumOperations.h:443-455).  The warp that holds a
+// segment's head owns it; an owned segment still open at the end of the
+// range is continued chunk by chunk (up to kExtChunks) and otherwise handed
+// to k_long_segments.  Results go to segval[head], segflag[head] = 1
+// (2 = long, pending); non-heads get segflag 0.
+constexpr int kFoldWarps = 4;
+constexpr int kLaneSpan = 32;
+constexpr u32 kFoldSpan = 32u * kLaneSpan;  // 1024 terms per warp
+constexpr u32 kFoldSlots = 33u * 32u;       // lane spans padded to 33 slots (no bank conflicts)
+constexpr int kExtChunks = 32;              // at most 1024 more
+constexpr size_t kFoldWarpSmem = kFoldSlots * (8 + 4 + 1);
+constexpr size_t kFoldSmem = ((kFoldWarpSmem + 15) & ~size_t(15)) * kFoldWarps;
+
+__device__ __forceinline__ bool lane_same_key(const SegCtx& C, u32 e, u64 ke, u64 kprev,
+                                              u32 pe, u32 pprev) {
+    // e and its predecessor, by top chunk (ke, kprev) and payloads (lower chunks)
     const u64 m_top = C.nchunks == 1 ? C.seg_mask0 : ~0ull;
-    if (((C.keys[a] ^ C.keys[b]) & m_top) != 0) return false;
+    if (((ke ^ kprev) & m_top) != 0) return false;
     if (C.nchunks == 1) return true;
-    const u32 ia = C.pay[a] & kIdxMask, ib = C.pay[b] & kIdxMask;
+    const u32 ia = pe & kIdxMask, ib = pprev & kIdxMask;
     for (int c = 0; c < C.nchunks - 1; ++c) {
         const u64 m = c == 0 ? C.seg_mask0 : ~0ull;
         if (((C.planes[(i64)c * C.n + ia] ^ C.planes[(i64)c * C.n + ib]) & m) != 0) return false;
@@ -455,105 +604,217 @@ __device__ __forceinline__ bool same_key(const SegCtx& C, u32 a, u32 b) {
     return true;
 }
 
-template <class Src>
-__device__ __forceinline__ double seg_sum_seq(const Src& src, const u32* pay, u32 b, u32 e,
-                                              int mode) {
-    double s0 = 0.0, s1 = 0.0;
-    for (u32 t = b; t < e; ++t) {
-        const u32 p = pay[t];
-        const double v = src.value(p & kIdxMask);
-        const bool neg = (p >> 31) != 0;
-        if (mode == kCanon) s0 = dadd(s0, neg ? -v : v);
-        else if (mode == kCombine) s0 = dadd(s0, v);
-        else if (neg) s1 = dadd(s1, v);
-        else s0 = dadd(s0, v);
-    }
-    return mode == kProp ? dadd(s0, -s1) : s0;
+template <int MODE>
+__device__ __forceinline__ void fold_add(double& r0, double& r1, double v, u32 p) {
+    const bool neg = (p >> 31) != 0;
+    if (MODE == kCanon) r0 = dadd(r0, neg ? -v : v);
+    else if (MODE == kCombine) r0 = dadd(r0, v);
+    else if (neg) r1 = dadd(r1, v);
+    else r0 = dadd(r0, v);
 }
 
-struct SegSmem {
-    u32 swarp[kWarps];
-    u32 tile;
-    u32 excl;
-};
+template <int MODE>
+__device__ __forceinline__ void fold_close(double* segval, u8* segflag, i64 h, double r0,
+                                           double r1) {
+    segval[h] = MODE == kProp ? dadd(r0, -r1) : r0;
+    segflag[h] = 1;
+}
 
-// Heads get dense ids; short runs are summed here, long runs listed.
-template <class Src>
-__global__ void __launch_bounds__(kThreads) k_segments(Src src, SegCtx C, u32* seg_start,
-                                                       double* seg_sum, u32* long_list,
-                                                       u32* counters, u32* lb, int* status) {
-    // counters: [0] tile ctr, [1] segment count, [2] long count
-    __shared__ SegSmem S;
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    if (tid == 0) S.tile = atomicAdd(&counters[0], 1u);
-    __syncthreads();
-    const u32 tile = S.tile;
-    const u32 wbase = tile * (u32)kTile + (u32)warp * (kItems * 32);
-    u32 headmask = 0;  // bit t: item t is a head
-    u32 wcount = 0;
-    u32 myoff[kItems];
-#pragma unroll
-    for (int t = 0; t < kItems; ++t) {
-        const u32 e = wbase + t * 32 + lane;
-        bool h = false;
-        if (e < C.n) h = (e == 0) || !same_key(C, e, e - 1);
-        const u32 bal = __ballot_sync(0xffffffffu, h);
-        myoff[t] = wcount + __popc(bal & lanemask_lt());
-        wcount += __popc(bal);
-        if (h) headmask |= 1u << t;
+template <int MODE>
+__global__ void __launch_bounds__(32 * kFoldWarps) k_fold(SegCtx C, double* segval,
+                                                          u8* segflag, u32* long_list,
+                                                          u32* counters) {
+    extern __shared__ __align__(16) unsigned char fsm[];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const u32 gwarp = blockIdx.x * kFoldWarps + warp;
+    const u32 w0 = gwarp * kFoldSpan;
+    if (w0 >= C.n) return;
+    const u32 w1 = min(w0 + kFoldSpan, C.n);
+    const u32 cnt = w1 - w0;
+    unsigned char* base = fsm + ((kFoldWarpSmem + 15) & ~size_t(15)) * warp;
+    double* sv = reinterpret_cast<double*>(base);
+    u32* sp = reinterpret_cast<u32*>(base + 8 * kFoldSlots);
+    u8* sh = base + 12 * kFoldSlots;
+    // ---- staging: coalesced loads, head flags, non-head segflag = 0
+    u64 ck = 0;
+    u32 cp = 0;
+    if (w0 > 0) {
+        ck = C.keys[w0 - 1];
+        cp = C.pay[w0 - 1];
     }
-    u32 total;
-    const u32 wexcl = block_excl_scan(lane == 0 ? wcount : 0u, S.swarp, total);
-    const u32 wpre = __shfl_sync(0xffffffffu, wexcl, 0);
-    if (tid == 0) S.excl = lookback(lb, tile, 1, total, status);
-    __syncthreads();
-    const u32 base_id = S.excl + wpre;
+    // 8 chunks of loads in flight per lane, then the head flags of those chunks
+    constexpr int kBatch = 8;
+    for (u32 c0 = 0; c0 * 32 < cnt; c0 += kBatch) {
+        u64 ke[kBatch];
+        u32 pe[kBatch];
+        double ve[kBatch];
 #pragma unroll
-    for (int t = 0; t < kItems; ++t) {
-        if (!(headmask & (1u << t))) continue;
-        const u32 e = wbase + t * 32 + lane;
-        const u32 s = base_id + myoff[t];
-        seg_start[s] = e;
-        // find the end of the run, up to kShortSeg + 1 terms
-        u32 end = e + 1;
-        while (end < C.n && end - e <= (u32)kShortSeg && same_key(C, end, e)) ++end;
-        if (end - e <= (u32)kShortSeg) {
-            seg_sum[s] = seg_sum_seq(src, C.pay, e, end, C.mode);
-        } else {
-            const u32 li = atomicAdd(&counters[2], 1u);
-            long_list[li] = s;
+        for (int b = 0; b < kBatch; ++b) {
+            const u32 i = (c0 + b) * 32 + lane;
+            const bool valid = i < cnt;
+            ke[b] = valid ? C.keys[w0 + i] : 0ull;
+            pe[b] = valid ? C.pay[w0 + i] : 0u;
+            ve[b] = valid ? C.vals[w0 + i] : 0.0;
+        }
+#pragma unroll
+        for (int b = 0; b < kBatch; ++b) {
+            const u32 c = c0 + b;
+            const u32 i = c * 32 + lane;
+            const u32 e = w0 + i;
+            u64 kp = __shfl_up_sync(0xffffffffu, ke[b], 1);
+            u32 pp = __shfl_up_sync(0xffffffffu, pe[b], 1);
+            if (lane == 0) {
+                kp = ck;
+                pp = cp;
+            }
+            if (i < cnt) {
+                const bool head = (e == 0) || !lane_same_key(C, e, ke[b], kp, pe[b], pp);
+                const u32 slot = c * 33 + lane;
+                sh[slot] = head;
+                sp[slot] = pe[b];
+                sv[slot] = ve[b];
+                if (!head) segflag[e] = 0;
+            }
+            ck = __shfl_sync(0xffffffffu, ke[b], 31);
+            cp = __shfl_sync(0xffffffffu, pe[b], 31);
         }
     }
-    // The last tile publishes the segment count and the end sentinel.
-    if (tile == gridDim.x - 1 && tid == 0) {
-        counters[1] = S.excl + total;
-        seg_start[S.excl + total] = C.n;
+    __syncwarp();
+    // ---- phase 1: each lane folds the segments that start inside its span
+    const u32 a = (u32)lane * kLaneSpan;
+    const u32 sa = (u32)lane * 33u;
+    const u32 lcnt = cnt > a ? min(cnt - a, (u32)kLaneSpan) : 0u;
+    u32 first_head = lcnt;  // prefix length (terms before the lane's first head)
+    i64 h = -1;
+    double r0 = 0.0, r1 = 0.0;
+    for (u32 i = 0; i < lcnt; ++i) {
+        if (sh[sa + i]) {
+            if (h >= 0) fold_close<MODE>(segval, segflag, h, r0, r1);
+            else first_head = i;
+            h = (i64)(w0 + a + i);
+            r0 = 0.0;
+            r1 = 0.0;
+        }
+        if (h >= 0) fold_add<MODE>(r0, r1, sv[sa + i], sp[sa + i]);
+    }
+    // ---- phase 2: lane-serial carry of the segment crossing lane borders
+    i64 ch = -1;  // head of the carried segment (-1: owned by an earlier warp)
+    double c0 = 0.0, c1 = 0.0;
+    for (int L = 0; L < 32; ++L) {
+        i64 nh = ch;
+        double n0 = c0, n1 = c1;
+        if (lane == L && lcnt) {
+            for (u32 i = 0; i < first_head; ++i) fold_add<MODE>(n0, n1, sv[sa + i], sp[sa + i]);
+            if (first_head < lcnt) {
+                if (ch >= (i64)w0) fold_close<MODE>(segval, segflag, ch, n0, n1);
+                nh = h;
+                n0 = r0;
+                n1 = r1;
+            }
+        }
+        ch = __shfl_sync(0xffffffffu, nh, L);
+        c0 = __shfl_sync(0xffffffffu, n0, L);
+        c1 = __shfl_sync(0xffffffffu, n1, L);
+    }
+    if (ch < (i64)w0) return;  // the open segment belongs to an earlier warp
+    if (w1 == C.n) {
+        if (lane == 0) fold_close<MODE>(segval, segflag, ch, c0, c1);
+        return;
+    }
+    // ---- extension: continue the owned open segment past the range
+    ck = C.keys[w1 - 1];
+    cp = C.pay[w1 - 1];
+    int ext = 0;
+    for (u32 cb = w1;; cb += 32) {
+        if (cb >= C.n) {
+            if (lane == 0) fold_close<MODE>(segval, segflag, ch, c0, c1);
+            return;
+        }
+        if (++ext > kExtChunks) {
+            if (lane == 0) {
+                segflag[ch] = 2;
+                long_list[atomicAdd(&counters[2], 1u)] = (u32)ch;
+            }
+            return;
+        }
+        const u32 e = cb + lane;
+        const bool valid = e < C.n;
+        const u64 ke = valid ? C.keys[e] : 0ull;
+        const u32 pe = valid ? C.pay[e] : 0u;
+        const double ve = valid ? C.vals[e] : 0.0;
+        u64 kp = __shfl_up_sync(0xffffffffu, ke, 1);
+        u32 pp = __shfl_up_sync(0xffffffffu, pe, 1);
+        if (lane == 0) {
+            kp = ck;
+            pp = cp;
+        }
+        const bool head = valid && !lane_same_key(C, e, ke, kp, pe, pp);
+        const u32 hb = __ballot_sync(0xffffffffu, head || !valid);
+        const u32 lim = hb ? (u32)(__ffs(hb) - 1) : 32u;
+        // the tail lanes [0, lim) continue the segment, in order
+        double q0 = c0, q1 = c1;
+        for (u32 k = 0; k < lim; ++k) {
+            const double vk = __shfl_sync(0xffffffffu, ve, k);
+            const u32 pk = __shfl_sync(0xffffffffu, pe, k);
+            fold_add<MODE>(q0, q1, vk, pk);
+        }
+        c0 = q0;
+        c1 = q1;
+        if (lim < 32) {
+            if (lane == 0) fold_close<MODE>(segval, segflag, ch, c0, c1);
+            return;
+        }
+        ck = __shfl_sync(0xffffffffu, ke, 31);
+        cp = __shfl_sync(0xffffffffu, pe, 31);
     }
 }
 
-// Long runs: one CTA per run, each thread sums a contiguous slice left to
-// right, slices combined by a fixed binary tree (deterministic).
-template <class Src>
-__global__ void __launch_bounds__(kThreads) k_long_segments(Src src, const u32* pay,
-                                                            const u32* seg_start,
-                                                            const u32* long_list,
-                                                            const u32* counters, int mode,
-                                                            double* seg_sum) {
+// Long runs: one CTA per run.  The run ends at the next term whose segflag
+// is set (every head has one after k_fold); thread t sums elements t,
+// t+256, ... in order and the 256 partial sums are combined by a fixed
+// binary tree -- a deterministic order for a given run.
+__global__ void __launch_bounds__(kThreads) k_long_segments(SegCtx C, const u32* long_list,
+                                                            const u32* counters, double* segval,
+                                                            u8* segflag) {
     __shared__ double s0[kThreads], s1[kThreads];
+    __shared__ u32 s_end;
     const u32 nlong = counters[2];
     for (u32 li = blockIdx.x; li < nlong; li += gridDim.x) {
-        const u32 s = long_list[li];
-        const u32 b = seg_start[s], e = seg_start[s + 1];
-        const u32 len = e - b;
-        const u32 per = (len + kThreads - 1) / kThreads;
-        const u32 lo = min(b + per * threadIdx.x, e), hi = min(lo + per, e);
+        const u32 b = long_list[li];
+        if (threadIdx.x == 0) s_end = C.n;
+        __syncthreads();
+        // scan 4096 flags per step, 16-byte aligned groups of 16 per thread
+        for (u32 base = (b + 1) & ~15u; base < C.n; base += kThreads * 16) {
+            u32 mine = C.n;
+            const u32 lo = base + threadIdx.x * 16;
+            if (lo + 16 <= C.n) {
+                const uint4 q = *reinterpret_cast<const uint4*>(segflag + lo);
+                const u32 w[4] = {q.x, q.y, q.z, q.w};
+#pragma unroll
+                for (int j = 0; j < 16; ++j)
+                    if (mine == C.n && lo + j > b && ((w[j >> 2] >> (8 * (j & 3))) & 0xffu))
+                        mine = lo + j;
+            } else {
+                for (u32 j = 0; j < 16 && lo + j < C.n; ++j)
+                    if (lo + j > b && segflag[lo + j]) {
+                        mine = lo + j;
+                        break;
+                    }
+            }
+            if (mine < C.n) atomicMin(&s_end, mine);
+            __syncthreads();
+            const bool found = s_end < C.n;
+            __syncthreads();
+            if (found) break;
+        }
+        const u32 e = s_end;
         double a0 = 0.0, a1 = 0.0;
-        for (u32 t = lo; t < hi; ++t) {
-            const u32 p = pay[t];
-            const double v = src.value(p & kIdxMask);
+        for (u32 t = b + threadIdx.x; t < e; t += kThreads) {
+            const u32 p = C.pay[t];
+            const double v = C.vals[t];
             const bool neg = (p >> 31) != 0;
-            if (mode == kCanon) a0 = dadd(a0, neg ? -v : v);
-            else if (mode == kCombine) a0 = dadd(a0, v);
+            if (C.mode == kCanon) a0 = dadd(a0, neg ? -v : v);
+            else if (C.mode == kCombine) a0 = dadd(a0, v);
             else if (neg) a1 = dadd(a1, v);
             else a0 = dadd(a0, v);
         }
@@ -567,41 +828,88 @@ __global__ void __launch_bounds__(kThreads) k_long_segments(Src src, const u32* 
             }
             __syncthreads();
         }
-        if (threadIdx.x == 0) seg_sum[s] = mode == kProp ? dadd(s0[0], -s1[0]) : s0[0];
+        if (threadIdx.x == 0) {
+            segval[b] = C.mode == kProp ? dadd(s0[0], -s1[0]) : s0[0];
+            segflag[b] = 1;
+        }
         __syncthreads();
     }
+}
+
+struct SegSmem {
+    u32 swarp[kWarps];
+    u32 tile;
+    u32 excl;
+};
+
+// No digit pass at all (every key equal): values in input order.
+template <class Src>
+__global__ void __launch_bounds__(256) k_gather_values(Src src, const u32* pay, u32 n,
+                                                       double* vals) {
+    for (u32 i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+        vals[i] = src.value(pay[i] & kIdxMask);
 }
 
 // ---------------------------------------------------------------------------
 // 5. Emit: keep-filter + order-preserving compaction into the output.
 // ---------------------------------------------------------------------------
 template <int AS, class Src>
-__global__ void __launch_bounds__(kThreads) k_emit(Src src, const u32* pay, const u32* seg_start,
-                                                   const double* seg_sum, u32* counters, u32* lb,
-                                                   int mode, double cutoff, u64 max_weight,
-                                                   SoAOut out, i64* d_out_count, int* status) {
-    // counters: [1] segment count (input), [3] tile ctr
+__device__ __forceinline__ void emit_key(const Src& src, const KeyLayout& L, u64 packed,
+                                         const u32* pay, u32 pos, int mode, u64* xw, u64* zw,
+                                         u32& fl) {
+    if (L.nchunks == 1) {
+        u32 fv;
+        unpack_key<AS>(L, packed, xw, zw, fv);
+        fl = out_flags(fv, mode);
+    } else {
+        src.key(pay[pos] & kIdxMask, xw, zw, fl);
+        fl = mode == kCombine ? (fl & 3u) : (fl & 1u);
+    }
+}
+
+template <int AS, class Src>
+__global__ void __launch_bounds__(kThreads) k_emit(Src src, KeyLayout L, const u64* keys,
+                                                   const u32* pay, const double* segval,
+                                                   const u8* segflag, u32 n, u32* counters,
+                                                   u32* lb, int mode, double cutoff,
+                                                   u64 max_weight, SoAOut out, i64* d_out_count,
+                                                   int* status) {
+    // Heads (segflag set) that survive the filters are compacted in order.
+    // Warp-striped items: coalesced loads; all flags are loaded before any
+    // value so the loads overlap.  counters: [3] tile ctr.
     __shared__ SegSmem S;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     if (tid == 0) S.tile = atomicAdd(&counters[3], 1u);
     __syncthreads();
-    const u32 nseg = counters[1];
     const u32 tile = S.tile;
     const u32 wbase = tile * (u32)kTile + (u32)warp * (kItems * 32);
+    u32 headmask = 0;
+#pragma unroll
+    for (int t = 0; t < kItems; ++t) {
+        const u32 e = wbase + t * 32 + lane;
+        if (e < n && segflag[e]) headmask |= 1u << t;
+    }
+    double v[kItems];
+    u64 kk[kItems];
+#pragma unroll
+    for (int t = 0; t < kItems; ++t) {
+        const bool hd = (headmask >> t) & 1u;
+        v[t] = hd ? segval[wbase + t * 32 + lane] : 0.0;
+        kk[t] = hd ? keys[wbase + t * 32 + lane] : 0ull;
+    }
     u32 keepmask = 0, wcount = 0;
     u32 myoff[kItems];
 #pragma unroll
     for (int t = 0; t < kItems; ++t) {
-        const u32 s = wbase + t * 32 + lane;
+        const u32 e = wbase + t * 32 + lane;
         bool keep = false;
-        if (s < nseg) {
-            const double v = seg_sum[s];
-            keep = (mode == kCombine) || (v != 0.0);
-            if (cutoff > 0.0) keep = keep && (fabs(v) >= cutoff);
+        if ((headmask >> t) & 1u) {
+            keep = (mode == kCombine) || (v[t] != 0.0);
+            if (cutoff > 0.0) keep = keep && (fabs(v[t]) >= cutoff);
             if (keep && max_weight != ~0ull) {
                 u64 xw[AS], zw[AS];
-                u32 fl;
-                src.key(pay[seg_start[s]] & kIdxMask, xw, zw, fl);
+                u32 f;
+                emit_key<AS>(src, L, kk[t], pay, e, mode, xw, zw, f);
                 u64 w = 0;
 #pragma unroll
                 for (int k = 0; k < AS; ++k) w += (u64)__popcll(xw[k] | zw[k]);
@@ -621,23 +929,23 @@ __global__ void __launch_bounds__(kThreads) k_emit(Src src, const u32* pay, cons
     const u32 base_o = S.excl + wpre;
 #pragma unroll
     for (int t = 0; t < kItems; ++t) {
-        if (!(keepmask & (1u << t))) continue;
-        const u32 s = wbase + t * 32 + lane;
+        if (!((keepmask >> t) & 1u)) continue;
+        const u32 e = wbase + t * 32 + lane;
         const i64 o = (i64)base_o + myoff[t];
         if (o >= out.capacity) {
             raise_status(status, PL_ERR_CAPACITY);
             continue;
         }
         u64 xw[AS], zw[AS];
-        u32 fl;
-        src.key(pay[seg_start[s]] & kIdxMask, xw, zw, fl);
+        u32 f;
+        emit_key<AS>(src, L, kk[t], pay, e, mode, xw, zw, f);
 #pragma unroll
         for (int k = 0; k < AS; ++k) {
             out.x[(i64)k * out.capacity + o] = xw[k];
             out.z[(i64)k * out.capacity + o] = zw[k];
         }
-        out.f[o] = (u8)(mode == kCombine ? (fl & 3u) : (fl & 1u));
-        out.v[o] = seg_sum[s];
+        out.f[o] = (u8)f;
+        out.v[o] = v[t];
     }
     if (tile == gridDim.x - 1 && tid == 0) *d_out_count = (i64)S.excl + total;
 }
@@ -669,14 +977,16 @@ int max_chunks(int as) { return (128 * as + 2 + 63) / 64; }
 
 size_t ws_for(int as, i64 n, int nch) {
     const i64 tiles = (n + kTile - 1) / kTile + 1;
+    const i64 rtiles = (n + kRTile - 1) / kRTile + 1;
     size_t b = 0;
     b += 2 * al(8 * n) + 2 * al(4 * n);                  // keys, payload (ping-pong)
+    b += al(8 * n);                                      // values in sorted order
     b += nch > 1 ? al(8 * (size_t)n * nch) : al(8);     // chunk planes
     b += al(4 * kMaxPasses * kRadix);                    // histograms / bucket starts
-    b += al(4 * (size_t)tiles * kRadix);                 // radix look-back (one pass)
+    b += al(4 * (size_t)rtiles * kRadix);                // radix look-back (one pass)
     b += al(4 * (n + 1)) + al(8 * n) + al(4 * n);         // seg_start, seg_sum, long list
     b += 2 * al(4 * tiles);                              // segment / emit look-back
-    b += al(4 * (kMaxPasses + 8));                       // counters
+    b += al(4 * (128 + 16 * kRadix));                    // counters + operand histograms
     b += 2 * al(8 * kMaxFields) + al(8) + al(4);          // masks, out count, status
     return b + 1024;
 }
@@ -687,6 +997,7 @@ void build_layout(int as, int mode, const u64* orm, const u64* andm, KeyLayout& 
     std::memset(&P, 0, sizeof(P));
     for (int f = 0; f < nf; ++f) {
         const u64 var = orm[f] ^ andm[f];
+        L.cbits[f] = andm[f];
         if (var == 0) continue;
         const int lo = __builtin_ctzll(var), hi = 63 - __builtin_clzll(var);
         L.lo[f] = lo;
@@ -722,7 +1033,7 @@ void build_layout(int as, int mode, const u64* orm, const u64* andm, KeyLayout& 
 struct Bufs {
     u64 *ka, *kb, *planes;
     u32 *pa, *pb, *hist, *lb, *seg_start, *long_list, *lb_seg, *lb_emit, *counters;
-    double* seg_sum;
+    double *seg_sum, *sv;
     u64 *orm, *andm;
     i64* d_count;
     int* d_status;
@@ -730,20 +1041,22 @@ struct Bufs {
 
 bool carve(void* ws, size_t bytes, i64 n, int nch, Bufs& B) {
     const i64 tiles = (n + kTile - 1) / kTile + 1;
+    const i64 rtiles = (n + kRTile - 1) / kRTile + 1;
     Carve c{(unsigned char*)ws, bytes};
     B.ka = c.take<u64>(n);
     B.kb = c.take<u64>(n);
     B.pa = c.take<u32>(n);
     B.pb = c.take<u32>(n);
+    B.sv = c.take<double>(n);
     B.planes = c.take<u64>(nch > 1 ? (size_t)n * nch : 1);
     B.hist = c.take<u32>(kMaxPasses * kRadix);
-    B.lb = c.take<u32>((size_t)tiles * kRadix);
+    B.lb = c.take<u32>((size_t)rtiles * kRadix);
     B.seg_start = c.take<u32>(n + 1);
     B.seg_sum = c.take<double>(n);
     B.long_list = c.take<u32>(n);
     B.lb_seg = c.take<u32>(tiles);
     B.lb_emit = c.take<u32>(tiles);
-    B.counters = c.take<u32>(kMaxPasses + 8);
+    B.counters = c.take<u32>(128 + 16 * kRadix);
     B.orm = c.take<u64>(kMaxFields);
     B.andm = c.take<u64>(kMaxFields);
     B.d_count = c.take<i64>(1);
@@ -751,60 +1064,122 @@ bool carve(void* ws, size_t bytes, i64 n, int nch, Bufs& B) {
     return c.ok;
 }
 
+// Histograms that can be derived instead of counted: none for a plain sum.
+template <int AS>
+u32 derive_histograms(const SoASrc<AS>&, const KeyLayout&, const PassPlan&, Bufs&,
+                      cudaStream_t) {
+    return 0u;
+}
+
+// Products: chunk-0 passes free of flags bits come from operand histograms.
+template <int AS>
+u32 derive_histograms(const ProdSrc<AS>& src, const KeyLayout& L, const PassPlan& P, Bufs& B,
+                      cudaStream_t st) {
+    const int np0 = P.first[1] - P.first[0];
+    const int wf = L.width[2 * AS];  // the flags field occupies packed bits [0, wf)
+    u32 mask = 0;
+    for (int p = 0; p < np0; ++p)
+        if (P.shift[p] >= wf) mask |= 1u << p;
+    if (!mask) return 0u;
+    u32* hA = B.counters + 128;                   // scratch after the counters
+    u32* hB = hA + 8 * kRadix;
+    if (cudaMemsetAsync(hA, 0, sizeof(u32) * 16 * kRadix, st) != cudaSuccess) return 0u;
+    const SoASrc<AS> a{src.ax, src.az, src.af, src.av, src.sa};
+    const SoASrc<AS> b{src.bx, src.bz, src.bf, src.bv, src.sb};
+    k_operand_hist<AS><<<grid_for(src.n, 256, 64), 256, 0, st>>>(a, src.n, L, P, mask, hA),
+        pl::note_launch();
+    k_operand_hist<AS><<<grid_for(src.m, 256, 64), 256, 0, st>>>(b, src.m, L, P, mask, hB),
+        pl::note_launch();
+    k_xor_conv<<<np0, 256, 0, st>>>(hA, hB, P, mask, B.hist), pl::note_launch();
+    return mask;
+}
+
 template <int AS, class Src>
 int run_collate(const Src& src, u32 n, int mode, const KeyLayout& L, const PassPlan& P,
                 const CollateArgs& a, const SoAOut& out, i64* out_count, Bufs& B,
                 cudaStream_t st) {
-    PL_CUDA_TRY(cudaFuncSetAttribute(k_radix_pass, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     (int)kRadixDynSmem));
     const u32 tiles = (n + kTile - 1) / kTile;
+    const u32 rtiles = (n + kRTile - 1) / kRTile;
     const int nsm = sm_count();
     PL_CUDA_TRY(cudaMemsetAsync(B.hist, 0, sizeof(u32) * kMaxPasses * kRadix, st));
     PL_CUDA_TRY(cudaMemsetAsync(B.counters, 0, sizeof(u32) * (kMaxPasses + 8), st));
     PL_CUDA_TRY(cudaMemsetAsync(B.d_status, 0, sizeof(int), st));
     PL_CUDA_TRY(cudaMemsetAsync(B.d_count, 0, sizeof(i64), st));
     const int gblocks = grid_for(n, 256, nsm * 8);
-    k_pack<AS, Src><<<gblocks, 256, 0, st>>>(src, n, mode, L, P, B.ka, B.pa, B.planes, B.hist), pl::note_launch();
+    cudaEvent_t e0 = timed_begin(st);
+    const u32 derived = derive_histograms<AS>(src, L, P, B, st);
+    timed_end(e0, st, "k_xor_conv", 0ull);
+    e0 = timed_begin(st);
+    k_pack<AS, Src><<<gblocks, 256, 0, st>>>(src, n, mode, L, P, ~derived, B.ka, B.pa, B.planes,
+                                             B.hist),
+        pl::note_launch();
+    timed_end(e0, st, "k_pack", 12ull * n);
     u64 *kin = B.ka, *kout = B.kb;
     u32 *vin = B.pa, *vout = B.pb;
+    const SoASrc<1> nosrc{nullptr, nullptr, nullptr, nullptr, 0};
     for (int c = 0; c < L.nchunks; ++c) {
         const int p0 = P.first[c], np = P.first[c + 1] - p0;
         if (np == 0) continue;
-        if (c > 0)
+        if (c > 0) {
+            e0 = timed_begin(st);
             k_gather_chunk<<<gblocks, 256, 0, st>>>(B.planes + (size_t)c * n, vin, n, P, c, kin,
                                                     B.hist, B.d_status), pl::note_launch();
+            timed_end(e0, st, "k_gather_chunk", 20ull * n);
+        }
         k_scan_buckets<<<np, kRadix, 0, st>>>(B.hist, p0), pl::note_launch();
         for (int p = p0; p < p0 + np; ++p) {
-            PL_CUDA_TRY(cudaMemsetAsync(B.lb, 0, sizeof(u32) * (size_t)tiles * kRadix, st));
-            cudaEvent_t ev0 = nullptr, ev1 = nullptr;
-            if (timing_enabled()) {
-                PL_CUDA_TRY(cudaEventCreate(&ev0));
-                PL_CUDA_TRY(cudaEventCreate(&ev1));
-                PL_CUDA_TRY(cudaEventRecord(ev0, st));
-            }
-            k_radix_pass<<<tiles, kThreads, kRadixDynSmem, st>>>(
-                kin, vin, kout, vout, n, P.shift[p], P.bits[p], B.hist + (size_t)p * kRadix, B.lb,
-                B.counters + 8 + p, B.d_status), pl::note_launch();
-            if (ev1) {
-                PL_CUDA_TRY(cudaEventRecord(ev1, st));
-                // algorithmic bytes: read and write one u64 key + one u32 payload per term
-                timed_push(ev0, ev1, 24ull * n);
-            }
+            PL_CUDA_TRY(cudaMemsetAsync(B.lb, 0, sizeof(u32) * (size_t)rtiles * kRadix, st));
+            cudaEvent_t ev0 = timed_begin(st);
+            const bool last = (p == P.npasses - 1);
+            if (last)
+                k_radix_pass<Src, true><<<rtiles, kThreads, kRadixDynSmem, st>>>(
+                    kin, vin, kout, vout, n, P.shift[p], P.bits[p], B.hist + (size_t)p * kRadix,
+                    B.lb, B.counters + 8 + p, B.d_status, src, B.sv), pl::note_launch();
+            else
+                k_radix_pass<SoASrc<1>, false><<<rtiles, kThreads, kRadixDynSmem, st>>>(
+                    kin, vin, kout, vout, n, P.shift[p], P.bits[p], B.hist + (size_t)p * kRadix,
+                    B.lb, B.counters + 8 + p, B.d_status, nosrc, nullptr), pl::note_launch();
+            // algorithmic bytes: read and write one u64 key + one u32 payload per
+            // term (+ the u64 coefficient written by the last pass)
+            timed_end(ev0, st, "k_radix_pass", 24ull * n + (last ? 8ull * n : 0ull));
             std::swap(kin, kout);
             std::swap(vin, vout);
         }
     }
-    PL_CUDA_TRY(cudaMemsetAsync(B.lb_seg, 0, sizeof(u32) * tiles, st));
-    SegCtx C{kin, vin, B.planes, n, L.nchunks, L.seg_mask0, mode};
-    k_segments<Src><<<tiles, kThreads, 0, st>>>(src, C, B.seg_start, B.seg_sum, B.long_list,
-                                                B.counters, B.lb_seg, B.d_status), pl::note_launch();
-    k_long_segments<Src><<<nsm * 4, kThreads, 0, st>>>(src, vin, B.seg_start, B.long_list,
-                                                       B.counters, mode, B.seg_sum), pl::note_launch();
+    if (P.npasses == 0)
+        k_gather_values<Src><<<gblocks, 256, 0, st>>>(src, vin, n, B.sv), pl::note_launch();
+    SegCtx C{kin, vin, B.sv, B.planes, n, L.nchunks, L.seg_mask0, mode};
+    u8* segflag = reinterpret_cast<u8*>(B.seg_start);
+    const u32 fold_blocks = (n + kFoldSpan * kFoldWarps - 1) / (kFoldSpan * kFoldWarps);
+    PL_CUDA_TRY(cudaFuncSetAttribute(k_fold<kCanon>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)kFoldSmem));
+    PL_CUDA_TRY(cudaFuncSetAttribute(k_fold<kCombine>,
+                                     cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kFoldSmem));
+    PL_CUDA_TRY(cudaFuncSetAttribute(k_fold<kProp>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)kFoldSmem));
+    e0 = timed_begin(st);
+    if (mode == kCanon)
+        k_fold<kCanon><<<fold_blocks, 32 * kFoldWarps, kFoldSmem, st>>>(
+            C, B.seg_sum, segflag, B.long_list, B.counters), pl::note_launch();
+    else if (mode == kCombine)
+        k_fold<kCombine><<<fold_blocks, 32 * kFoldWarps, kFoldSmem, st>>>(
+            C, B.seg_sum, segflag, B.long_list, B.counters), pl::note_launch();
+    else
+        k_fold<kProp><<<fold_blocks, 32 * kFoldWarps, kFoldSmem, st>>>(
+            C, B.seg_sum, segflag, B.long_list, B.counters), pl::note_launch();
+    timed_end(e0, st, "k_fold", 20ull * n);
+    e0 = timed_begin(st);
+    k_long_segments<<<nsm * 2, kThreads, 0, st>>>(C, B.long_list, B.counters, B.seg_sum,
+                                                  segflag), pl::note_launch();
+    timed_end(e0, st, "k_long_segments", 0ull);
     // Emit over the segment count; the grid covers the worst case (n).
     PL_CUDA_TRY(cudaMemsetAsync(B.lb_emit, 0, sizeof(u32) * tiles, st));
-    k_emit<AS, Src><<<tiles, kThreads, 0, st>>>(src, vin, B.seg_start, B.seg_sum, B.counters,
-                                                B.lb_emit, mode, a.cutoff, a.max_weight, out,
-                                                B.d_count, B.d_status), pl::note_launch();
+    e0 = timed_begin(st);
+    k_emit<AS, Src><<<tiles, kThreads, 0, st>>>(src, L, kin, vin, B.seg_sum, segflag, n,
+                                                B.counters, B.lb_emit, mode, a.cutoff,
+                                                a.max_weight, out, B.d_count, B.d_status),
+        pl::note_launch();
+    timed_end(e0, st, "k_emit", 0ull);
     PL_CUDA_TRY(cudaGetLastError());
     i64 cnt = 0;
     int dstat = 0;
@@ -924,8 +1299,9 @@ int multiply_collate(int as, const SoAView& lhs, const SoAView& rhs, const SoAOu
         KeyLayout L;
         PassPlan P;
         build_layout(AS, a.mode, por, pand, L, P);
-        ProdSrc<AS> src{lhs.x, lhs.z, rhs.x,    rhs.z,      lhs.f,     rhs.f,
-                        lhs.v, rhs.v, (u32)lhs.n, (u32)rhs.n, lhs.stride, rhs.stride};
+        ProdSrc<AS> src{lhs.x, lhs.z, rhs.x,      rhs.z,      lhs.f,      rhs.f,
+                        lhs.v, rhs.v, (u32)lhs.n, (u32)rhs.n, lhs.stride, rhs.stride,
+                        FastDiv::make((u32)lhs.n)};
         rc = run_collate<AS>(src, n, a.mode, L, P, a, out, out_count, B, st);
     });
     return rc;

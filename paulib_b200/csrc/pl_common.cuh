@@ -122,5 +122,8 @@ int record_status(int code, const char* what);
 // Measurement hooks (pl_profile_*): launch counter and event-timed passes.
 void note_launch();
 bool timing_enabled();
-void timed_push(cudaEvent_t start, cudaEvent_t stop, unsigned long long bytes);
+void timed_push(cudaEvent_t start, cudaEvent_t stop, unsigned long long bytes, const char* name);
+// Event pair around one launch when timing is enabled (no-op otherwise).
+cudaEvent_t timed_begin(cudaStream_t st);
+void timed_end(cudaEvent_t start, cudaStream_t st, const char* name, unsigned long long bytes);
 }  // namespace pl

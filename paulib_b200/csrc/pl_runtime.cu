@@ -24,6 +24,7 @@ std::atomic<bool> g_timing{false};
 struct Timed {
     cudaEvent_t start, stop;
     unsigned long long bytes;
+    const char* name;
 };
 std::mutex g_timed_mu;
 std::vector<Timed> g_timed;
@@ -51,9 +52,25 @@ int record_cuda(cudaError_t e) {
 
 void note_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
 bool timing_enabled() { return g_timing.load(std::memory_order_relaxed); }
-void timed_push(cudaEvent_t start, cudaEvent_t stop, unsigned long long bytes) {
+void timed_push(cudaEvent_t start, cudaEvent_t stop, unsigned long long bytes, const char* name) {
     std::lock_guard<std::mutex> lock(g_timed_mu);
-    g_timed.push_back(Timed{start, stop, bytes});
+    g_timed.push_back(Timed{start, stop, bytes, name});
+}
+
+cudaEvent_t timed_begin(cudaStream_t st) {
+    if (!timing_enabled()) return nullptr;
+    cudaEvent_t e = nullptr;
+    if (cudaEventCreate(&e) != cudaSuccess) return nullptr;
+    cudaEventRecord(e, st);
+    return e;
+}
+
+void timed_end(cudaEvent_t start, cudaStream_t st, const char* name, unsigned long long bytes) {
+    if (!start) return;
+    cudaEvent_t e = nullptr;
+    if (cudaEventCreate(&e) != cudaSuccess) return;
+    cudaEventRecord(e, st);
+    timed_push(start, e, bytes, name);
 }
 
 int sm_count() {
@@ -114,6 +131,7 @@ extern "C" int pl_profile_read(uint64_t* launches, uint64_t* timed_launches, dou
     {
         std::lock_guard<std::mutex> lock(g_timed_mu);
         for (auto& t : g_timed) {
+            if (std::string(t.name) != "k_radix_pass") continue;
             float e = 0.f;
             if (cudaEventSynchronize(t.stop) != cudaSuccess ||
                 cudaEventElapsedTime(&e, t.start, t.stop) != cudaSuccess)
@@ -128,4 +146,41 @@ extern "C" int pl_profile_read(uint64_t* launches, uint64_t* timed_launches, dou
     if (timed_ms) *timed_ms = ms;
     if (timed_bytes) *timed_bytes = bytes;
     return pl::record_status(PL_OK, nullptr);
+}
+
+extern "C" int pl_profile_report(char* buf, size_t cap) {
+    // "name count total_ms bytes\n" per kernel name, in first-seen order
+    std::vector<std::string> names;
+    std::vector<double> ms;
+    std::vector<unsigned long long> cnt, bytes;
+    {
+        std::lock_guard<std::mutex> lock(g_timed_mu);
+        for (auto& t : g_timed) {
+            float e = 0.f;
+            if (cudaEventSynchronize(t.stop) != cudaSuccess ||
+                cudaEventElapsedTime(&e, t.start, t.stop) != cudaSuccess)
+                return pl::record_cuda(cudaGetLastError());
+            size_t k = 0;
+            while (k < names.size() && names[k] != t.name) ++k;
+            if (k == names.size()) {
+                names.push_back(t.name);
+                ms.push_back(0.0);
+                cnt.push_back(0);
+                bytes.push_back(0);
+            }
+            ms[k] += e;
+            cnt[k] += 1;
+            bytes[k] += t.bytes;
+        }
+    }
+    std::string out;
+    char line[256];
+    for (size_t k = 0; k < names.size(); ++k) {
+        snprintf(line, sizeof(line), "%s %llu %.6f %llu\n", names[k].c_str(), cnt[k], ms[k],
+                 bytes[k]);
+        out += line;
+    }
+    if (!buf || cap == 0) return pl::record_status(PL_ERR_INVALID_ARG, "pl_profile_report");
+    snprintf(buf, cap, "%s", out.c_str());
+    return pl::record_status(out.size() < cap ? PL_OK : PL_ERR_CAPACITY, nullptr);
 }

@@ -176,3 +176,45 @@ def test_expectation_helper(cuda, oracle):
     o = oracle.propagate(as_planes(obs), as_planes(circ.rotations), circ.ops,
                          max_weight=tr["max_weight"], cutoff=tr["cutoff"])
     assert abs(e - oracle.zero_state_expectation(o)) <= 1e-10
+
+
+# ---------------------------------------------------------------------------
+# algebra on device-resident states (pl_state_multiply / _canonicalize /
+# pl_state_commutator)
+# ---------------------------------------------------------------------------
+def test_state_multiply(cuda, oracle):
+    import ctypes
+    from paulib_b200 import _abi
+    a, b = random_sum(37, 2, 1, 100), random_sum(23, 2, 2, 100, "normal")
+    with state_of(a, hint=8) as sa, state_of(b, hint=8) as sb:
+        _abi.check(_abi.lib().pl_state_multiply(sa._h, sb._h))
+        g = planes_of(sa)
+    o = oracle.multiply(a, b)
+    assert_keys_equal(g, o)
+    assert bit_identical(g, o)
+
+
+def test_state_multiply_canonicalize(cuda, oracle):
+    from paulib_b200 import _abi
+    a, b = W.product_operands(seed=5, terms=300)
+    a, b = as_planes(a), as_planes(b)
+    with state_of(a, hint=16) as sa, state_of(b, hint=16) as sb:
+        _abi.check(_abi.lib().pl_state_multiply_canonicalize(sa._h, sb._h))
+        g = planes_of(sa)
+    prod = oracle.multiply(a, b)
+    o = oracle.canonicalize(prod)
+    assert_keys_equal(g, o)
+    assert_values_close(g, o, abs_scale(oracle, prod))
+
+
+@pytest.mark.parametrize("mul_i", [0, 1])
+def test_state_commutator(cuda, oracle, mul_i):
+    from paulib_b200 import _abi
+    a, b = W.window_sums(seed=4, terms=700)
+    a, b = as_planes(a), as_planes(b)
+    with state_of(a) as sa, state_of(b) as sb, PR.State(4, 16) as so:
+        _abi.check(_abi.lib().pl_state_commutator(so._h, sa._h, sb._h, mul_i))
+        g = planes_of(so)
+    o = oracle.commutator(a, b, bool(mul_i))
+    assert_keys_equal(g, o)
+    assert bit_identical(g, o)
