@@ -103,6 +103,26 @@ PL_API int pl_commutator(int array_size, int multiply_by_i, const uint64_t* lhs_
                   uint64_t* out_z, uint8_t* out_flags, double* out_val, int64_t capacity,
                   unsigned long long* d_count, cudaStream_t stream);
 
+/* pl_commutator for callers that cannot let the library allocate device
+ * memory -- hosts that own the whole device through their own pool or an
+ * HBM budget, and callers that cannot afford the synchronisation an
+ * allocation may cause.  No counterpart in the reference.  Same arguments,
+ * result and order as pl_commutator; its scratch is a static 512 KB device
+ * array of this library, so n*m is limited to 2^29 pairs (larger requests
+ * return PL_ERR_INVALID_ARG).  The first call on a device looks the array's
+ * address up (cudaGetSymbolAddress); make that first call before any stream
+ * capture.  All calls share the array: calls that overlap on the GPU (other
+ * streams, other threads) race and must be serialised by the caller.
+ * Synchronous, like pl_commutator.  Calls no cudaMalloc / cudaFree. */
+PL_API int pl_commutator_noalloc(int array_size, int multiply_by_i, const uint64_t* lhs_x,
+                                 const uint64_t* lhs_z, const uint8_t* lhs_flags,
+                                 const double* lhs_val, int64_t n, const uint64_t* rhs_x,
+                                 const uint64_t* rhs_z, const uint8_t* rhs_flags,
+                                 const double* rhs_val, int64_t m, uint64_t* out_x,
+                                 uint64_t* out_z, uint8_t* out_flags, double* out_val,
+                                 int64_t capacity, unsigned long long* d_count,
+                                 cudaStream_t stream);
+
 /* ---- collate: sort_and_combine / canonicalize / cutoff / weight ------- */
 
 /* canonicalize() (PauliSumUtils.h:315-328): fold the sign bit into the

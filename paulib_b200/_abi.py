@@ -42,6 +42,7 @@ EXPORTS = (
     "pl_state_apply_cnot", "pl_state_zero_state_expectation", "pl_propagate",
     "pl_profile_reset", "pl_profile_read", "pl_state_multiply",
     "pl_state_multiply_canonicalize", "pl_state_commutator", "pl_profile_report",
+    "pl_commutator_noalloc",
 )
 
 
@@ -85,6 +86,8 @@ def lib():
                               VP]),
         "pl_commutator": (I32, [I32, I32, VP, VP, VP, VP, I64, VP, VP, VP, VP, I64, VP, VP,
                                 VP, VP, I64, VP, VP]),
+        "pl_commutator_noalloc": (I32, [I32, I32, VP, VP, VP, VP, I64, VP, VP, VP, VP, I64, VP,
+                                        VP, VP, VP, I64, VP, VP]),
         "pl_collate_workspace_size": (I32, [I32, I64, C.POINTER(C.c_size_t)]),
         "pl_collate": (I32, [I32, VP, VP, VP, VP, I64, VP, VP, VP, VP, I64, C.POINTER(I64),
                              C.POINTER(CollateOpts), VP, C.c_size_t, VP]),

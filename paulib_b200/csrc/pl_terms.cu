@@ -9,6 +9,8 @@
 //   zero_state_exp.   PauliSumUtils.h:163-177
 
 #include <algorithm>
+#include <mutex>
+#include <vector>
 
 #include "pl_common.cuh"
 
@@ -383,5 +385,84 @@ extern "C" int pl_zero_state_expectation(int array_size, const uint64_t* x, cons
     PL_DISPATCH_AS(array_size, k_zero_state<AS><<<1, 1024, 0, stream>>>(
                                    (const u64*)x, flags, val, (u64)n, (u64)stride, d_result), pl::note_launch());
     PL_CUDA_TRY(cudaGetLastError());
+    return record_status(PL_OK, nullptr);
+}
+
+// ---------------------------------------------------------------------------
+// Commutator without allocation.
+//
+// Some callers cannot let a library allocate device memory: hosts that carve
+// the whole device into their own pool up front (an HBM-budgeted serving
+// process, a framework with its own caching allocator), and callers that
+// cannot afford the device-wide synchronisation that cudaMalloc / cudaFree
+// may cause.  pl_commutator_noalloc runs the same kernel as pl_commutator
+// but keeps its only scratch -- the per-tile look-back words, the tile
+// counter and the status word -- in the file-scope array below, which every
+// GPU that loads this library holds until the process exits.
+// ---------------------------------------------------------------------------
+namespace pl {
+namespace {
+constexpr u64 kNoAllocMaxTiles = 1ull << 16;  // 2^16 tiles of 8192 pairs = 2^29 pairs
+constexpr size_t kNoAllocBytes = 256 + kNoAllocMaxTiles * 8 + 256;
+static __device__ __align__(256) unsigned char g_commutator_scratch[kNoAllocBytes];
+
+// Device address of g_commutator_scratch, looked up once per device with
+// that device current.  In host code the symbol is only a host-side stand-in,
+// so the kernel must be given this address instead.
+int noalloc_scratch(void** ptr) {
+    static std::mutex mu;
+    static std::vector<void*> by_device;
+    int dev = 0;
+    PL_CUDA_TRY(cudaGetDevice(&dev));
+    std::lock_guard<std::mutex> lock(mu);
+    if ((int)by_device.size() <= dev) by_device.resize(dev + 1, nullptr);
+    if (!by_device[dev]) {
+        void* p = nullptr;
+        const cudaError_t e = cudaGetSymbolAddress(&p, g_commutator_scratch);
+        if (e != cudaSuccess) return record_cuda(e);
+        by_device[dev] = p;
+    }
+    *ptr = by_device[dev];
+    return PL_OK;
+}
+}  // namespace
+}  // namespace pl
+
+extern "C" int pl_commutator_noalloc(int array_size, int multiply_by_i, const uint64_t* lhs_x,
+                                     const uint64_t* lhs_z, const uint8_t* lhs_flags,
+                                     const double* lhs_val, int64_t n, const uint64_t* rhs_x,
+                                     const uint64_t* rhs_z, const uint8_t* rhs_flags,
+                                     const double* rhs_val, int64_t m, uint64_t* out_x,
+                                     uint64_t* out_z, uint8_t* out_flags, double* out_val,
+                                     int64_t capacity, unsigned long long* d_count,
+                                     cudaStream_t stream) {
+    if (array_size < 1 || array_size > kMaxAS || n < 0 || m < 0 || capacity < 0 || !d_count)
+        return record_status(PL_ERR_INVALID_ARG, "pl_commutator_noalloc: bad argument");
+    if (n == 0 || m == 0) return record_status(PL_OK, nullptr);
+    const u64 npairs = (u64)n * (u64)m;
+    if ((u64)m > (kNoAllocMaxTiles * kCTile) / (u64)n)
+        return record_status(PL_ERR_INVALID_ARG,
+                             "pl_commutator_noalloc: n*m exceeds the 2^29-pair limit of its "
+                             "static scratch (use pl_commutator)");
+    if (!lhs_x || !lhs_z || !lhs_flags || !lhs_val || !rhs_x || !rhs_z || !rhs_flags ||
+        !rhs_val || !out_x || !out_z || !out_flags || !out_val)
+        return record_status(PL_ERR_INVALID_ARG, "pl_commutator_noalloc: null pointer");
+    void* scratch = nullptr;
+    int rc = noalloc_scratch(&scratch);
+    if (rc) return rc;
+    int* d_status = (int*)((unsigned char*)scratch + kNoAllocBytes - 256);
+    // the array keeps the previous call's contents: clear what must start at 0
+    PL_CUDA_TRY(cudaMemsetAsync(d_status, 0, sizeof(int), stream));
+    rc = commutator_launch(array_size, multiply_by_i ? 1 : 0, (const u64*)lhs_x,
+                           (const u64*)lhs_z, lhs_flags, lhs_val, n, n, (const u64*)rhs_x,
+                           (const u64*)rhs_z, rhs_flags, rhs_val, m, m, (u64*)out_x,
+                           (u64*)out_z, out_flags, out_val, capacity, d_count, scratch, d_status,
+                           stream);
+    if (rc) return rc;
+    (void)npairs;
+    int dstat = 0;
+    PL_CUDA_TRY(cudaMemcpyAsync(&dstat, d_status, sizeof(int), cudaMemcpyDeviceToHost, stream));
+    PL_CUDA_TRY(cudaStreamSynchronize(stream));
+    if (dstat != 0) return record_status(dstat, "pl_commutator_noalloc: device-side check");
     return record_status(PL_OK, nullptr);
 }
