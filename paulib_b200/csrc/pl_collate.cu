@@ -40,8 +40,6 @@ namespace pl {
 namespace {
 
 constexpr int kThreads = 256;
-constexpr int kItems = 16;
-constexpr int kTile = kThreads * kItems;    // 4096 terms per segment / emit tile
 constexpr int kRItems = 8;
 constexpr int kRTile = kThreads * kRItems;  // 2048 keys per radix tile
 constexpr int kRadix = 256;
@@ -50,7 +48,6 @@ constexpr u32 kIdxMask = 0x7fffffffu;
 constexpr u32 kSentinel = 0xffffffffu;
 constexpr int kMaxFields = 2 * kMaxAS + 1;
 constexpr int kMaxPasses = 72;
-constexpr int kShortSeg = 32;
 constexpr u32 kFlagAgg = 1u << 30;
 constexpr u32 kFlagPre = 2u << 30;
 constexpr u32 kCountMask = (1u << 30) - 1;
@@ -572,23 +569,41 @@ struct SegCtx {
     int mode;
 };
 
+// Keep-filter applied when a segment is closed.  With on = 1 the zero and
+// cutoff filters are decided here and every warp adds its survivors to the
+// count of its kETile-term tile, so the emit pass needs no look-back; with
+// on = 0 (a weight filter, which needs the unpacked key) every head is
+// marked kept and the emit pass filters.
+struct FoldFilter {
+    int on;
+    double cutoff;
+    u32* tile_kept;
+};
+
 // Segment fold.  A warp owns 1024 consecutive sorted terms, staged in shared
 // memory; lane L folds its own 32 terms left to right (32 independent
-// chains per warp), and a second, lane-serial phase folds each lane's
-// prefix (the tail of the segment carried in from its left neighbour) onto
-// that carry.  Every segment is therefore summed in exactly the reference's
-// left-to-right order (PauliSumOperations.h:443-455).  The warp that holds a
-// segment's head owns it; an owned segment still open at the end of the
-// range is continued chunk by chunk (up to kExtChunks) and otherwise handed
-// to k_long_segments.  Results go to segval[head], segflag[head] = 1
-// (2 = long, pending); non-heads get segflag 0.
+// chains per warp).  Carries then cross lane borders: a lane holding a head
+// is resolved at once, a headless lane continues its left neighbour's open
+// segment over its whole span as soon as that neighbour is resolved, and
+// finally each lane folds its prefix (the terms before its first head) onto
+// the carry it received and closes that segment.  Every segment is therefore
+// summed in exactly the reference's left-to-right order
+// (PauliSumOperations.h:443-455).  The warp that holds a segment's head owns
+// it; an owned segment still open at the end of the range is continued chunk
+// by chunk (up to kExtChunks) and otherwise handed to the long-run kernels.
+// segflag[head] = 1 kept, 3 dropped, 2 long (pending); non-heads get 0.
+// wfirst[warp] = offset of the range's first head, kNoHead if none.
 constexpr int kFoldWarps = 4;
 constexpr int kLaneSpan = 32;
 constexpr u32 kFoldSpan = 32u * kLaneSpan;  // 1024 terms per warp
 constexpr u32 kFoldSlots = 33u * 32u;       // lane spans padded to 33 slots (no bank conflicts)
 constexpr int kExtChunks = 32;              // at most 1024 more
-constexpr size_t kFoldWarpSmem = kFoldSlots * (8 + 4 + 1);
+constexpr size_t kFoldWarpSmem = kFoldSlots * (8 + 1);  // value, head | sign << 1
 constexpr size_t kFoldSmem = ((kFoldWarpSmem + 15) & ~size_t(15)) * kFoldWarps;
+constexpr u32 kNoHead = 0xffffffffu;
+constexpr u32 kPiece = 4096;  // terms per partial sum of a long run
+constexpr int kEItems = 8;
+constexpr u32 kETile = kThreads * kEItems;  // 2048 terms per emit tile
 
 __device__ __forceinline__ bool lane_same_key(const SegCtx& C, u32 e, u64 ke, u64 kprev,
                                               u32 pe, u32 pprev) {
@@ -604,6 +619,8 @@ __device__ __forceinline__ bool lane_same_key(const SegCtx& C, u32 e, u64 ke, u6
     return true;
 }
 
+// One term onto a running sum: kCanon folds the sign into the value, kProp
+// keeps the sign-0 and sign-1 sums apart (S0 - S1 at the close).
 template <int MODE>
 __device__ __forceinline__ void fold_add(double& r0, double& r1, double v, u32 p) {
     const bool neg = (p >> 31) != 0;
@@ -613,17 +630,31 @@ __device__ __forceinline__ void fold_add(double& r0, double& r1, double v, u32 p
     else r0 = dadd(r0, v);
 }
 
+// The same for a staged term whose kCanon value already carries its sign.
 template <int MODE>
-__device__ __forceinline__ void fold_close(double* segval, u8* segflag, i64 h, double r0,
-                                           double r1) {
-    segval[h] = MODE == kProp ? dadd(r0, -r1) : r0;
-    segflag[h] = 1;
+__device__ __forceinline__ void fold_term(double& r0, double& r1, double v, u32 neg) {
+    if (MODE == kProp && neg) r1 = dadd(r1, v);
+    else r0 = dadd(r0, v);
 }
 
 template <int MODE>
-__global__ void __launch_bounds__(32 * kFoldWarps) k_fold(SegCtx C, double* segval,
-                                                          u8* segflag, u32* long_list,
-                                                          u32* counters) {
+__device__ __forceinline__ u32 fold_close(double* segval, u8* segflag, i64 h, double r0,
+                                          double r1, const FoldFilter& F) {
+    const double v = MODE == kProp ? dadd(r0, -r1) : r0;
+    segval[h] = v;
+    bool keep = true;
+    if (F.on) {
+        keep = (MODE == kCombine) || (v != 0.0);
+        if (F.cutoff > 0.0) keep = keep && (fabs(v) >= F.cutoff);
+    }
+    segflag[h] = keep ? 1 : 3;
+    return keep ? 1u : 0u;
+}
+
+template <int MODE>
+__global__ void __launch_bounds__(32 * kFoldWarps)
+    k_fold(SegCtx C, double* segval, u8* segflag, u32* wfirst, u32* long_list, u32* counters,
+           FoldFilter F) {
     extern __shared__ __align__(16) unsigned char fsm[];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const u32 gwarp = blockIdx.x * kFoldWarps + warp;
@@ -633,8 +664,7 @@ __global__ void __launch_bounds__(32 * kFoldWarps) k_fold(SegCtx C, double* segv
     const u32 cnt = w1 - w0;
     unsigned char* base = fsm + ((kFoldWarpSmem + 15) & ~size_t(15)) * warp;
     double* sv = reinterpret_cast<double*>(base);
-    u32* sp = reinterpret_cast<u32*>(base + 8 * kFoldSlots);
-    u8* sh = base + 12 * kFoldSlots;
+    u8* sh = base + 8 * kFoldSlots;
     // ---- staging: coalesced loads, head flags, non-head segflag = 0
     u64 ck = 0;
     u32 cp = 0;
@@ -642,6 +672,7 @@ __global__ void __launch_bounds__(32 * kFoldWarps) k_fold(SegCtx C, double* segv
         ck = C.keys[w0 - 1];
         cp = C.pay[w0 - 1];
     }
+    u32 first = kNoHead;
     // 8 chunks of loads in flight per lane, then the head flags of those chunks
     constexpr int kBatch = 8;
     for (u32 c0 = 0; c0 * 32 < cnt; c0 += kBatch) {
@@ -667,173 +698,319 @@ __global__ void __launch_bounds__(32 * kFoldWarps) k_fold(SegCtx C, double* segv
                 kp = ck;
                 pp = cp;
             }
+            bool head = false;
             if (i < cnt) {
-                const bool head = (e == 0) || !lane_same_key(C, e, ke[b], kp, pe[b], pp);
+                head = (e == 0) || !lane_same_key(C, e, ke[b], kp, pe[b], pp);
+                const u32 neg = pe[b] >> 31;
                 const u32 slot = c * 33 + lane;
-                sh[slot] = head;
-                sp[slot] = pe[b];
-                sv[slot] = ve[b];
+                sh[slot] = (u8)((head ? 1u : 0u) | (neg << 1));
+                sv[slot] = (MODE == kCanon && neg) ? -ve[b] : ve[b];
                 if (!head) segflag[e] = 0;
             }
+            const u32 hb = __ballot_sync(0xffffffffu, head);
+            if (first == kNoHead && hb) first = c * 32 + (u32)(__ffs(hb) - 1);
             ck = __shfl_sync(0xffffffffu, ke[b], 31);
             cp = __shfl_sync(0xffffffffu, pe[b], 31);
         }
     }
+    if (lane == 0) wfirst[gwarp] = first;
     __syncwarp();
     // ---- phase 1: each lane folds the segments that start inside its span
     const u32 a = (u32)lane * kLaneSpan;
     const u32 sa = (u32)lane * 33u;
     const u32 lcnt = cnt > a ? min(cnt - a, (u32)kLaneSpan) : 0u;
-    u32 first_head = lcnt;  // prefix length (terms before the lane's first head)
+    u32 fh = lcnt;  // prefix length (terms before the lane's first head)
     i64 h = -1;
     double r0 = 0.0, r1 = 0.0;
+    u32 kept = 0;
     for (u32 i = 0; i < lcnt; ++i) {
-        if (sh[sa + i]) {
-            if (h >= 0) fold_close<MODE>(segval, segflag, h, r0, r1);
-            else first_head = i;
+        const u32 s = sh[sa + i];
+        const double v = sv[sa + i];
+        if (s & 1u) {
+            if (h >= 0) kept += fold_close<MODE>(segval, segflag, h, r0, r1, F);
+            else fh = i;
             h = (i64)(w0 + a + i);
             r0 = 0.0;
             r1 = 0.0;
         }
-        if (h >= 0) fold_add<MODE>(r0, r1, sv[sa + i], sp[sa + i]);
+        if (h >= 0) fold_term<MODE>(r0, r1, v, s >> 1);
     }
-    // ---- phase 2: lane-serial carry of the segment crossing lane borders
-    i64 ch = -1;  // head of the carried segment (-1: owned by an earlier warp)
-    double c0 = 0.0, c1 = 0.0;
-    for (int L = 0; L < 32; ++L) {
-        i64 nh = ch;
-        double n0 = c0, n1 = c1;
-        if (lane == L && lcnt) {
-            for (u32 i = 0; i < first_head; ++i) fold_add<MODE>(n0, n1, sv[sa + i], sp[sa + i]);
-            if (first_head < lcnt) {
-                if (ch >= (i64)w0) fold_close<MODE>(segval, segflag, ch, n0, n1);
-                nh = h;
-                n0 = r0;
-                n1 = r1;
+    // ---- phase 2: carries across lane borders.  (oh, o0, o1) is the segment
+    // open at the end of the lane's span; oh = -1 when it belongs to an
+    // earlier warp.
+    const bool hh = fh < lcnt;
+    i64 oh = hh ? h : -1;
+    double o0 = hh ? r0 : 0.0, o1 = hh ? r1 : 0.0;
+    bool ready = hh || lane == 0;
+    for (int it = 0; it < 32; ++it) {
+        if (__all_sync(0xffffffffu, ready)) break;
+        const i64 ph = __shfl_up_sync(0xffffffffu, oh, 1);
+        const double p0 = __shfl_up_sync(0xffffffffu, o0, 1);
+        const double p1 = __shfl_up_sync(0xffffffffu, o1, 1);
+        const int pr = __shfl_up_sync(0xffffffffu, (int)ready, 1);
+        if (!ready && pr) {
+            oh = ph;
+            o0 = p0;
+            o1 = p1;
+            if (ph >= 0)
+                for (u32 i = 0; i < lcnt; ++i) fold_term<MODE>(o0, o1, sv[sa + i], sh[sa + i] >> 1);
+            ready = true;
+        }
+    }
+    {
+        i64 cin = __shfl_up_sync(0xffffffffu, oh, 1);
+        double q0 = __shfl_up_sync(0xffffffffu, o0, 1);
+        double q1 = __shfl_up_sync(0xffffffffu, o1, 1);
+        if (lane == 0) cin = -1;
+        if (hh && cin >= 0) {
+            for (u32 i = 0; i < fh; ++i) fold_term<MODE>(q0, q1, sv[sa + i], sh[sa + i] >> 1);
+            kept += fold_close<MODE>(segval, segflag, cin, q0, q1, F);
+        }
+    }
+    const i64 ch = __shfl_sync(0xffffffffu, oh, 31);
+    double c0 = __shfl_sync(0xffffffffu, o0, 31);
+    double c1 = __shfl_sync(0xffffffffu, o1, 31);
+    // ---- the open segment at the end of the range, when this warp owns it
+    if (ch >= 0) {
+        if (w1 == C.n) {
+            if (lane == 0) kept += fold_close<MODE>(segval, segflag, ch, c0, c1, F);
+        } else {
+            // extension: continue past the range, 32 terms at a time
+            ck = C.keys[w1 - 1];
+            cp = C.pay[w1 - 1];
+            for (int ext = 0;; ++ext) {
+                const u32 cb = w1 + (u32)ext * 32u;
+                if (cb >= C.n) {
+                    if (lane == 0) kept += fold_close<MODE>(segval, segflag, ch, c0, c1, F);
+                    break;
+                }
+                if (ext >= kExtChunks) {
+                    if (lane == 0) {
+                        segflag[ch] = 2;
+                        long_list[atomicAdd(&counters[2], 1u)] = (u32)ch;
+                    }
+                    break;
+                }
+                const u32 e = cb + lane;
+                const bool valid = e < C.n;
+                const u64 ke = valid ? C.keys[e] : 0ull;
+                const u32 pe = valid ? C.pay[e] : 0u;
+                const double ve = valid ? C.vals[e] : 0.0;
+                u64 kp = __shfl_up_sync(0xffffffffu, ke, 1);
+                u32 pp = __shfl_up_sync(0xffffffffu, pe, 1);
+                if (lane == 0) {
+                    kp = ck;
+                    pp = cp;
+                }
+                const bool head = valid && !lane_same_key(C, e, ke, kp, pe, pp);
+                const u32 hb = __ballot_sync(0xffffffffu, head || !valid);
+                const u32 lim = hb ? (u32)(__ffs(hb) - 1) : 32u;
+                // the tail lanes [0, lim) continue the segment, in order
+                for (u32 k = 0; k < lim; ++k) {
+                    const double vk = __shfl_sync(0xffffffffu, ve, k);
+                    const u32 pk = __shfl_sync(0xffffffffu, pe, k);
+                    fold_add<MODE>(c0, c1, vk, pk);
+                }
+                if (lim < 32) {
+                    if (lane == 0) kept += fold_close<MODE>(segval, segflag, ch, c0, c1, F);
+                    break;
+                }
+                ck = __shfl_sync(0xffffffffu, ke, 31);
+                cp = __shfl_sync(0xffffffffu, pe, 31);
             }
         }
-        ch = __shfl_sync(0xffffffffu, nh, L);
-        c0 = __shfl_sync(0xffffffffu, n0, L);
-        c1 = __shfl_sync(0xffffffffu, n1, L);
     }
-    if (ch < (i64)w0) return;  // the open segment belongs to an earlier warp
-    if (w1 == C.n) {
-        if (lane == 0) fold_close<MODE>(segval, segflag, ch, c0, c1);
-        return;
-    }
-    // ---- extension: continue the owned open segment past the range
-    ck = C.keys[w1 - 1];
-    cp = C.pay[w1 - 1];
-    int ext = 0;
-    for (u32 cb = w1;; cb += 32) {
-        if (cb >= C.n) {
-            if (lane == 0) fold_close<MODE>(segval, segflag, ch, c0, c1);
-            return;
-        }
-        if (++ext > kExtChunks) {
-            if (lane == 0) {
-                segflag[ch] = 2;
-                long_list[atomicAdd(&counters[2], 1u)] = (u32)ch;
-            }
-            return;
-        }
-        const u32 e = cb + lane;
-        const bool valid = e < C.n;
-        const u64 ke = valid ? C.keys[e] : 0ull;
-        const u32 pe = valid ? C.pay[e] : 0u;
-        const double ve = valid ? C.vals[e] : 0.0;
-        u64 kp = __shfl_up_sync(0xffffffffu, ke, 1);
-        u32 pp = __shfl_up_sync(0xffffffffu, pe, 1);
-        if (lane == 0) {
-            kp = ck;
-            pp = cp;
-        }
-        const bool head = valid && !lane_same_key(C, e, ke, kp, pe, pp);
-        const u32 hb = __ballot_sync(0xffffffffu, head || !valid);
-        const u32 lim = hb ? (u32)(__ffs(hb) - 1) : 32u;
-        // the tail lanes [0, lim) continue the segment, in order
-        double q0 = c0, q1 = c1;
-        for (u32 k = 0; k < lim; ++k) {
-            const double vk = __shfl_sync(0xffffffffu, ve, k);
-            const u32 pk = __shfl_sync(0xffffffffu, pe, k);
-            fold_add<MODE>(q0, q1, vk, pk);
-        }
-        c0 = q0;
-        c1 = q1;
-        if (lim < 32) {
-            if (lane == 0) fold_close<MODE>(segval, segflag, ch, c0, c1);
-            return;
-        }
-        ck = __shfl_sync(0xffffffffu, ke, 31);
-        cp = __shfl_sync(0xffffffffu, pe, 31);
+    if (F.on) {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) kept += __shfl_xor_sync(0xffffffffu, kept, o);
+        if (lane == 0 && kept) atomicAdd(&F.tile_kept[w0 / kETile], kept);
     }
 }
 
-// Long runs: one CTA per run.  The run ends at the next term whose segflag
-// is set (every head has one after k_fold); thread t sums elements t,
-// t+256, ... in order and the 256 partial sums are combined by a fixed
-// binary tree -- a deterministic order for a given run.
-__global__ void __launch_bounds__(kThreads) k_long_segments(SegCtx C, const u32* long_list,
-                                                            const u32* counters, double* segval,
-                                                            u8* segflag) {
-    __shared__ double s0[kThreads], s1[kThreads];
-    __shared__ u32 s_end;
+// Long runs (segflag 2): a run [h, end) ends at the next head, found in the
+// per-warp first-head table; it is cut into kPiece-term pieces.  One warp
+// per run.  counters: [2] runs.
+__global__ void __launch_bounds__(256) k_long_ends(const u32* wfirst, u32 ngw, u32 n,
+                                                   const u32* long_list, const u32* counters,
+                                                   u32* long_end, u32* long_np) {
     const u32 nlong = counters[2];
-    for (u32 li = blockIdx.x; li < nlong; li += gridDim.x) {
-        const u32 b = long_list[li];
-        if (threadIdx.x == 0) s_end = C.n;
-        __syncthreads();
-        // scan 4096 flags per step, 16-byte aligned groups of 16 per thread
-        for (u32 base = (b + 1) & ~15u; base < C.n; base += kThreads * 16) {
-            u32 mine = C.n;
-            const u32 lo = base + threadIdx.x * 16;
-            if (lo + 16 <= C.n) {
-                const uint4 q = *reinterpret_cast<const uint4*>(segflag + lo);
-                const u32 w[4] = {q.x, q.y, q.z, q.w};
+    const int lane = threadIdx.x & 31;
+    const u32 nw = (gridDim.x * blockDim.x) >> 5;
+    for (u32 li = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; li < nlong; li += nw) {
+        const u32 h = long_list[li];
+        u32 end = n;
+        for (u32 g0 = h / kFoldSpan + 1; g0 < ngw; g0 += 32u * 8u) {
+            u32 f[8];
 #pragma unroll
-                for (int j = 0; j < 16; ++j)
-                    if (mine == C.n && lo + j > b && ((w[j >> 2] >> (8 * (j & 3))) & 0xffu))
-                        mine = lo + j;
-            } else {
-                for (u32 j = 0; j < 16 && lo + j < C.n; ++j)
-                    if (lo + j > b && segflag[lo + j]) {
-                        mine = lo + j;
-                        break;
-                    }
+            for (int b = 0; b < 8; ++b) {
+                const u32 g = g0 + (u32)b * 32u + lane;
+                f[b] = g < ngw ? wfirst[g] : kNoHead;
             }
-            if (mine < C.n) atomicMin(&s_end, mine);
-            __syncthreads();
-            const bool found = s_end < C.n;
-            __syncthreads();
-            if (found) break;
-        }
-        const u32 e = s_end;
-        double a0 = 0.0, a1 = 0.0;
-        for (u32 t = b + threadIdx.x; t < e; t += kThreads) {
-            const u32 p = C.pay[t];
-            const double v = C.vals[t];
-            const bool neg = (p >> 31) != 0;
-            if (C.mode == kCanon) a0 = dadd(a0, neg ? -v : v);
-            else if (C.mode == kCombine) a0 = dadd(a0, v);
-            else if (neg) a1 = dadd(a1, v);
-            else a0 = dadd(a0, v);
-        }
-        s0[threadIdx.x] = a0;
-        s1[threadIdx.x] = a1;
-        __syncthreads();
-        for (int st = kThreads / 2; st > 0; st >>= 1) {
-            if ((int)threadIdx.x < st) {
-                s0[threadIdx.x] = dadd(s0[threadIdx.x], s0[threadIdx.x + st]);
-                s1[threadIdx.x] = dadd(s1[threadIdx.x], s1[threadIdx.x + st]);
+            u32 found = kNoHead;
+#pragma unroll
+            for (int b = 0; b < 8; ++b) {
+                const u32 bal = __ballot_sync(0xffffffffu, f[b] != kNoHead);
+                if (found == kNoHead && bal) {
+                    const int l = __ffs(bal) - 1;
+                    found = (g0 + (u32)b * 32u + (u32)l) * kFoldSpan +
+                            __shfl_sync(0xffffffffu, f[b], l);
+                }
             }
-            __syncthreads();
+            if (found != kNoHead) {
+                end = found;
+                break;
+            }
         }
-        if (threadIdx.x == 0) {
-            segval[b] = C.mode == kProp ? dadd(s0[0], -s1[0]) : s0[0];
-            segflag[b] = 1;
+        if (lane == 0) {
+            long_end[li] = end;
+            long_np[li] = (end - h + kPiece - 1) / kPiece;
+        }
+    }
+}
+
+// Block-wide exclusive scan of one value per thread (NW warps).
+template <int NW>
+__device__ __forceinline__ u32 block_scan_n(u32 v, u32* s_warp, u32& total) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    u32 inc = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const u32 t = __shfl_up_sync(0xffffffffu, inc, o);
+        if (lane >= o) inc += t;
+    }
+    if (lane == 31) s_warp[warp] = inc;
+    __syncthreads();
+    if (warp == 0) {
+        const u32 c = lane < NW ? s_warp[lane] : 0u;
+        u32 ci = c;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const u32 t = __shfl_up_sync(0xffffffffu, ci, o);
+            if (lane >= o) ci += t;
+        }
+        if (lane < NW) s_warp[32 + lane] = ci - c;
+        if (lane == 31) s_warp[64] = ci;
+    }
+    __syncthreads();
+    total = s_warp[64];
+    const u32 r = s_warp[32 + warp] + inc - v;
+    __syncthreads();
+    return r;
+}
+
+// Piece offsets of the long runs (exclusive scan of long_np; one CTA).
+// counters: [4] pieces.
+__global__ void __launch_bounds__(1024) k_long_scan(const u32* long_np, u32* long_poff,
+                                                    u32* long_tick, u32* counters) {
+    __shared__ u32 sw[65];
+    const u32 nlong = counters[2];
+    const u32 per = (nlong + 1023u) / 1024u;
+    const u32 b = threadIdx.x * per, e = min(b + per, nlong);
+    u32 s = 0;
+    for (u32 i = b; i < e; ++i) s += long_np[i];
+    u32 total;
+    u32 run = block_scan_n<32>(s, sw, total);
+    for (u32 i = b; i < e; ++i) {
+        long_poff[i] = run;
+        run += long_np[i];
+        long_tick[i] = 0;
+    }
+    if (threadIdx.x == 0) {
+        long_poff[nlong] = total;
+        counters[4] = total;
+    }
+}
+
+// One CTA per piece: thread t sums terms t, t+256, ... of the piece in order
+// and the partial sums meet in a fixed binary tree; the last piece of a run
+// to finish sums the run's pieces the same way and closes the run.  The
+// order depends only on the run, so results are deterministic.
+template <int MODE>
+__device__ __forceinline__ void tree_sum(double* s0, double* s1, double a0, double a1) {
+    s0[threadIdx.x] = a0;
+    s1[threadIdx.x] = a1;
+    __syncthreads();
+    for (int st = kThreads / 2; st > 0; st >>= 1) {
+        if ((int)threadIdx.x < st) {
+            s0[threadIdx.x] = dadd(s0[threadIdx.x], s0[threadIdx.x + st]);
+            if (MODE == kProp) s1[threadIdx.x] = dadd(s1[threadIdx.x], s1[threadIdx.x + st]);
         }
         __syncthreads();
     }
+}
+
+template <int MODE>
+__global__ void __launch_bounds__(kThreads)
+    k_long_pieces(SegCtx C, const u32* long_list, const u32* long_end, const u32* long_poff,
+                  u32* long_tick, const u32* counters, double* partials, double* segval,
+                  u8* segflag, FoldFilter F) {
+    __shared__ double s0[kThreads], s1[kThreads];
+    __shared__ u32 s_last;
+    constexpr int kPer = kPiece / kThreads;
+    const u32 nlong = counters[2], npieces = counters[4];
+    for (u32 p = blockIdx.x; p < npieces; p += gridDim.x) {
+        u32 lo = 0, hi = nlong;  // long_poff[lo] <= p < long_poff[hi]
+        while (hi - lo > 1) {
+            const u32 mid = (lo + hi) >> 1;
+            if (long_poff[mid] <= p) lo = mid;
+            else hi = mid;
+        }
+        const u32 h = long_list[lo], end = long_end[lo];
+        const u32 pb = long_poff[lo], pe = long_poff[lo + 1];
+        const u32 s = h + (p - pb) * kPiece, e = min(s + kPiece, end);
+        u32 q[kPer];
+        double v[kPer];
+#pragma unroll
+        for (int j = 0; j < kPer; ++j) {
+            const u32 t = s + threadIdx.x + (u32)j * kThreads;
+            q[j] = t < e ? C.pay[t] : 0u;
+            v[j] = t < e ? C.vals[t] : 0.0;
+        }
+        double a0 = 0.0, a1 = 0.0;
+#pragma unroll
+        for (int j = 0; j < kPer; ++j)
+            if (s + threadIdx.x + (u32)j * kThreads < e) fold_add<MODE>(a0, a1, v[j], q[j]);
+        tree_sum<MODE>(s0, s1, a0, a1);
+        if (threadIdx.x == 0) {
+            partials[2 * (size_t)p] = s0[0];
+            partials[2 * (size_t)p + 1] = s1[0];
+            __threadfence();
+            s_last = (atomicAdd(&long_tick[lo], 1u) + 1u == pe - pb) ? 1u : 0u;
+        }
+        __syncthreads();
+        if (s_last) {
+            __threadfence();
+            double b0 = 0.0, b1 = 0.0;
+            for (u32 r = pb + threadIdx.x; r < pe; r += kThreads) {
+                b0 = dadd(b0, __ldcg(partials + 2 * (size_t)r));
+                b1 = dadd(b1, __ldcg(partials + 2 * (size_t)r + 1));
+            }
+            tree_sum<MODE>(s0, s1, b0, b1);
+            if (threadIdx.x == 0) {
+                const u32 keep = fold_close<MODE>(segval, segflag, h, s0[0], s1[0], F);
+                if (F.on && keep) atomicAdd(&F.tile_kept[h / kETile], 1u);
+            }
+        }
+        __syncthreads();
+    }
+}
+
+// Output offsets of the emit tiles (exclusive scan of the kept counts; one
+// CTA) and the output size.
+__global__ void __launch_bounds__(1024) k_tile_scan(const u32* tile_kept, u32 tiles,
+                                                    u32* tile_off, i64* d_out_count) {
+    __shared__ u32 sw[65];
+    const u32 per = (tiles + 1023u) / 1024u;
+    const u32 b = threadIdx.x * per, e = min(b + per, tiles);
+    u32 s = 0;
+    for (u32 i = b; i < e; ++i) s += tile_kept[i];
+    u32 total;
+    u32 run = block_scan_n<32>(s, sw, total);
+    for (u32 i = b; i < e; ++i) {
+        tile_off[i] = run;
+        run += tile_kept[i];
+    }
+    if (threadIdx.x == 0) *d_out_count = (i64)total;
 }
 
 struct SegSmem {
@@ -851,7 +1028,7 @@ __global__ void __launch_bounds__(256) k_gather_values(Src src, const u32* pay, 
 }
 
 // ---------------------------------------------------------------------------
-// 5. Emit: keep-filter + order-preserving compaction into the output.
+// 5. Emit: order-preserving compaction of the kept heads into the output.
 // ---------------------------------------------------------------------------
 template <int AS, class Src>
 __device__ __forceinline__ void emit_key(const Src& src, const KeyLayout& L, u64 packed,
@@ -868,39 +1045,103 @@ __device__ __forceinline__ void emit_key(const Src& src, const KeyLayout& L, u64
 }
 
 template <int AS, class Src>
+__device__ __forceinline__ void emit_term(const Src& src, const KeyLayout& L, u64 packed,
+                                          const u32* pay, u32 e, int mode, double v, i64 o,
+                                          const SoAOut& out, int* status) {
+    if (o >= out.capacity) {
+        raise_status(status, PL_ERR_CAPACITY);
+        return;
+    }
+    u64 xw[AS], zw[AS];
+    u32 f;
+    emit_key<AS>(src, L, packed, pay, e, mode, xw, zw, f);
+#pragma unroll
+    for (int k = 0; k < AS; ++k) {
+        out.x[(i64)k * out.capacity + o] = xw[k];
+        out.z[(i64)k * out.capacity + o] = zw[k];
+    }
+    out.f[o] = (u8)f;
+    out.v[o] = v;
+}
+
+// Filters decided by the fold (segflag 1 = kept): each tile writes at the
+// offset k_tile_scan gave it.  Warp-striped items; all flags are loaded
+// before any value so the loads overlap.
+template <int AS, class Src>
+__global__ void __launch_bounds__(kThreads)
+    k_emit_counted(Src src, KeyLayout L, const u64* keys, const u32* pay, const double* segval,
+                   const u8* segflag, u32 n, const u32* tile_off, int mode, SoAOut out,
+                   int* status) {
+    __shared__ u32 swarp[kWarps];
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const u32 tile = blockIdx.x;
+    const u32 wbase = tile * kETile + (u32)warp * (kEItems * 32);
+    u32 keepmask = 0;
+#pragma unroll
+    for (int t = 0; t < kEItems; ++t) {
+        const u32 e = wbase + t * 32 + lane;
+        if (e < n && segflag[e] == 1) keepmask |= 1u << t;
+    }
+    double v[kEItems];
+    u64 kk[kEItems];
+#pragma unroll
+    for (int t = 0; t < kEItems; ++t) {
+        const bool k = (keepmask >> t) & 1u;
+        v[t] = k ? segval[wbase + t * 32 + lane] : 0.0;
+        kk[t] = k ? keys[wbase + t * 32 + lane] : 0ull;
+    }
+    u32 wcount = 0;
+    u32 myoff[kEItems];
+#pragma unroll
+    for (int t = 0; t < kEItems; ++t) {
+        const u32 bal = __ballot_sync(0xffffffffu, (keepmask >> t) & 1u);
+        myoff[t] = wcount + __popc(bal & lanemask_lt());
+        wcount += __popc(bal);
+    }
+    u32 total;
+    const u32 wexcl = block_excl_scan(lane == 0 ? wcount : 0u, swarp, total);
+    const u32 base_o = tile_off[tile] + __shfl_sync(0xffffffffu, wexcl, 0);
+#pragma unroll
+    for (int t = 0; t < kEItems; ++t)
+        if ((keepmask >> t) & 1u)
+            emit_term<AS>(src, L, kk[t], pay, wbase + t * 32 + lane, mode, v[t],
+                          (i64)base_o + myoff[t], out, status);
+}
+
+// All filters here (the weight filter needs the unpacked key), with a
+// decoupled look-back across tiles for the output offsets.  counters: [3]
+// tile counter.
+template <int AS, class Src>
 __global__ void __launch_bounds__(kThreads) k_emit(Src src, KeyLayout L, const u64* keys,
                                                    const u32* pay, const double* segval,
                                                    const u8* segflag, u32 n, u32* counters,
                                                    u32* lb, int mode, double cutoff,
                                                    u64 max_weight, SoAOut out, i64* d_out_count,
                                                    int* status) {
-    // Heads (segflag set) that survive the filters are compacted in order.
-    // Warp-striped items: coalesced loads; all flags are loaded before any
-    // value so the loads overlap.  counters: [3] tile ctr.
     __shared__ SegSmem S;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     if (tid == 0) S.tile = atomicAdd(&counters[3], 1u);
     __syncthreads();
     const u32 tile = S.tile;
-    const u32 wbase = tile * (u32)kTile + (u32)warp * (kItems * 32);
+    const u32 wbase = tile * kETile + (u32)warp * (kEItems * 32);
     u32 headmask = 0;
 #pragma unroll
-    for (int t = 0; t < kItems; ++t) {
+    for (int t = 0; t < kEItems; ++t) {
         const u32 e = wbase + t * 32 + lane;
         if (e < n && segflag[e]) headmask |= 1u << t;
     }
-    double v[kItems];
-    u64 kk[kItems];
+    double v[kEItems];
+    u64 kk[kEItems];
 #pragma unroll
-    for (int t = 0; t < kItems; ++t) {
+    for (int t = 0; t < kEItems; ++t) {
         const bool hd = (headmask >> t) & 1u;
         v[t] = hd ? segval[wbase + t * 32 + lane] : 0.0;
         kk[t] = hd ? keys[wbase + t * 32 + lane] : 0ull;
     }
     u32 keepmask = 0, wcount = 0;
-    u32 myoff[kItems];
+    u32 myoff[kEItems];
 #pragma unroll
-    for (int t = 0; t < kItems; ++t) {
+    for (int t = 0; t < kEItems; ++t) {
         const u32 e = wbase + t * 32 + lane;
         bool keep = false;
         if ((headmask >> t) & 1u) {
@@ -928,25 +1169,10 @@ __global__ void __launch_bounds__(kThreads) k_emit(Src src, KeyLayout L, const u
     __syncthreads();
     const u32 base_o = S.excl + wpre;
 #pragma unroll
-    for (int t = 0; t < kItems; ++t) {
-        if (!((keepmask >> t) & 1u)) continue;
-        const u32 e = wbase + t * 32 + lane;
-        const i64 o = (i64)base_o + myoff[t];
-        if (o >= out.capacity) {
-            raise_status(status, PL_ERR_CAPACITY);
-            continue;
-        }
-        u64 xw[AS], zw[AS];
-        u32 f;
-        emit_key<AS>(src, L, kk[t], pay, e, mode, xw, zw, f);
-#pragma unroll
-        for (int k = 0; k < AS; ++k) {
-            out.x[(i64)k * out.capacity + o] = xw[k];
-            out.z[(i64)k * out.capacity + o] = zw[k];
-        }
-        out.f[o] = (u8)f;
-        out.v[o] = v[t];
-    }
+    for (int t = 0; t < kEItems; ++t)
+        if ((keepmask >> t) & 1u)
+            emit_term<AS>(src, L, kk[t], pay, wbase + t * 32 + lane, mode, v[t],
+                          (i64)base_o + myoff[t], out, status);
     if (tile == gridDim.x - 1 && tid == 0) *d_out_count = (i64)S.excl + total;
 }
 
@@ -955,40 +1181,78 @@ __global__ void __launch_bounds__(kThreads) k_emit(Src src, KeyLayout L, const u
 // ---------------------------------------------------------------------------
 inline size_t al(size_t b) { return (b + 255) & ~size_t(255); }
 
+// Bump allocator over the workspace; with base == nullptr it only measures.
 struct Carve {
-    unsigned char* p;
-    size_t left;
-    bool ok = true;
+    unsigned char* base;
+    size_t bytes;
+    size_t used = 0;
     template <class T>
     T* take(size_t count) {
         const size_t b = al(sizeof(T) * (count ? count : 1));
-        if (b > left) {
-            ok = false;
-            return nullptr;
-        }
-        T* r = reinterpret_cast<T*>(p);
-        p += b;
-        left -= b;
+        T* r = base ? reinterpret_cast<T*>(base + used) : nullptr;
+        used += b;
         return r;
     }
+    bool ok() const { return used <= bytes; }
 };
 
 int max_chunks(int as) { return (128 * as + 2 + 63) / 64; }
 
-size_t ws_for(int as, i64 n, int nch) {
-    const i64 tiles = (n + kTile - 1) / kTile + 1;
+struct Bufs {
+    u64 *ka, *kb, *planes;
+    u32 *pa, *pb, *hist, *lb, *counters;
+    u8* segflag;
+    double *seg_sum, *sv, *partials;
+    u32 *wfirst, *long_list, *long_end, *long_np, *long_poff, *long_tick;
+    u32 *tile_kept, *tile_off, *lb_emit;
+    u64 *orm, *andm;
+    i64* d_count;
+    int* d_status;
+};
+
+void carve_all(Carve& c, i64 n, int nch, Bufs& B) {
     const i64 rtiles = (n + kRTile - 1) / kRTile + 1;
-    size_t b = 0;
-    b += 2 * al(8 * n) + 2 * al(4 * n);                  // keys, payload (ping-pong)
-    b += al(8 * n);                                      // values in sorted order
-    b += nch > 1 ? al(8 * (size_t)n * nch) : al(8);     // chunk planes
-    b += al(4 * kMaxPasses * kRadix);                    // histograms / bucket starts
-    b += al(4 * (size_t)rtiles * kRadix);                // radix look-back (one pass)
-    b += al(4 * (n + 1)) + al(8 * n) + al(4 * n);         // seg_start, seg_sum, long list
-    b += 2 * al(4 * tiles);                              // segment / emit look-back
-    b += al(4 * (128 + 16 * kRadix));                    // counters + operand histograms
-    b += 2 * al(8 * kMaxFields) + al(8) + al(4);          // masks, out count, status
-    return b + 1024;
+    const i64 etiles = (n + kETile - 1) / kETile + 1;
+    const i64 ngw = (n + kFoldSpan - 1) / kFoldSpan + 16;  // fold warps; also bounds long runs
+    const i64 npieces = n / kPiece + ngw;
+    B.ka = c.take<u64>(n);
+    B.kb = c.take<u64>(n);
+    B.pa = c.take<u32>(n);
+    B.pb = c.take<u32>(n);
+    B.sv = c.take<double>(n);
+    B.planes = c.take<u64>(nch > 1 ? (size_t)n * nch : 1);
+    B.hist = c.take<u32>(kMaxPasses * kRadix);
+    B.lb = c.take<u32>((size_t)rtiles * kRadix);
+    B.segflag = c.take<u8>(n + 16);
+    B.seg_sum = c.take<double>(n);
+    B.wfirst = c.take<u32>(ngw);
+    B.long_list = c.take<u32>(ngw);
+    B.long_end = c.take<u32>(ngw);
+    B.long_np = c.take<u32>(ngw);
+    B.long_poff = c.take<u32>(ngw + 1);
+    B.long_tick = c.take<u32>(ngw);
+    B.partials = c.take<double>(2 * npieces);
+    B.tile_kept = c.take<u32>(etiles);
+    B.tile_off = c.take<u32>(etiles);
+    B.lb_emit = c.take<u32>(etiles);
+    B.counters = c.take<u32>(128 + 16 * kRadix);
+    B.orm = c.take<u64>(kMaxFields);
+    B.andm = c.take<u64>(kMaxFields);
+    B.d_count = c.take<i64>(1);
+    B.d_status = c.take<int>(1);
+}
+
+size_t ws_for(int, i64 n, int nch) {
+    Carve c{nullptr, ~size_t(0)};
+    Bufs B;
+    carve_all(c, n, nch, B);
+    return c.used + 1024;
+}
+
+bool carve(void* ws, size_t bytes, i64 n, int nch, Bufs& B) {
+    Carve c{reinterpret_cast<unsigned char*>(ws), bytes};
+    carve_all(c, n, nch, B);
+    return c.ok();
 }
 
 void build_layout(int as, int mode, const u64* orm, const u64* andm, KeyLayout& L, PassPlan& P) {
@@ -1030,38 +1294,30 @@ void build_layout(int as, int mode, const u64* orm, const u64* andm, KeyLayout& 
     P.npasses = np;
 }
 
-struct Bufs {
-    u64 *ka, *kb, *planes;
-    u32 *pa, *pb, *hist, *lb, *seg_start, *long_list, *lb_seg, *lb_emit, *counters;
-    double *seg_sum, *sv;
-    u64 *orm, *andm;
-    i64* d_count;
-    int* d_status;
-};
-
-bool carve(void* ws, size_t bytes, i64 n, int nch, Bufs& B) {
-    const i64 tiles = (n + kTile - 1) / kTile + 1;
-    const i64 rtiles = (n + kRTile - 1) / kRTile + 1;
-    Carve c{(unsigned char*)ws, bytes};
-    B.ka = c.take<u64>(n);
-    B.kb = c.take<u64>(n);
-    B.pa = c.take<u32>(n);
-    B.pb = c.take<u32>(n);
-    B.sv = c.take<double>(n);
-    B.planes = c.take<u64>(nch > 1 ? (size_t)n * nch : 1);
-    B.hist = c.take<u32>(kMaxPasses * kRadix);
-    B.lb = c.take<u32>((size_t)rtiles * kRadix);
-    B.seg_start = c.take<u32>(n + 1);
-    B.seg_sum = c.take<double>(n);
-    B.long_list = c.take<u32>(n);
-    B.lb_seg = c.take<u32>(tiles);
-    B.lb_emit = c.take<u32>(tiles);
-    B.counters = c.take<u32>(128 + 16 * kRadix);
-    B.orm = c.take<u64>(kMaxFields);
-    B.andm = c.take<u64>(kMaxFields);
-    B.d_count = c.take<i64>(1);
-    B.d_status = c.take<int>(1);
-    return c.ok;
+// Segment sums: the warp fold, then the long runs (ends, piece offsets,
+// pieces with the last piece of each run closing it).
+template <int MODE>
+int fold_segments(const SegCtx& C, Bufs& B, const FoldFilter& F, int nsm, cudaStream_t st) {
+    const u32 n = C.n;
+    const u32 ngw = (n + kFoldSpan - 1) / kFoldSpan;
+    const u32 fold_blocks = (ngw + kFoldWarps - 1) / kFoldWarps;
+    PL_CUDA_TRY(cudaFuncSetAttribute(k_fold<MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)kFoldSmem));
+    k_fold<MODE><<<fold_blocks, 32 * kFoldWarps, kFoldSmem, st>>>(
+        C, B.seg_sum, B.segflag, B.wfirst, B.long_list, B.counters, F), pl::note_launch();
+    // a long run is longer than kFoldSpan terms, so there are fewer than ngw
+    const int lw_blocks = (int)std::min<u32>((ngw + 7) / 8, (u32)nsm * 4);
+    k_long_ends<<<lw_blocks, 256, 0, st>>>(B.wfirst, ngw, n, B.long_list, B.counters,
+                                           B.long_end, B.long_np), pl::note_launch();
+    k_long_scan<<<1, 1024, 0, st>>>(B.long_np, B.long_poff, B.long_tick, B.counters),
+        pl::note_launch();
+    const u32 max_pieces = n / kPiece + ngw;
+    const int lp_blocks = (int)std::min<u32>(max_pieces, (u32)nsm * 8);
+    k_long_pieces<MODE><<<lp_blocks, kThreads, 0, st>>>(C, B.long_list, B.long_end, B.long_poff,
+                                                        B.long_tick, B.counters, B.partials,
+                                                        B.seg_sum, B.segflag, F),
+        pl::note_launch();
+    return PL_OK;
 }
 
 // Histograms that can be derived instead of counted: none for a plain sum.
@@ -1098,7 +1354,6 @@ template <int AS, class Src>
 int run_collate(const Src& src, u32 n, int mode, const KeyLayout& L, const PassPlan& P,
                 const CollateArgs& a, const SoAOut& out, i64* out_count, Bufs& B,
                 cudaStream_t st) {
-    const u32 tiles = (n + kTile - 1) / kTile;
     const u32 rtiles = (n + kRTile - 1) / kRTile;
     const int nsm = sm_count();
     PL_CUDA_TRY(cudaMemsetAsync(B.hist, 0, sizeof(u32) * kMaxPasses * kRadix, st));
@@ -1149,36 +1404,33 @@ int run_collate(const Src& src, u32 n, int mode, const KeyLayout& L, const PassP
     if (P.npasses == 0)
         k_gather_values<Src><<<gblocks, 256, 0, st>>>(src, vin, n, B.sv), pl::note_launch();
     SegCtx C{kin, vin, B.sv, B.planes, n, L.nchunks, L.seg_mask0, mode};
-    u8* segflag = reinterpret_cast<u8*>(B.seg_start);
-    const u32 fold_blocks = (n + kFoldSpan * kFoldWarps - 1) / (kFoldSpan * kFoldWarps);
-    PL_CUDA_TRY(cudaFuncSetAttribute(k_fold<kCanon>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     (int)kFoldSmem));
-    PL_CUDA_TRY(cudaFuncSetAttribute(k_fold<kCombine>,
-                                     cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kFoldSmem));
-    PL_CUDA_TRY(cudaFuncSetAttribute(k_fold<kProp>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     (int)kFoldSmem));
+    const u32 etiles = (n + kETile - 1) / kETile;
+    // Without a weight filter the fold decides the zero / cutoff filters and
+    // counts survivors per emit tile, so the emit needs no look-back.
+    const bool counted = a.max_weight == ~0ull;
+    const FoldFilter F{counted ? 1 : 0, a.cutoff, B.tile_kept};
+    if (counted) PL_CUDA_TRY(cudaMemsetAsync(B.tile_kept, 0, sizeof(u32) * etiles, st));
     e0 = timed_begin(st);
-    if (mode == kCanon)
-        k_fold<kCanon><<<fold_blocks, 32 * kFoldWarps, kFoldSmem, st>>>(
-            C, B.seg_sum, segflag, B.long_list, B.counters), pl::note_launch();
-    else if (mode == kCombine)
-        k_fold<kCombine><<<fold_blocks, 32 * kFoldWarps, kFoldSmem, st>>>(
-            C, B.seg_sum, segflag, B.long_list, B.counters), pl::note_launch();
-    else
-        k_fold<kProp><<<fold_blocks, 32 * kFoldWarps, kFoldSmem, st>>>(
-            C, B.seg_sum, segflag, B.long_list, B.counters), pl::note_launch();
+    int rc = PL_OK;
+    if (mode == kCanon) rc = fold_segments<kCanon>(C, B, F, nsm, st);
+    else if (mode == kCombine) rc = fold_segments<kCombine>(C, B, F, nsm, st);
+    else rc = fold_segments<kProp>(C, B, F, nsm, st);
+    if (rc != PL_OK) return rc;
     timed_end(e0, st, "k_fold", 20ull * n);
     e0 = timed_begin(st);
-    k_long_segments<<<nsm * 2, kThreads, 0, st>>>(C, B.long_list, B.counters, B.seg_sum,
-                                                  segflag), pl::note_launch();
-    timed_end(e0, st, "k_long_segments", 0ull);
-    // Emit over the segment count; the grid covers the worst case (n).
-    PL_CUDA_TRY(cudaMemsetAsync(B.lb_emit, 0, sizeof(u32) * tiles, st));
-    e0 = timed_begin(st);
-    k_emit<AS, Src><<<tiles, kThreads, 0, st>>>(src, L, kin, vin, B.seg_sum, segflag, n,
-                                                B.counters, B.lb_emit, mode, a.cutoff,
-                                                a.max_weight, out, B.d_count, B.d_status),
-        pl::note_launch();
+    if (counted) {
+        k_tile_scan<<<1, 1024, 0, st>>>(B.tile_kept, etiles, B.tile_off, B.d_count),
+            pl::note_launch();
+        k_emit_counted<AS, Src><<<etiles, kThreads, 0, st>>>(src, L, kin, vin, B.seg_sum,
+                                                             B.segflag, n, B.tile_off, mode, out,
+                                                             B.d_status), pl::note_launch();
+    } else {
+        PL_CUDA_TRY(cudaMemsetAsync(B.lb_emit, 0, sizeof(u32) * etiles, st));
+        k_emit<AS, Src><<<etiles, kThreads, 0, st>>>(src, L, kin, vin, B.seg_sum, B.segflag, n,
+                                                     B.counters, B.lb_emit, mode, a.cutoff,
+                                                     a.max_weight, out, B.d_count, B.d_status),
+            pl::note_launch();
+    }
     timed_end(e0, st, "k_emit", 0ull);
     PL_CUDA_TRY(cudaGetLastError());
     i64 cnt = 0;
