@@ -246,6 +246,79 @@ PL_API int pl_propagate(pl_state* state, const uint64_t* rot_x, const uint64_t* 
                  const uint8_t* rot_flags, const double* rot_theta, int64_t n_rot,
                  const int32_t* ops, int64_t n_ops, const pl_truncation* opts);
 
+/* State options (pl_state_set_option). */
+#define PL_OPT_GRAPHS 1  /* value != 0: runs of single-qubit rotations replay a captured
+                            CUDA graph of their kernel chain (gate records live in device
+                            memory, so one graph serves every run of that length) */
+PL_API int pl_state_set_option(pl_state* state, int option, int64_t value);
+/* Device bytes the state's buffers and workspace hold. */
+PL_API int pl_state_memory(pl_state* state, uint64_t* bytes);
+
+/* ---- many propagations on one device: batch and serving ---------------
+ *
+ * A job is one propagate_expectation (PauliPropagation.h:65-71): the
+ * observable is uploaded, propagated backwards through the circuit with
+ * truncation after every rotation, and reduced to zero_state_expectation.
+ * Jobs run on `lanes` device-resident states, each with its own stream and
+ * host thread, so the kernels of different jobs overlap on the GPU and the
+ * host-side waits of one job hide behind the work of others.  The buffers
+ * of all lanes count against an HBM budget: a lane that must grow past it
+ * waits for others to release memory.  Every job computes exactly what
+ * pl_propagate computes on its own: results do not depend on the mix. */
+typedef struct {
+    int array_size;
+    const uint64_t* obs_x;       /* host planes, stride obs_n */
+    const uint64_t* obs_z;
+    const uint8_t* obs_flags;
+    const double* obs_val;
+    int64_t obs_n;
+    const uint64_t* rot_x;       /* host planes, stride n_rot; rot_theta = angles */
+    const uint64_t* rot_z;
+    const uint8_t* rot_flags;
+    const double* rot_theta;
+    int64_t n_rot;
+    const int32_t* ops;          /* (kind, a, b) rows as for pl_propagate */
+    int64_t n_ops;
+    pl_truncation trunc;
+    double arrival_s;            /* pl_serve: seconds after its start the job arrives */
+} pl_job;
+
+typedef struct {
+    double expectation;          /* zero_state_expectation of the propagated sum */
+    int64_t final_terms;
+    int status;                  /* PL_OK or the job's error */
+    int lane;
+    double start_s;              /* seconds from the call's start */
+    double end_s;
+} pl_job_result;
+
+#define PL_ORDER_GIVEN 0
+#define PL_ORDER_LONGEST_FIRST 1  /* by estimated cost (rotations x words), descending */
+
+typedef struct {
+    int lanes;                   /* concurrent jobs, >= 1 */
+    int use_graphs;              /* PL_OPT_GRAPHS for every lane */
+    int order;                   /* pl_batch_propagate only */
+    uint64_t hbm_budget;         /* bytes all lanes may hold; 0 = 85% of free device memory */
+    uint64_t keep_bytes;         /* a lane keeps at most this between jobs; 0 = budget / lanes */
+    cudaStream_t sync_stream;    /* work queued here before the call completes first (or NULL) */
+} pl_batch_opts;
+
+typedef struct {
+    double wall_s;
+    uint64_t peak_bytes;         /* peak of the budgeted bytes */
+    uint64_t budget_waits;       /* times a lane waited for memory */
+    uint64_t jobs_failed;
+} pl_batch_stats;
+
+/* All jobs available at once. */
+PL_API int pl_batch_propagate(const pl_job* jobs, int64_t count, const pl_batch_opts* opts,
+                              pl_job_result* results, pl_batch_stats* stats);
+/* Jobs arrive at their arrival_s; each free lane takes the earliest arrived
+ * job (continuous batching).  Latency of job i = end_s - arrival_s. */
+PL_API int pl_serve(const pl_job* jobs, int64_t count, const pl_batch_opts* opts,
+                    pl_job_result* results, pl_batch_stats* stats);
+
 /* ---- measurement hooks ------------------------------------------------ */
 
 /* Reset the library's counters.  With enable_timing != 0, every kernel of

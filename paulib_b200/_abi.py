@@ -42,8 +42,12 @@ EXPORTS = (
     "pl_state_apply_cnot", "pl_state_zero_state_expectation", "pl_propagate",
     "pl_profile_reset", "pl_profile_read", "pl_state_multiply",
     "pl_state_multiply_canonicalize", "pl_state_commutator", "pl_profile_report",
-    "pl_commutator_noalloc",
+    "pl_commutator_noalloc", "pl_state_set_option", "pl_state_memory", "pl_batch_propagate",
+    "pl_serve",
 )
+PL_OPT_GRAPHS = 1
+PL_ORDER_GIVEN = 0
+PL_ORDER_LONGEST_FIRST = 1
 
 
 class CollateOpts(C.Structure):
@@ -54,6 +58,28 @@ class CollateOpts(C.Structure):
 class Truncation(C.Structure):
     _fields_ = [("max_weight", C.c_uint64), ("coefficient_cutoff", C.c_double),
                 ("max_terms", C.c_uint64)]
+
+
+class Job(C.Structure):
+    _fields_ = [("array_size", C.c_int32), ("obs_x", VP), ("obs_z", VP), ("obs_flags", VP),
+                ("obs_val", VP), ("obs_n", I64), ("rot_x", VP), ("rot_z", VP),
+                ("rot_flags", VP), ("rot_theta", VP), ("n_rot", I64), ("ops", VP),
+                ("n_ops", I64), ("trunc", Truncation), ("arrival_s", C.c_double)]
+
+
+class JobResult(C.Structure):
+    _fields_ = [("expectation", C.c_double), ("final_terms", I64), ("status", C.c_int32),
+                ("lane", C.c_int32), ("start_s", C.c_double), ("end_s", C.c_double)]
+
+
+class BatchOpts(C.Structure):
+    _fields_ = [("lanes", C.c_int32), ("use_graphs", C.c_int32), ("order", C.c_int32),
+                ("hbm_budget", C.c_uint64), ("keep_bytes", C.c_uint64), ("sync_stream", VP)]
+
+
+class BatchStats(C.Structure):
+    _fields_ = [("wall_s", C.c_double), ("peak_bytes", C.c_uint64),
+                ("budget_waits", C.c_uint64), ("jobs_failed", C.c_uint64)]
 
 
 class PLError(RuntimeError):
@@ -116,6 +142,12 @@ def lib():
         "pl_state_multiply": (I32, [VP, VP]),
         "pl_state_multiply_canonicalize": (I32, [VP, VP]),
         "pl_state_commutator": (I32, [VP, VP, VP, I32]),
+        "pl_state_set_option": (I32, [VP, I32, I64]),
+        "pl_state_memory": (I32, [VP, C.POINTER(C.c_uint64)]),
+        "pl_batch_propagate": (I32, [C.POINTER(Job), I64, C.POINTER(BatchOpts),
+                                     C.POINTER(JobResult), C.POINTER(BatchStats)]),
+        "pl_serve": (I32, [C.POINTER(Job), I64, C.POINTER(BatchOpts), C.POINTER(JobResult),
+                           C.POINTER(BatchStats)]),
         "pl_profile_read": (I32, [C.POINTER(C.c_uint64), C.POINTER(C.c_uint64),
                                   C.POINTER(C.c_double), C.POINTER(C.c_uint64)]),
     }

@@ -121,6 +121,14 @@ int record_cuda(cudaError_t e);
 int record_status(int code, const char* what);
 // Measurement hooks (pl_profile_*): launch counter and event-timed passes.
 void note_launch();
+// Device allocation and release, serialised with CUDA graph capture: a
+// cudaFree synchronises the device, which a capture running on another
+// thread must not see.
+cudaError_t dev_alloc(void** p, size_t bytes);
+void dev_free(void* p);
+void capture_lock();
+void capture_unlock();
+void note_launches(unsigned long long n);
 bool timing_enabled();
 void timed_push(cudaEvent_t start, cudaEvent_t stop, unsigned long long bytes, const char* name);
 // Event pair around one launch when timing is enabled (no-op otherwise).

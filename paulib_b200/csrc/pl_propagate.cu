@@ -35,8 +35,11 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <map>
+#include <tuple>
 #include <vector>
 
+#include "pl_budget.h"
 #include "pl_collate.cuh"
 
 namespace pl {
@@ -74,6 +77,17 @@ struct GateP {
     int cw;      // class bit: word,
     u64 cmask;   //            mask,
     int cls_x;   //            and plane (1: x, 0: z)
+};
+
+// One op of a propagation as the fast-path kernels read it from device
+// memory, so a chain of rotations can be replayed from a CUDA graph.
+template <int AS>
+struct GateRec {
+    GateP<AS> g;
+    int mode;
+    int op;        // op index (reported on a capacity overflow)
+    double c;      // cos(theta)
+    double neg_s;  // -sin(theta)
 };
 
 __device__ __forceinline__ int status_set(const int* status) {
@@ -159,12 +173,17 @@ __device__ __forceinline__ u64 lookback2(u64* lb, u32 tile, u64 v, int* status) 
 // ---------------------------------------------------------------------------
 template <int AS>
 __global__ void __launch_bounds__(kPT)
-    k_expand(Buf old, const i64* d_m, GateP<AS> g, int mode, double neg_s, Buf r0, Buf r1,
-             i64* d_k, u64* lb, u32* ctr, int* status, i64 cap_out, int gate, int* d_fail) {
+    k_expand(Buf old, const i64* d_m, const GateRec<AS>* table, const int* cursor, Buf r0, Buf r1,
+             i64* d_k, u64* lb, u32* ctr, int* status, i64 cap_out, int* d_fail) {
     __shared__ u32 s_tile;
     __shared__ u64 s_warp[kPT / 32];
     __shared__ u64 s_base;
     if (status_set(status)) return;
+    const GateRec<AS>& rec = table[*cursor];
+    const GateP<AS> g = rec.g;
+    const int mode = rec.mode, gate = rec.op;
+    const double neg_s = rec.neg_s;
+    const bool branching = mode == kGeneral || mode == kHalfPos || mode == kHalfNeg;
     const i64 m = *d_m;
     const u32 ntiles = (u32)((m + kExpTile - 1) / kExpTile);
     if (ntiles == 0) {
@@ -192,7 +211,7 @@ __global__ void __launch_bounds__(kPT)
                     x[k] = old.x[k * old.cap + j];
                     z[k] = old.z[k * old.cap + j];
                 }
-                a = anticommutes<AS>(x, z, g);
+                a = branching && anticommutes<AS>(x, z, g);
                 const u64 w = g.cls_x ? x[g.cw] : z[g.cw];
                 cl = (w & g.cmask) != 0;
             }
@@ -477,13 +496,17 @@ __device__ __forceinline__ u32 lookback1(u32* lb, u32 tile, u32 cnt, int* status
 template <int AS>
 __global__ void __launch_bounds__(kPT)
     k_merge_reduce(Buf old, const i64* d_m, Buf nw, const i64* d_k, const u32* lo_s,
-                   const u32* hi_s, GateP<AS> g, int mode, double c, Buf out, i64* d_out,
-                   u64 max_weight, double cutoff, u32* lb, u32* ctr, int* status, int gate,
+                   const u32* hi_s, const GateRec<AS>* table, const int* cursor, Buf out,
+                   i64* d_out, u64 max_weight, double cutoff, u32* lb, u32* ctr, int* status,
                    int* d_fail) {
     extern __shared__ __align__(16) unsigned char smem[];
     __shared__ u32 s_tile, s_excl;
     __shared__ u32 s_warp[kPT / 32];
     if (status_set(status)) return;
+    const GateRec<AS>& rec = table[*cursor];
+    const GateP<AS> g = rec.g;
+    const int mode = rec.mode, gate = rec.op;
+    const double c = rec.c;
     constexpr int IT = PItems<AS>::v;
     constexpr int T = ptile<AS>();
     const STile<AS> S = carve_tile<AS>(smem, T + 2);
@@ -517,8 +540,9 @@ __global__ void __launch_bounds__(kPT)
                         x[w] = S.x[w * S.cap + i];
                         z[w] = S.z[w * S.cap + i];
                     }
-                    if (anticommutes<AS>(x, z, g)) {
+                    if (mode != kSkip && anticommutes<AS>(x, z, g)) {
                         if (mode == kGeneral) S.v[i] = dmul(S.v[i], c);
+                        else if (mode == kNegate) S.v[i] = -S.v[i];
                         else S.f[i] |= 4u;  // +-pi/2: the old term moved to its child
                     }
                 } else {
@@ -851,6 +875,64 @@ __global__ void __launch_bounds__(256) k_cnot_state(Buf b, const i64* d_n, int w
     }
 }
 
+// Start of a fast-path rotation: zero the look-back words and tile counters
+// of the chain and select its gate record (idx >= 0: op idx; idx < 0: the
+// op after the current one, which is how a captured chain advances).
+__global__ void __launch_bounds__(256) k_rot_begin(uint4* zero, size_t n16, int* cursor,
+                                                   int idx) {
+    const uint4 z = make_uint4(0u, 0u, 0u, 0u);
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n16;
+         i += (size_t)gridDim.x * blockDim.x)
+        zero[i] = z;
+    if (blockIdx.x == 0 && threadIdx.x == 0) *cursor = idx >= 0 ? idx : *cursor + 1;
+}
+
+__global__ void k_set_int(int* p, int v) { *p = v; }
+
+// A layer of CNOTs (PauliSumClifford.h:213-239) applied in op order to each
+// term in one pass: pairs[2k] = control, pairs[2k+1] = target.
+template <int AS>
+__global__ void __launch_bounds__(256) k_cnot_layer(Buf b, const i64* d_n, const int* pairs,
+                                                    int count, const int* status) {
+    if (status_set(status)) return;
+    const i64 n = *d_n;
+    for (i64 i = (i64)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+         i += (i64)gridDim.x * blockDim.x) {
+        u64 x[AS], z[AS];
+#pragma unroll
+        for (int k = 0; k < AS; ++k) {
+            x[k] = b.x[k * b.cap + i];
+            z[k] = b.z[k * b.cap + i];
+        }
+        u32 f = b.f[i];
+        for (int q = 0; q < count; ++q) {
+            const int c = pairs[2 * q], t = pairs[2 * q + 1];
+            const int wc = c >> 6, wt = t >> 6;
+            const u64 mc = 1ull << (c & 63), mt = 1ull << (t & 63);
+            u64 xwc = 0, zwc = 0, xwt = 0, zwt = 0;
+#pragma unroll
+            for (int k = 0; k < AS; ++k) {
+                if (k == wc) { xwc = x[k]; zwc = z[k]; }
+                if (k == wt) { xwt = x[k]; zwt = z[k]; }
+            }
+            const u64 xc = (xwc & mc) != 0, zc = (zwc & mc) != 0;
+            const u64 xt = (xwt & mt) != 0, zt = (zwt & mt) != 0;
+            f ^= (u32)((xc & zt & (1ull ^ xt ^ zc)) << 1);
+#pragma unroll
+            for (int k = 0; k < AS; ++k) {
+                if (k == wt) x[k] ^= (0ull - xc) & mt;
+                if (k == wc) z[k] ^= (0ull - zt) & mc;
+            }
+        }
+#pragma unroll
+        for (int k = 0; k < AS; ++k) {
+            b.x[k * b.cap + i] = x[k];
+            b.z[k * b.cap + i] = z[k];
+        }
+        b.f[i] = (u8)f;
+    }
+}
+
 // isCloseOne (PauliSumOperations.h:19-21).
 bool close_one(double v) { return std::fabs(v - 1.0) <= 1e-14; }
 
@@ -883,6 +965,18 @@ struct pl_state {
     DevArena ws;            // collate workspace
     // 0: anything; 1: distinct (x,z,phase) keys; 2: canonical and sorted
     int cls = 0;
+    int* d_cursor = nullptr;  // op whose gate record the fast-path kernels read
+    void* d_table = nullptr;  // gate records of the running propagation (one per op)
+    size_t table_bytes = 0;
+    int* d_pairs = nullptr;   // CNOT (control, target) per op
+    size_t pairs_bytes = 0;
+    bool use_graphs = false;
+    // Captured rotation chains keyed by (length, start buffer, max_weight,
+    // cutoff bits); they hold the buffer pointers, so growing drops them.
+    std::map<std::tuple<int, int, uint64_t, uint64_t>, cudaGraphExec_t> graphs;
+    pl::MemBudget* budget = nullptr;
+    size_t held_bytes = 0;    // device bytes of mem (counted against budget)
+    cudaStream_t cap_st = nullptr;  // private stream the chains are captured on
 };
 
 namespace pl {
@@ -909,15 +1003,18 @@ Buf carve_buf(unsigned char*& p, int as, i64 cap) {
 }
 
 // Allocate all buffers for capacity cap (contents undefined).
-int state_alloc(pl_state* s, i64 cap, void** mem_out, Buf* S, Buf& R0, Buf& R1, Buf& N,
-                size_t* small_off) {
+size_t state_bytes(int as, i64 cap) {
     const u32 max_tiles = (u32)((2 * cap) / 256 + 4);
-    size_t total = 5 * buf_bytes(s->as, cap);
     const size_t small = a256(8 * (size_t)max_tiles) + a256(4 * (size_t)max_tiles) +
                          a256(4 * 16) + 4 * a256(4 * (size_t)max_tiles) + a256(8 * 8) + a256(64);
-    total += small;
+    return 5 * buf_bytes(as, cap) + small;
+}
+
+int state_alloc(pl_state* s, i64 cap, void** mem_out, Buf* S, Buf& R0, Buf& R1, Buf& N,
+                size_t* small_off) {
+    const size_t total = state_bytes(s->as, cap);
     void* mem = nullptr;
-    if (cudaMalloc(&mem, total) != cudaSuccess) {
+    if (dev_alloc(&mem, total) != cudaSuccess) {
         cudaGetLastError();
         return record_status(PL_ERR_OOM, "pl_state buffers");
     }
@@ -956,6 +1053,12 @@ void wire_small(pl_state* s, unsigned char* p, u32 max_tiles) {
     p += a256(8 * 8);
     s->d_status = (int*)p;
     s->d_fail = s->d_status + 1;
+    s->d_cursor = s->d_status + 2;
+}
+
+void drop_graphs(pl_state* s) {
+    for (auto& kv : s->graphs) cudaGraphExecDestroy(kv.second);
+    s->graphs.clear();
 }
 
 // (Re)build all buffers with capacity >= need, keeping the current state.
@@ -970,8 +1073,14 @@ int state_grow(pl_state* s, i64 need) {
     void* mem = nullptr;
     Buf S[2], R0, R1, N;
     size_t off = 0;
+    const size_t nbytes = state_bytes(s->as, cap);
+    if (s->budget) s->budget->resize(s->held_bytes, nbytes);
     const int rc = state_alloc(s, cap, &mem, S, R0, R1, N, &off);
-    if (rc) return rc;
+    if (rc) {
+        if (s->budget) s->budget->resize(nbytes, s->held_bytes);
+        return rc;
+    }
+    drop_graphs(s);
     int status = 0, fail = 0;
     if (s->mem) {
         const Buf& o = s->S[s->cur];
@@ -986,9 +1095,10 @@ int state_grow(pl_state* s, i64 need) {
         PL_CUDA_TRY(cudaMemcpyAsync(&status, s->d_status, sizeof(int), cudaMemcpyDeviceToHost,
                                     s->st));
         PL_CUDA_TRY(cudaStreamSynchronize(s->st));
-        cudaFree(s->mem);
+        dev_free(s->mem);
     }
     s->mem = mem;
+    s->held_bytes = nbytes;
     s->cap = cap;
     s->S[0] = S[0];
     s->S[1] = S[1];
@@ -1032,13 +1142,20 @@ SoAOut out_of(const Buf& b) { return SoAOut{b.x, b.z, b.f, b.v, b.cap}; }
 int state_collate(pl_state* s, i64 n, const CollateArgs& a) {
     if (n > s->cap) return record_status(PL_ERR_INTERNAL, "state_collate size");
     const size_t need = collate_ws_bytes(s->as, n);
+    const size_t ws_before = s->ws.bytes;
+    if (need > ws_before && s->budget) s->budget->resize(s->held_bytes + ws_before, s->held_bytes + need);
     int rc = s->ws.ensure(need);
-    if (rc) return rc;
+    if (rc) {
+        if (need > ws_before && s->budget) s->budget->resize(s->held_bytes + need, s->held_bytes + ws_before);
+        return rc;
+    }
     const int other = 1 - s->cur;
     i64 cnt = 0;
+    cudaEvent_t e0 = timed_begin(s->st);
     rc = collate_soa(s->as, view_of(s->S[s->cur], n), out_of(s->S[other]), a, &cnt, s->ws.ptr,
                      s->ws.bytes, s->st);
     if (rc) return rc;
+    timed_end(e0, s->st, "state_collate_span", 0ull);
     PL_CUDA_TRY(cudaMemcpyAsync(s->d_size + other, &cnt, sizeof(i64), cudaMemcpyHostToDevice,
                                 s->st));
     PL_CUDA_TRY(cudaStreamSynchronize(s->st));
@@ -1110,31 +1227,88 @@ int set_smem_attrs() {
     return PL_OK;
 }
 
-// One fast-path rotation on a canonical state: S[cur] -> S[1-cur].
+// One fast-path rotation on a canonical state, S[in] -> S[1-in], reading its
+// gate record table[op] (op < 0: the record after the current one).  With
+// timed = false nothing but kernels is issued, so the chain can be captured.
 template <int AS>
-int fast_rotation(pl_state* s, const GateP<AS>& g, int mode, double c, double sn,
-                  const pl_truncation& tr, int gate_index) {
-    PL_CUDA_TRY(cudaMemsetAsync(s->lbA, 0, s->zero_bytes, s->st));
-    const int in = s->cur, outb = 1 - s->cur;
+int rotation_chain(pl_state* s, int in, int op, const pl_truncation& tr, bool timed) {
+    const int outb = 1 - in;
     constexpr int T = ptile<AS>();
-    k_expand<AS><<<grid_persistent(4), kPT, 0, s->st>>>(
-        s->S[in], s->d_size + in, g, mode, -sn, s->R0, s->R1, s->d_k, s->lbA, s->ctr + 0,
-        s->d_status, s->cap, gate_index, s->d_fail), pl::note_launch();
-    const int pgrid = std::max(1, (int)((s->max_tiles + 255) / 256));
-    k_partition<AS><<<pgrid, 256, 0, s->st>>>(s->R0, s->d_k, s->R1, s->d_k + 1, nullptr, T, 0,
-                                              s->spB_lo, s->spB_hi, s->max_tiles, s->d_status), pl::note_launch();
-    k_merge_runs<AS><<<grid_persistent(2), kPT, tile_smem_bytes<AS>(T), s->st>>>(
-        s->R0, s->R1, s->d_k, s->spB_lo, s->spB_hi, s->N, s->ctr + 1, s->d_status), pl::note_launch();
-    k_partition<AS><<<pgrid, 256, 0, s->st>>>(s->S[in], s->d_size + in, s->N, s->d_k, s->d_k + 1,
-                                              T, 1, s->spC_lo, s->spC_hi, s->max_tiles,
-                                              s->d_status), pl::note_launch();
+    const auto* table = static_cast<const GateRec<AS>*>(s->d_table);
+    const int pgrid = std::max(1, std::min((int)((s->max_tiles + 255) / 256), sm_count() * 4));
     const u64 mw = tr.max_weight;
     const double cut = tr.coefficient_cutoff > 0.0 ? tr.coefficient_cutoff : 0.0;
+    cudaEvent_t e0 = timed ? timed_begin(s->st) : nullptr;
+    k_rot_begin<<<sm_count(), 256, 0, s->st>>>(reinterpret_cast<uint4*>(s->lbA), s->zero_bytes / 16,
+                                               s->d_cursor, op);
+    k_expand<AS><<<grid_persistent(4), kPT, 0, s->st>>>(
+        s->S[in], s->d_size + in, table, s->d_cursor, s->R0, s->R1, s->d_k, s->lbA, s->ctr + 0,
+        s->d_status, s->cap, s->d_fail);
+    if (timed) timed_end(e0, s->st, "k_expand", 0ull);
+    e0 = timed ? timed_begin(s->st) : nullptr;
+    k_partition<AS><<<pgrid, 256, 0, s->st>>>(s->R0, s->d_k, s->R1, s->d_k + 1, nullptr, T, 0,
+                                              s->spB_lo, s->spB_hi, s->max_tiles, s->d_status);
+    k_merge_runs<AS><<<grid_persistent(2), kPT, tile_smem_bytes<AS>(T), s->st>>>(
+        s->R0, s->R1, s->d_k, s->spB_lo, s->spB_hi, s->N, s->ctr + 1, s->d_status);
+    k_partition<AS><<<pgrid, 256, 0, s->st>>>(s->S[in], s->d_size + in, s->N, s->d_k, s->d_k + 1,
+                                              T, 1, s->spC_lo, s->spC_hi, s->max_tiles,
+                                              s->d_status);
+    if (timed) timed_end(e0, s->st, "k_merge_runs+partitions", 0ull);
+    e0 = timed ? timed_begin(s->st) : nullptr;
     k_merge_reduce<AS><<<grid_persistent(2), kPT, tile_smem_bytes<AS>(T + 2), s->st>>>(
-        s->S[in], s->d_size + in, s->N, s->d_k, s->spC_lo, s->spC_hi, g, mode, c, s->S[outb],
-        s->d_size + outb, mw, cut, s->lbC, s->ctr + 2, s->d_status, gate_index, s->d_fail), pl::note_launch();
-    PL_CUDA_TRY(cudaGetLastError());
-    s->cur = outb;
+        s->S[in], s->d_size + in, s->N, s->d_k, s->spC_lo, s->spC_hi, table, s->d_cursor,
+        s->S[outb], s->d_size + outb, mw, cut, s->lbC, s->ctr + 2, s->d_status, s->d_fail);
+    if (timed) timed_end(e0, s->st, "k_merge_reduce", 0ull);
+    pl::note_launches(6);
+    return PL_OK;
+}
+constexpr int kChainKernels = 6;
+
+// A run of len fast-path rotations starting at op first, replayed from a
+// CUDA graph captured once per (len, start buffer, truncation) and state
+// buffers.  The graph advances the device cursor itself.
+template <int AS>
+int rotation_graph(pl_state* s, int first, int len, const pl_truncation& tr) {
+    const double cut = tr.coefficient_cutoff > 0.0 ? tr.coefficient_cutoff : 0.0;
+    u64 cut_bits;
+    std::memcpy(&cut_bits, &cut, sizeof(cut_bits));
+    const auto key = std::make_tuple(len, s->cur, (uint64_t)tr.max_weight, (uint64_t)cut_bits);
+    auto it = s->graphs.find(key);
+    cudaGraphExec_t ex = nullptr;
+    if (it != s->graphs.end()) {
+        ex = it->second;
+    } else {
+        // Capture on a private stream (the caller's may be the legacy default
+        // stream, which cannot be captured); the graph then runs on s->st.
+        if (!s->cap_st)
+            PL_CUDA_TRY(cudaStreamCreateWithFlags(&s->cap_st, cudaStreamNonBlocking));
+        capture_lock();
+        const cudaError_t eb = cudaStreamBeginCapture(s->cap_st, cudaStreamCaptureModeThreadLocal);
+        if (eb != cudaSuccess) {
+            capture_unlock();
+            return record_cuda(eb);
+        }
+        const cudaStream_t user_st = s->st;
+        s->st = s->cap_st;
+        int in = s->cur;
+        for (int r = 0; r < len; ++r) {
+            rotation_chain<AS>(s, in, -1, tr, false);
+            in = 1 - in;
+        }
+        s->st = user_st;
+        cudaGraph_t g = nullptr;
+        const cudaError_t ec = cudaStreamEndCapture(s->cap_st, &g);
+        capture_unlock();
+        if (ec != cudaSuccess) return record_cuda(ec);
+        const cudaError_t ei = cudaGraphInstantiate(&ex, g, 0);
+        cudaGraphDestroy(g);
+        if (ei != cudaSuccess) return record_cuda(ei);
+        s->graphs[key] = ex;
+    }
+    k_set_int<<<1, 1, 0, s->st>>>(s->d_cursor, first - 1);
+    PL_CUDA_TRY(cudaGraphLaunch(ex, s->st));
+    pl::note_launches(1 + (unsigned long long)kChainKernels * len);
+    s->cur ^= (len & 1);
     return PL_OK;
 }
 
@@ -1223,6 +1397,39 @@ struct Op {
     int a, b;
 };
 
+// Device copies of the op tables (gate records, CNOT pairs), grow-only with
+// headroom; captured graphs hold the table pointer, so a reallocation drops
+// them.
+template <int AS>
+int upload_tables(pl_state* s, const std::vector<GateRec<AS>>& recs,
+                  const std::vector<int>& pairs) {
+    const size_t tb = sizeof(GateRec<AS>) * std::max<size_t>(recs.size(), 1);
+    const size_t pb = sizeof(int) * std::max<size_t>(pairs.size(), 2);
+    if (tb > s->table_bytes || pb > s->pairs_bytes) {
+        PL_CUDA_TRY(cudaStreamSynchronize(s->st));
+        drop_graphs(s);
+        if (s->d_table) dev_free(s->d_table);
+        if (s->d_pairs) dev_free(s->d_pairs);
+        s->d_table = nullptr;
+        s->d_pairs = nullptr;
+        s->table_bytes = s->pairs_bytes = 0;
+        const size_t tcap = std::max(tb, sizeof(GateRec<AS>) * 16384);
+        const size_t pcap = std::max(pb, sizeof(int) * 2 * 16384);
+        PL_CUDA_TRY(dev_alloc(&s->d_table, tcap));
+        PL_CUDA_TRY(dev_alloc(reinterpret_cast<void**>(&s->d_pairs), pcap));
+        s->table_bytes = tcap;
+        s->pairs_bytes = pcap;
+    }
+    // pageable sources: the calls return once the data is staged
+    PL_CUDA_TRY(cudaMemcpyAsync(s->d_table, recs.data(), sizeof(GateRec<AS>) * recs.size(),
+                                cudaMemcpyHostToDevice, s->st));
+    PL_CUDA_TRY(cudaMemcpyAsync(s->d_pairs, pairs.data(), sizeof(int) * pairs.size(),
+                                cudaMemcpyHostToDevice, s->st));
+    return PL_OK;
+}
+
+constexpr int kGraphMin = 8;  // shortest run of rotations replayed from a graph
+
 template <int AS>
 int run_ops(pl_state* s, const std::vector<Rot>& rots, const std::vector<Op>& ops,
             const pl_truncation& tr) {
@@ -1230,7 +1437,7 @@ int run_ops(pl_state* s, const std::vector<Rot>& rots, const std::vector<Op>& op
         return record_status(PL_ERR_UNSUPPORTED, "max_terms truncation (trim) is not built");
     int rc = set_smem_attrs<AS>();
     if (rc) return rc;
-    // per-rotation device parameters
+    // per-rotation parameters, then one record per op for the device
     std::vector<GateP<AS>> gates(rots.size());
     std::vector<int> modes(rots.size()), singles(rots.size());
     std::vector<double> cs(rots.size()), sns(rots.size());
@@ -1240,12 +1447,33 @@ int run_ops(pl_state* s, const std::vector<Rot>& rots, const std::vector<Op>& op
         singles[r] = single;
         modes[r] = classify(rots[r].theta, &cs[r], &sns[r]);
     }
+    if (ops.empty()) return PL_OK;
+    {
+        std::vector<GateRec<AS>> recs(ops.size());
+        std::vector<int> pairs(2 * ops.size(), 0);
+        for (size_t q = 0; q < ops.size(); ++q) {
+            std::memset(&recs[q], 0, sizeof(recs[q]));
+            if (ops[q].kind == 1) {
+                pairs[2 * q] = ops[q].a;
+                pairs[2 * q + 1] = ops[q].b;
+            } else {
+                const int r = ops[q].a;
+                recs[q].g = gates[r];
+                recs[q].mode = modes[r];
+                recs[q].op = (int)q;
+                recs[q].c = cs[r];
+                recs[q].neg_s = -sns[r];
+            }
+        }
+        rc = upload_tables<AS>(s, recs, pairs);
+        if (rc) return rc;
+    }
     constexpr int kWindow = 192;
     std::vector<int> in_buf(ops.size(), 0);
     size_t i = 0, since_sync = 0;
     bool pending = false;  // fast-path work not yet checked
     // Check queued work; on a capacity overflow, grow and rewind to the
-    // failing gate (its input buffer is untouched).  Returns false on error.
+    // failing gate (its input buffer is untouched).
     auto checkpoint = [&](bool* rewound) -> int {
         *rewound = false;
         int st = 0, fail = 0;
@@ -1274,14 +1502,18 @@ int run_ops(pl_state* s, const std::vector<Rot>& rots, const std::vector<Op>& op
         const Op& op = ops[i];
         bool rewound = false;
         if (op.kind == 1) {
+            // consecutive CNOTs (one brickwork layer) in one pass
+            size_t j = i;
+            while (j < ops.size() && ops[j].kind == 1) in_buf[j++] = s->cur;
             if (s->cls == 2) s->cls = 1;
-            in_buf[i] = s->cur;
-            k_cnot_state<AS><<<grid_persistent(8), 256, 0, s->st>>>(
-                s->S[s->cur], s->d_size + s->cur, op.a / 64, 1ull << (op.a % 64), op.b / 64,
-                1ull << (op.b % 64), s->d_status), pl::note_launch();
+            cudaEvent_t e0 = timed_begin(s->st);
+            k_cnot_layer<AS><<<grid_persistent(8), 256, 0, s->st>>>(
+                s->S[s->cur], s->d_size + s->cur, s->d_pairs + 2 * i, (int)(j - i), s->d_status),
+                pl::note_launch();
+            timed_end(e0, s->st, "k_cnot_layer", 0ull);
             pending = true;
-            ++i;
-            ++since_sync;
+            since_sync += j - i;
+            i = j;
         } else {
             const int r = op.a;
             const bool fast_ok = singles[r] && (s->cls == 2 || s->cls == 1);
@@ -1294,17 +1526,30 @@ int run_ops(pl_state* s, const std::vector<Rot>& rots, const std::vector<Op>& op
                 if (rc) return rc;
             }
             if (fast_ok && s->cls == 2) {
-                in_buf[i] = s->cur;
-                if (modes[r] == kNegate) {
-                    k_negate<AS><<<grid_persistent(8), 256, 0, s->st>>>(
-                        s->S[s->cur], s->d_size + s->cur, gates[r], 1, s->d_status), pl::note_launch();
-                } else if (modes[r] != kSkip) {
-                    rc = fast_rotation<AS>(s, gates[r], modes[r], cs[r], sns[r], tr, (int)i);
+                size_t j = i;
+                while (j < ops.size() && ops[j].kind == 0 && singles[ops[j].a]) ++j;
+                const int len = (int)(j - i);
+                if (s->use_graphs && len >= kGraphMin && !timing_enabled()) {
+                    for (int q = 0; q < len; ++q) in_buf[i + q] = s->cur ^ (q & 1);
+                    rc = rotation_graph<AS>(s, (int)i, len, tr);
                     if (rc) return rc;
+                    since_sync += len;
+                    i = j;
+                } else {
+                    in_buf[i] = s->cur;
+                    if (modes[r] == kNegate) {
+                        k_negate<AS><<<grid_persistent(8), 256, 0, s->st>>>(
+                            s->S[s->cur], s->d_size + s->cur, gates[r], 1, s->d_status),
+                            pl::note_launch();
+                    } else if (modes[r] != kSkip) {
+                        rc = rotation_chain<AS>(s, s->cur, (int)i, tr, true);
+                        if (rc) return rc;
+                        s->cur ^= 1;
+                    }
+                    ++i;
+                    ++since_sync;
                 }
                 pending = true;
-                ++i;
-                ++since_sync;
             } else if (modes[r] == kSkip && s->cls == 2) {
                 ++i;
             } else {
@@ -1322,6 +1567,7 @@ int run_ops(pl_state* s, const std::vector<Rot>& rots, const std::vector<Op>& op
             if (rc) return rc;
         }
     }
+    PL_CUDA_TRY(cudaGetLastError());
     return PL_OK;
 }
 
@@ -1371,10 +1617,61 @@ extern "C" int pl_state_create(pl_state** out, int array_size, int64_t capacity_
 extern "C" int pl_state_destroy(pl_state* s) {
     if (!s) return record_status(PL_OK, nullptr);
     cudaStreamSynchronize(s->st);
-    if (s->mem) cudaFree(s->mem);
+    drop_graphs(s);
+    if (s->cap_st) cudaStreamDestroy(s->cap_st);
+    if (s->mem) dev_free(s->mem);
+    if (s->d_table) dev_free(s->d_table);
+    if (s->d_pairs) dev_free(s->d_pairs);
+    if (s->budget) s->budget->resize(s->held_bytes + s->ws.bytes, 0);
     delete s;
     return record_status(PL_OK, nullptr);
 }
+
+extern "C" int pl_state_set_option(pl_state* s, int option, int64_t value) {
+    int rc = check_state(s);
+    if (rc) return rc;
+    if (option == PL_OPT_GRAPHS) {
+        s->use_graphs = value != 0;
+        if (!s->use_graphs) drop_graphs(s);
+        return record_status(PL_OK, nullptr);
+    }
+    return record_status(PL_ERR_INVALID_ARG, "pl_state_set_option: unknown option");
+}
+
+extern "C" int pl_state_memory(pl_state* s, uint64_t* bytes) {
+    int rc = check_state(s);
+    if (rc) return rc;
+    if (!bytes) return record_status(PL_ERR_INVALID_ARG, "pl_state_memory");
+    *bytes = s->held_bytes + s->ws.bytes + s->table_bytes + s->pairs_bytes;
+    return record_status(PL_OK, nullptr);
+}
+
+namespace pl {
+// Internal hooks of the batch executor (pl_batch.cu).
+void state_attach_budget(pl_state* s, MemBudget* b) {
+    if (s->budget == b) return;
+    if (s->budget) s->budget->resize(s->held_bytes + s->ws.bytes, 0);
+    s->budget = b;
+    if (b) b->resize(0, s->held_bytes + s->ws.bytes);
+}
+size_t state_held_bytes(pl_state* s) { return s->held_bytes + s->ws.bytes; }
+// Give the buffers back (down to the minimum capacity) between jobs.
+int state_shrink(pl_state* s) {
+    PL_CUDA_TRY(cudaStreamSynchronize(s->st));
+    drop_graphs(s);
+    const size_t before = s->held_bytes + s->ws.bytes;
+    if (s->ws.ptr) dev_free(s->ws.ptr);
+    s->ws.ptr = nullptr;
+    s->ws.bytes = 0;
+    if (s->mem) dev_free(s->mem);
+    s->mem = nullptr;
+    s->cap = 0;
+    s->held_bytes = 0;
+    if (s->budget) s->budget->resize(before, 0);
+    s->cls = 0;
+    return state_grow(s, 1 << 16);
+}
+}  // namespace pl
 
 extern "C" int pl_state_upload(pl_state* s, const uint64_t* x, const uint64_t* z,
                                const uint8_t* flags, const double* val, int64_t n) {

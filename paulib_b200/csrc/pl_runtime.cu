@@ -50,7 +50,21 @@ int record_cuda(cudaError_t e) {
     return g_last_status;
 }
 
+static std::mutex g_alloc_mu;
+cudaError_t dev_alloc(void** p, size_t bytes) {
+    std::lock_guard<std::mutex> lock(g_alloc_mu);
+    return cudaMalloc(p, bytes);
+}
+void dev_free(void* p) {
+    if (!p) return;
+    std::lock_guard<std::mutex> lock(g_alloc_mu);
+    cudaFree(p);
+}
+void capture_lock() { g_alloc_mu.lock(); }
+void capture_unlock() { g_alloc_mu.unlock(); }
+
 void note_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
+void note_launches(unsigned long long n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
 bool timing_enabled() { return g_timing.load(std::memory_order_relaxed); }
 void timed_push(cudaEvent_t start, cudaEvent_t stop, unsigned long long bytes, const char* name) {
     std::lock_guard<std::mutex> lock(g_timed_mu);

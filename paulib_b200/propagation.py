@@ -54,6 +54,17 @@ class State:
     def __exit__(self, *exc):
         self.close()
 
+    def use_graphs(self, enable: bool = True):
+        """Replay runs of single-qubit rotations from captured CUDA graphs."""
+        _abi.check(self._lib.pl_state_set_option(self._h, _abi.PL_OPT_GRAPHS, int(bool(enable))),
+                   "pl_state_set_option")
+        return self
+
+    def memory(self) -> int:
+        b = C.c_uint64()
+        _abi.check(self._lib.pl_state_memory(self._h, C.byref(b)), "pl_state_memory")
+        return b.value
+
     # -- data ------------------------------------------------------------
     def upload(self, x, z, flags, val):
         x = np.ascontiguousarray(x, np.uint64).reshape(self.array_size, -1)
