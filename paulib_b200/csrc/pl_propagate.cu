@@ -32,6 +32,8 @@
 // Other states and generators take the general path: materialise old and
 // new terms, then the collate engine (pl_collate.cu) in the matching mode.
 
+#include <cuda_pipeline.h>
+
 #include <algorithm>
 #include <cmath>
 #include <cstring>
@@ -172,7 +174,7 @@ __device__ __forceinline__ u64 lookback2(u64* lb, u32 tile, u64 v, int* status) 
 // A: expansion into two runs.
 // ---------------------------------------------------------------------------
 template <int AS>
-__global__ void __launch_bounds__(kPT)
+__global__ void __launch_bounds__(kPT, AS == 1 ? 4 : 2)
     k_expand(Buf old, const i64* d_m, const GateRec<AS>* table, const int* cursor, Buf r0, Buf r1,
              i64* d_k, u64* lb, u32* ctr, int* status, i64 cap_out, int* d_fail) {
     __shared__ u32 s_tile;
@@ -493,8 +495,70 @@ __device__ __forceinline__ u32 lookback1(u32* lb, u32 tile, u32 cnt, int* status
     return excl;
 }
 
+// Keys of two terms name the same canonical string: (x, z, phase) equal;
+// the sign bit of the order key does not take part.
+// The same look-back run by a whole warp: each round reads 32 predecessors
+// at once, so a tile whose neighbours have only published aggregates still
+// finds its prefix in one or two round trips.  All lanes return the
+// exclusive prefix.  Bounded.
+__device__ __forceinline__ u32 warp_lookback1(u32* lb, u32 tile, u32 cnt, int* status) {
+    constexpr u32 kAgg = 1u << 30, kPre = 2u << 30, kMask = (1u << 30) - 1;
+    const int lane = threadIdx.x & 31;
+    if (tile == 0) {
+        if (lane == 0) st_volatile(lb, kPre | cnt);
+        return 0;
+    }
+    if (lane == 0) st_volatile(lb + tile, kAgg | cnt);
+    u32 excl = 0;
+    i64 t = (i64)tile - 1;  // closest predecessor of this window
+    u32 spins = 0;
+    while (t >= 0) {
+        const i64 q = t - lane;
+        const u32 w = q >= 0 ? ld_volatile(lb + q) : kPre;  // before tile 0: prefix 0
+        const u32 fl = w >> 30;
+        const u32 pre = __ballot_sync(0xffffffffu, fl == 2u);
+        const u32 zero = __ballot_sync(0xffffffffu, fl == 0u);
+        const u32 upto = pre ? (pre & (0u - pre)) * 2u - 1u : 0xffffffffu;  // lanes <= first prefix
+        if (zero & upto) {
+            if (++spins > kSpinLimit) {
+                if (lane == 0) raise_status(status, PL_ERR_TIMEOUT);
+                break;
+            }
+            if (spins > 64) __nanosleep(64);
+            continue;
+        }
+        u32 v = ((upto >> lane) & 1u) ? (w & kMask) : 0u;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+        excl += v;
+        if (pre) break;
+        t -= 32;
+    }
+    if (lane == 0) st_volatile(lb + tile, kPre | ((excl + cnt) & kMask));
+    return excl;
+}
+
 template <int AS>
-__global__ void __launch_bounds__(kPT)
+__device__ __forceinline__ bool same_string(const Key<AS>& a, const Key<AS>& b) {
+    bool same = ((a.ps ^ b.ps) & 2u) == 0;
+#pragma unroll
+    for (int w = 0; w < AS; ++w) same = same && a.x[w] == b.x[w] && a.z[w] == b.z[w];
+    return same;
+}
+
+// Merge of the old terms A (canonical: distinct keys, sign 0) with the sorted
+// children C; a string occurs at most once in each, so equal strings meet as
+// an adjacent (A, C) pair (ties take A first).  The tile covers merged
+// positions [D, D + T); each thread merges IT consecutive positions
+// sequentially from shared memory, holding the current A and C keys in
+// registers.  A term is a head unless it is a C term whose A predecessor has
+// the same string; a head A term adds its C twin (peeked, possibly in the
+// next thread's or tile's range).  Each head is reduced as S(sign 0) -
+// S(sign 1) of its members in merged order -- the reference's `+=` followed
+// by canonicalize -- filtered (zero, cutoff, weight) and compacted with a
+// decoupled look-back.
+template <int AS>
+__global__ void __launch_bounds__(kPT, AS == 1 ? 4 : 2)
     k_merge_reduce(Buf old, const i64* d_m, Buf nw, const i64* d_k, const u32* lo_s,
                    const u32* hi_s, const GateRec<AS>* table, const int* cursor, Buf out,
                    i64* d_out, u64 max_weight, double cutoff, u32* lb, u32* ctr, int* status,
@@ -524,84 +588,129 @@ __global__ void __launch_bounds__(kPT)
         __syncthreads();
         if (tile >= ntiles) break;
         const i64 D = (i64)tile * T;
-        const i64 s0 = D > 0 ? D - 1 : 0;
-        const i64 s1 = D + T + 1 < total ? D + T + 1 : total;
+        const i64 dend = D + T < total ? D + T : total;
         const i64 a0 = lo_s[tile], a1 = hi_s[tile];
-        const i64 b0 = s0 - a0, b1 = s1 - a1;
+        const i64 b0 = D - a0, b1 = dend - a1;
         const int la = (int)(a1 - a0), lbn = (int)(b1 - b0);
-        const bool bad = la < 0 || lbn < 0 || la + lbn > T + 2;
+        const int ha = a0 > 0 ? 1 : 0;        // A[a0 - 1] staged before the tile's A terms
+        const int hc = b1 < nb ? 1 : 0;       // C[b1] staged after the tile's C terms
+        const int cb = ha + la;               // smem index of C[b0]
+        const bool bad = la < 0 || lbn < 0 || la + lbn > T || (la + lbn) != (int)(dend - D);
         if (!bad) {
-            for (int i = tid; i < la + lbn; i += kPT) {
-                if (i < la) {
-                    tile_load<AS>(S, i, old, a0 + i);
-                    u64 x[AS], z[AS];
+            // x, z, v by asynchronous copies straight into shared memory (all in
+            // flight at once); the flags bytes through registers
+            constexpr int kLd = (T + 2 + kPT - 1) / kPT;
+            const int cnt = cb + lbn + hc;
+            u32 fr[kLd];
+#pragma unroll
+            for (int r = 0; r < kLd; ++r) {
+                const int i = tid + r * kPT;
+                fr[r] = 0;
+                if (i < cnt) {
+                    const bool isA = i < cb;
+                    const Buf& B = isA ? old : nw;
+                    const i64 src = isA ? a0 - ha + i : b0 + (i - cb);
 #pragma unroll
                     for (int w = 0; w < AS; ++w) {
-                        x[w] = S.x[w * S.cap + i];
-                        z[w] = S.z[w * S.cap + i];
+                        __pipeline_memcpy_async(&S.x[w * S.cap + i], &B.x[w * B.cap + src], 8);
+                        __pipeline_memcpy_async(&S.z[w * S.cap + i], &B.z[w * B.cap + src], 8);
                     }
-                    if (mode != kSkip && anticommutes<AS>(x, z, g)) {
-                        if (mode == kGeneral) S.v[i] = dmul(S.v[i], c);
-                        else if (mode == kNegate) S.v[i] = -S.v[i];
-                        else S.f[i] |= 4u;  // +-pi/2: the old term moved to its child
-                    }
-                } else {
-                    tile_load<AS>(S, i, nw, b0 + (i - la));
+                    __pipeline_memcpy_async(&S.v[i], &B.v[src], 8);
+                    fr[r] = B.f[src];
+                }
+            }
+            __pipeline_commit();
+#pragma unroll
+            for (int r = 0; r < kLd; ++r) {
+                const int i = tid + r * kPT;
+                if (i < cnt) S.f[i] = (u8)(fr[r] & 3u);
+            }
+            __pipeline_wait_prior(0);
+        }
+        __syncthreads();
+        if (!bad && mode != kSkip) {
+            for (int i = tid; i < cb; i += kPT) {
+                u64 x[AS], z[AS];
+#pragma unroll
+                for (int w = 0; w < AS; ++w) {
+                    x[w] = S.x[w * S.cap + i];
+                    z[w] = S.z[w * S.cap + i];
+                }
+                if (anticommutes<AS>(x, z, g)) {
+                    if (mode == kGeneral) S.v[i] = dmul(S.v[i], c);
+                    else if (mode == kNegate) S.v[i] = -S.v[i];
+                    else S.f[i] |= 4u;  // +-pi/2: the old term moved to its child
                 }
             }
         }
         __syncthreads();
-        if (!bad) block_merge<AS>(S, la, lbn);
-        __syncthreads();
-        // output positions of this tile: global [D, min(D+T, total))
-        const i64 dend = D + T < total ? D + T : total;
-        const int q0 = (int)(D - s0);
-        const int L = la + lbn;
-        bool keep[IT];
-        double res[IT];
-        int head_e[IT];
+        // this thread's merged positions [d, d + IT) of the tile
+        const int d = tid * IT;
+        const int L = bad ? 0 : la + lbn;
+        int ai = 0, bi = 0;
+        if (d < L) {
+            int lo = d > lbn ? d - lbn : 0, hi = d < la ? d : la;
+            while (lo < hi) {
+                const int mid = (lo + hi) >> 1;
+                if (kcmp<AS>(S.key(ha + mid), S.key(cb + d - 1 - mid)) <= 0) lo = mid + 1;
+                else hi = mid;
+            }
+            ai = lo;
+            bi = d - lo;
+        }
+        Key<AS> ka, kc, kp;  // current A, current C, last A taken (or staged before)
+        if (ai < la) ka = S.key(ha + ai);
+        if (bi < lbn + hc) kc = S.key(cb + bi);
+        bool has_p = ha + ai - 1 >= 0;
+        if (has_p) kp = S.key(ha + ai - 1);
+        // kept heads: their smem index in S.order[d + j], the reduced value
+        // written over the head's own slot (no other thread reads it again)
         u32 nkeep = 0;
 #pragma unroll
         for (int it = 0; it < IT; ++it) {
-            keep[it] = false;
-            res[it] = 0.0;
-            head_e[it] = 0;
-            const int q = q0 + tid * IT + it;
-            if (bad || D + tid * IT + it >= dend) continue;
-            const int e = S.order[q];
-            const Key<AS> ke = S.key(e);
-            bool head = (q == 0);
-            if (!head) {
-                const Key<AS> kp = S.key(S.order[q - 1]);
-                head = false;
-#pragma unroll
-                for (int w = 0; w < AS; ++w)
-                    head = head || kp.x[w] != ke.x[w] || kp.z[w] != ke.z[w];
-                head = head || ((kp.ps ^ ke.ps) & 2u);
-            }
-            if (!head) continue;
+            if (d + it >= L) continue;
+            const bool take_a = ai < la && (bi >= lbn || kcmp<AS>(ka, kc) <= 0);
             double sp = 0.0, sm = 0.0;
             bool has = false;
-            int members = 0;
-            for (int r = q; r < L; ++r) {
-                const int er = S.order[r];
-                if (r > q) {
-                    const Key<AS> kr = S.key(er);
-                    bool same = ((kr.ps ^ ke.ps) & 2u) == 0;
-#pragma unroll
-                    for (int w = 0; w < AS; ++w)
-                        same = same && kr.x[w] == ke.x[w] && kr.z[w] == ke.z[w];
-                    if (!same) break;
+            int e;
+            Key<AS> ke;
+            if (take_a) {
+                e = ha + ai;
+                ke = ka;
+                const u32 fa = S.f[e];
+                if (!(fa & 4u)) {
+                    has = true;
+                    sp = dadd(sp, S.v[e]);  // canonical A terms carry sign 0
                 }
-                if (++members > 2) {
-                    raise_status(status, PL_ERR_INTERNAL);
-                    break;
+                // the C twin follows directly (ties take A first)
+                if (bi < lbn + hc && same_string<AS>(ka, kc)) {
+                    const int ec = cb + bi;
+                    const u32 fc = S.f[ec];
+                    if (!(fc & 4u)) {
+                        has = true;
+                        if (fc & 2u) sm = dadd(sm, S.v[ec]);
+                        else sp = dadd(sp, S.v[ec]);
+                    }
                 }
-                const u32 fr = S.f[er];
-                if (fr & 4u) continue;
-                has = true;
-                if (fr & 2u) sm = dadd(sm, S.v[er]);
-                else sp = dadd(sp, S.v[er]);
+                kp = ka;
+                has_p = true;
+                ++ai;
+                if (ai < la) ka = S.key(ha + ai);
+            } else {
+                e = cb + bi;
+                ke = kc;
+                // a C term is a head unless the A term before it is its twin
+                const bool twin = has_p && same_string<AS>(kp, kc);
+                if (!twin) {
+                    const u32 fc = S.f[e];
+                    if (!(fc & 4u)) {
+                        has = true;
+                        if (fc & 2u) sm = dadd(sm, S.v[e]);
+                        else sp = dadd(sp, S.v[e]);
+                    }
+                }
+                ++bi;
+                if (bi < lbn + hc) kc = S.key(cb + bi);
             }
             if (!has) continue;
             const double rv = dadd(sp, -sm);
@@ -613,10 +722,10 @@ __global__ void __launch_bounds__(kPT)
                 for (int w = 0; w < AS; ++w) wsum += (u64)__popcll(ke.x[w] | ke.z[w]);
                 k = wsum <= max_weight;
             }
-            keep[it] = k;
-            res[it] = rv;
-            head_e[it] = e;
-            nkeep += k ? 1u : 0u;
+            if (!k) continue;
+            S.order[d + nkeep] = (u16)e;
+            S.v[e] = rv;
+            ++nkeep;
         }
         // block exclusive scan of per-thread keep counts
         u32 inc = nkeep;
@@ -626,6 +735,9 @@ __global__ void __launch_bounds__(kPT)
             if (lane >= o) inc += t;
         }
         if (lane == 31) s_warp[warp] = inc;
+        u32 mine[IT];
+#pragma unroll
+        for (int j = 0; j < IT; ++j) mine[j] = (u32)j < nkeep ? S.order[d + j] : 0u;
         __syncthreads();
         u32 wpre = 0, tot = 0;
 #pragma unroll
@@ -634,27 +746,34 @@ __global__ void __launch_bounds__(kPT)
             if (w < warp) wpre += cw;
             tot += cw;
         }
-        if (tid == 0) s_excl = lookback1(lb, tile, tot, status);
-        __syncthreads();
-        i64 o = (i64)s_excl + wpre + (inc - nkeep);
+        // the tile's kept heads, compacted in output order
+        const u32 tbase = wpre + (inc - nkeep);
 #pragma unroll
-        for (int it = 0; it < IT; ++it) {
-            if (!keep[it]) continue;
+        for (int j = 0; j < IT; ++j)
+            if ((u32)j < nkeep) S.order[tbase + j] = (u16)mine[j];
+        if (warp == 0) {
+            const u32 ex = warp_lookback1(lb, tile, tot, status);
+            if (lane == 0) s_excl = ex;
+        }
+        __syncthreads();
+        const i64 obase = (i64)s_excl;
+        for (u32 p = tid; p < tot; p += kPT) {
+            const int e = S.order[p];
+            const i64 o = obase + p;
             if (o >= out.cap) {
                 raise_status(status, PL_ERR_CAPACITY);
                 atomicExch(d_fail, gate);
                 break;
             }
-            const int e = head_e[it];
 #pragma unroll
             for (int w = 0; w < AS; ++w) {
                 out.x[w * out.cap + o] = S.x[w * S.cap + e];
                 out.z[w * out.cap + o] = S.z[w * S.cap + e];
             }
             out.f[o] = (u8)(S.f[e] & 1u);
-            out.v[o] = res[it];
-            ++o;
+            out.v[o] = S.v[e];
         }
+        if (bad && tid == 0) raise_status(status, PL_ERR_INTERNAL);
         if (tile == ntiles - 1 && tid == 0) *d_out = (i64)s_excl + tot;
         __syncthreads();
     }
@@ -1223,6 +1342,10 @@ int set_smem_attrs() {
     PL_CUDA_TRY(cudaFuncSetAttribute(k_merge_reduce<AS>,
                                      cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      (int)tile_smem_bytes<AS>(T + 2)));
+    PL_CUDA_TRY(cudaFuncSetAttribute(k_merge_reduce<AS>,
+                                     cudaFuncAttributePreferredSharedMemoryCarveout, 100));
+    PL_CUDA_TRY(cudaFuncSetAttribute(k_merge_runs<AS>,
+                                     cudaFuncAttributePreferredSharedMemoryCarveout, 100));
     done[AS] = true;
     return PL_OK;
 }
@@ -1251,11 +1374,11 @@ int rotation_chain(pl_state* s, int in, int op, const pl_truncation& tr, bool ti
     k_merge_runs<AS><<<grid_persistent(2), kPT, tile_smem_bytes<AS>(T), s->st>>>(
         s->R0, s->R1, s->d_k, s->spB_lo, s->spB_hi, s->N, s->ctr + 1, s->d_status);
     k_partition<AS><<<pgrid, 256, 0, s->st>>>(s->S[in], s->d_size + in, s->N, s->d_k, s->d_k + 1,
-                                              T, 1, s->spC_lo, s->spC_hi, s->max_tiles,
+                                              T, 0, s->spC_lo, s->spC_hi, s->max_tiles,
                                               s->d_status);
     if (timed) timed_end(e0, s->st, "k_merge_runs+partitions", 0ull);
     e0 = timed ? timed_begin(s->st) : nullptr;
-    k_merge_reduce<AS><<<grid_persistent(2), kPT, tile_smem_bytes<AS>(T + 2), s->st>>>(
+    k_merge_reduce<AS><<<grid_persistent(AS == 1 ? 4 : 2), kPT, tile_smem_bytes<AS>(T + 2), s->st>>>(
         s->S[in], s->d_size + in, s->N, s->d_k, s->spC_lo, s->spC_hi, table, s->d_cursor,
         s->S[outb], s->d_size + outb, mw, cut, s->lbC, s->ctr + 2, s->d_status, s->d_fail);
     if (timed) timed_end(e0, s->st, "k_merge_reduce", 0ull);
