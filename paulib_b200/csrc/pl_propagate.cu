@@ -173,6 +173,54 @@ __device__ __forceinline__ u64 lookback2(u64* lb, u32 tile, u64 v, int* status) 
 // ---------------------------------------------------------------------------
 // A: expansion into two runs.
 // ---------------------------------------------------------------------------
+// The look-back of lookback2 run by a whole warp (32 predecessors per round
+// trip); every lane returns the exclusive pair of counters.  Bounded.
+__device__ __forceinline__ u64 warp_lookback2(u64* lb, u32 tile, u64 v, int* status) {
+    const int lane = threadIdx.x & 31;
+    const u64 enc = ((v >> 32) << 31) | (v & 0xffffffffull);
+    if (tile == 0) {
+        if (lane == 0) st_volatile64(lb, kF2Pre | enc);
+        return 0;
+    }
+    if (lane == 0) st_volatile64(lb + tile, kF2Agg | enc);
+    u64 excl = 0;
+    i64 t = (i64)tile - 1;
+    u32 spins = 0;
+    while (t >= 0) {
+        const i64 q = t - lane;
+        const u64 w = q >= 0 ? ld_volatile64(lb + q) : kF2Pre;
+        const u32 fl = (u32)(w >> 62);
+        const u32 pre = __ballot_sync(0xffffffffu, fl == 2u);
+        const u32 zero = __ballot_sync(0xffffffffu, fl == 0u);
+        const u32 upto = pre ? (pre & (0u - pre)) * 2u - 1u : 0xffffffffu;
+        if (zero & upto) {
+            if (++spins > kSpinLimit) {
+                if (lane == 0) raise_status(status, PL_ERR_TIMEOUT);
+                break;
+            }
+            if (spins > 64) __nanosleep(64);
+            continue;
+        }
+        u64 c0 = 0, c1 = 0;
+        if ((upto >> lane) & 1u) {
+            c0 = w & kC31;
+            c1 = (w >> 31) & kC31;
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            c0 += __shfl_xor_sync(0xffffffffu, c0, o);
+            c1 += __shfl_xor_sync(0xffffffffu, c1, o);
+        }
+        excl += (c1 << 32) | c0;
+        if (pre) break;
+        t -= 32;
+    }
+    const u64 inc = excl + v;
+    if (lane == 0)
+        st_volatile64(lb + tile, kF2Pre | (((inc >> 32) << 31) | (inc & 0xffffffffull)));
+    return excl;
+}
+
 template <int AS>
 __global__ void __launch_bounds__(kPT, AS == 1 ? 4 : 2)
     k_expand(Buf old, const i64* d_m, const GateRec<AS>* table, const int* cursor, Buf r0, Buf r1,
@@ -235,7 +283,10 @@ __global__ void __launch_bounds__(kPT, AS == 1 ? 4 : 2)
             if (w < warp) wpre += v;
             tot += v;
         }
-        if (tid == 0) s_base = lookback2(lb, tile, tot, status);
+        if (warp == 0) {
+            const u64 ex = warp_lookback2(lb, tile, tot, status);
+            if (lane == 0) s_base = ex;
+        }
         __syncthreads();
         const u64 base = s_base + wpre;
         const i64 base0 = (u32)base, base1 = (u32)(base >> 32);
@@ -305,33 +356,48 @@ __global__ void __launch_bounds__(kPT, AS == 1 ? 4 : 2)
 // ---------------------------------------------------------------------------
 // Merge-path partition: split points of each tile's diagonal range.
 // ---------------------------------------------------------------------------
+// First i in [lo, hi] with !(A[i] <= B[d-1-i]) (the merge-path split of
+// diagonal d, ties taking A first), found by a whole warp: each round tests
+// 32 evenly spaced candidates at once, so a split costs about log32(n)
+// dependent memory round trips instead of log2(n).  Warp-uniform.
 template <int AS>
-__device__ __forceinline__ i64 merge_split(const Buf& A, i64 na, const Buf& B, i64 nb, i64 d) {
+__device__ __forceinline__ i64 warp_merge_split(const Buf& A, i64 na, const Buf& B, i64 nb,
+                                                i64 d) {
+    const int lane = threadIdx.x & 31;
     i64 lo = d > nb ? d - nb : 0, hi = d < na ? d : na;
     while (lo < hi) {
-        const i64 mid = (lo + hi) >> 1;
-        if (kcmp<AS>(gkey<AS>(A, mid), gkey<AS>(B, d - 1 - mid)) <= 0) lo = mid + 1;
-        else hi = mid;
+        const i64 step = (hi - lo + 31) / 32;
+        const i64 i = lo + (i64)lane * step;
+        bool p = false;
+        if (i < hi) p = kcmp<AS>(gkey<AS>(A, i), gkey<AS>(B, d - 1 - i)) <= 0;
+        const int c = __popc(__ballot_sync(0xffffffffu, p));  // the true tests are a prefix
+        if (c == 0) break;                                     // pred(lo) is false
+        const i64 next = lo + (i64)c * step;
+        lo = lo + (i64)(c - 1) * step + 1;
+        hi = next < hi ? next : hi;
     }
     return lo;
 }
 
-// For tile t: lo split at max(t*T - halo, 0), hi split at min(t*T + T + halo, total).
+// Splits of the diagonals t*T, t = 0..ntiles (one warp each): tile t merges
+// the output range [lo_s[t] + ..., hi_s[t] + ...) of both inputs.
 template <int AS>
 __global__ void __launch_bounds__(256) k_partition(Buf A, const i64* pa, Buf B, const i64* pb,
-                                                   const i64* pb2, int T, int halo, u32* lo_s,
-                                                   u32* hi_s, u32 max_tiles, const int* status) {
+                                                   const i64* pb2, int T, u32* lo_s, u32* hi_s,
+                                                   u32 max_tiles, const int* status) {
     if (status_set(status)) return;
     const i64 na = *pa, nb = *pb + (pb2 ? *pb2 : 0);
     const i64 total = na + nb;
     const u32 ntiles = (u32)((total + T - 1) / T);
-    for (u32 t = blockIdx.x * blockDim.x + threadIdx.x; t < ntiles && t < max_tiles;
-         t += gridDim.x * blockDim.x) {
-        const i64 D = (i64)t * T;
-        const i64 s0 = D - halo > 0 ? D - halo : 0;
-        const i64 s1 = D + T + halo < total ? D + T + halo : total;
-        lo_s[t] = (u32)merge_split<AS>(A, na, B, nb, s0);
-        hi_s[t] = (u32)merge_split<AS>(A, na, B, nb, s1);
+    const int lane = threadIdx.x & 31;
+    const u32 nw = (gridDim.x * blockDim.x) >> 5;
+    for (u32 t = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; t <= ntiles; t += nw) {
+        const i64 D = (i64)t * T < total ? (i64)t * T : total;
+        const u32 sp = (u32)warp_merge_split<AS>(A, na, B, nb, D);
+        if (lane == 0) {
+            if (t < ntiles && t < max_tiles) lo_s[t] = sp;
+            if (t >= 1 && t - 1 < max_tiles) hi_s[t - 1] = sp;
+        }
     }
 }
 
@@ -407,11 +473,45 @@ __device__ __forceinline__ void tile_load(const STile<AS>& S, int dst, const Buf
     S.f[dst] = B.f[src] & 3u;
 }
 
+// Stage cnt terms into S: item i < split from A[a_src + i], the rest from
+// B[b_src + i - split].  x, z and v by asynchronous copies (all of a
+// thread's items in flight at once), the flags byte through registers.
+template <int AS, int NL>
+__device__ __forceinline__ void tile_load_async(const STile<AS>& S, int cnt, int split,
+                                                const Buf& A, i64 a_src, const Buf& B,
+                                                i64 b_src) {
+    u32 fr[NL];
+#pragma unroll
+    for (int r = 0; r < NL; ++r) {
+        const int i = threadIdx.x + r * kPT;
+        fr[r] = 0;
+        if (i < cnt) {
+            const bool isA = i < split;
+            const Buf& G = isA ? A : B;
+            const i64 src = isA ? a_src + i : b_src + (i - split);
+#pragma unroll
+            for (int w = 0; w < AS; ++w) {
+                __pipeline_memcpy_async(&S.x[w * S.cap + i], &G.x[w * G.cap + src], 8);
+                __pipeline_memcpy_async(&S.z[w * S.cap + i], &G.z[w * G.cap + src], 8);
+            }
+            __pipeline_memcpy_async(&S.v[i], &G.v[src], 8);
+            fr[r] = G.f[src];
+        }
+    }
+    __pipeline_commit();
+#pragma unroll
+    for (int r = 0; r < NL; ++r) {
+        const int i = threadIdx.x + r * kPT;
+        if (i < cnt) S.f[i] = (u8)(fr[r] & 3u);
+    }
+    __pipeline_wait_prior(0);
+}
+
 // ---------------------------------------------------------------------------
 // B: merge the two runs into one sorted child list.
 // ---------------------------------------------------------------------------
 template <int AS>
-__global__ void __launch_bounds__(kPT)
+__global__ void __launch_bounds__(kPT, AS == 1 ? 4 : 2)
     k_merge_runs(Buf r0, Buf r1, const i64* d_k, const u32* lo_s, const u32* hi_s, Buf out,
                  u32* ctr, int* status) {
     extern __shared__ __align__(16) unsigned char smem[];
@@ -437,10 +537,7 @@ __global__ void __launch_bounds__(kPT)
             __syncthreads();
             continue;
         }
-        for (int i = threadIdx.x; i < la + lb; i += kPT) {
-            if (i < la) tile_load<AS>(S, i, r0, a0 + i);
-            else tile_load<AS>(S, i, r1, b0 + (i - la));
-        }
+        tile_load_async<AS, (T + kPT - 1) / kPT>(S, la + lb, la, r0, a0, r1, b0);
         __syncthreads();
         block_merge<AS>(S, la, lb);
         __syncthreads();
@@ -597,35 +694,8 @@ __global__ void __launch_bounds__(kPT, AS == 1 ? 4 : 2)
         const int cb = ha + la;               // smem index of C[b0]
         const bool bad = la < 0 || lbn < 0 || la + lbn > T || (la + lbn) != (int)(dend - D);
         if (!bad) {
-            // x, z, v by asynchronous copies straight into shared memory (all in
-            // flight at once); the flags bytes through registers
-            constexpr int kLd = (T + 2 + kPT - 1) / kPT;
-            const int cnt = cb + lbn + hc;
-            u32 fr[kLd];
-#pragma unroll
-            for (int r = 0; r < kLd; ++r) {
-                const int i = tid + r * kPT;
-                fr[r] = 0;
-                if (i < cnt) {
-                    const bool isA = i < cb;
-                    const Buf& B = isA ? old : nw;
-                    const i64 src = isA ? a0 - ha + i : b0 + (i - cb);
-#pragma unroll
-                    for (int w = 0; w < AS; ++w) {
-                        __pipeline_memcpy_async(&S.x[w * S.cap + i], &B.x[w * B.cap + src], 8);
-                        __pipeline_memcpy_async(&S.z[w * S.cap + i], &B.z[w * B.cap + src], 8);
-                    }
-                    __pipeline_memcpy_async(&S.v[i], &B.v[src], 8);
-                    fr[r] = B.f[src];
-                }
-            }
-            __pipeline_commit();
-#pragma unroll
-            for (int r = 0; r < kLd; ++r) {
-                const int i = tid + r * kPT;
-                if (i < cnt) S.f[i] = (u8)(fr[r] & 3u);
-            }
-            __pipeline_wait_prior(0);
+            tile_load_async<AS, (T + 2 + kPT - 1) / kPT>(S, cb + lbn + hc, cb, old, a0 - ha, nw,
+                                                         b0);
         }
         __syncthreads();
         if (!bad && mode != kSkip) {
@@ -1358,24 +1428,23 @@ int rotation_chain(pl_state* s, int in, int op, const pl_truncation& tr, bool ti
     const int outb = 1 - in;
     constexpr int T = ptile<AS>();
     const auto* table = static_cast<const GateRec<AS>*>(s->d_table);
-    const int pgrid = std::max(1, std::min((int)((s->max_tiles + 255) / 256), sm_count() * 4));
+    const int pgrid = std::max(1, std::min((int)((s->max_tiles + 8) / 8), sm_count() * 8));
     const u64 mw = tr.max_weight;
     const double cut = tr.coefficient_cutoff > 0.0 ? tr.coefficient_cutoff : 0.0;
     cudaEvent_t e0 = timed ? timed_begin(s->st) : nullptr;
     k_rot_begin<<<sm_count(), 256, 0, s->st>>>(reinterpret_cast<uint4*>(s->lbA), s->zero_bytes / 16,
                                                s->d_cursor, op);
-    k_expand<AS><<<grid_persistent(4), kPT, 0, s->st>>>(
+    k_expand<AS><<<grid_persistent(AS == 1 ? 4 : 2), kPT, 0, s->st>>>(
         s->S[in], s->d_size + in, table, s->d_cursor, s->R0, s->R1, s->d_k, s->lbA, s->ctr + 0,
         s->d_status, s->cap, s->d_fail);
     if (timed) timed_end(e0, s->st, "k_expand", 0ull);
     e0 = timed ? timed_begin(s->st) : nullptr;
-    k_partition<AS><<<pgrid, 256, 0, s->st>>>(s->R0, s->d_k, s->R1, s->d_k + 1, nullptr, T, 0,
+    k_partition<AS><<<pgrid, 256, 0, s->st>>>(s->R0, s->d_k, s->R1, s->d_k + 1, nullptr, T,
                                               s->spB_lo, s->spB_hi, s->max_tiles, s->d_status);
-    k_merge_runs<AS><<<grid_persistent(2), kPT, tile_smem_bytes<AS>(T), s->st>>>(
+    k_merge_runs<AS><<<grid_persistent(AS == 1 ? 4 : 2), kPT, tile_smem_bytes<AS>(T), s->st>>>(
         s->R0, s->R1, s->d_k, s->spB_lo, s->spB_hi, s->N, s->ctr + 1, s->d_status);
     k_partition<AS><<<pgrid, 256, 0, s->st>>>(s->S[in], s->d_size + in, s->N, s->d_k, s->d_k + 1,
-                                              T, 0, s->spC_lo, s->spC_hi, s->max_tiles,
-                                              s->d_status);
+                                              T, s->spC_lo, s->spC_hi, s->max_tiles, s->d_status);
     if (timed) timed_end(e0, s->st, "k_merge_runs+partitions", 0ull);
     e0 = timed ? timed_begin(s->st) : nullptr;
     k_merge_reduce<AS><<<grid_persistent(AS == 1 ? 4 : 2), kPT, tile_smem_bytes<AS>(T + 2), s->st>>>(
