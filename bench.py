@@ -380,7 +380,13 @@ def main(argv=None):
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", default="product_collate",
-                    choices=["product_collate", "propagation", "commutator"])
+                    choices=["product_collate", "propagation", "commutator", "batch", "serve"])
+    ap.add_argument("--batch-stride", type=int, default=16,
+                    help="batch workload: every n-th job of the 512-job set")
+    ap.add_argument("--serve-jobs", type=int, default=40)
+    ap.add_argument("--serve-lanes", type=int, default=6)
+    ap.add_argument("--serve-load", type=float, default=1.2,
+                    help="serve workload: arrival rate as a multiple of the plain path's capacity")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args(argv)
     if args.warmup < 3:

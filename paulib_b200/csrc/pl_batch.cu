@@ -192,8 +192,16 @@ int run_all(const pl_job* jobs, int64_t count, const pl_batch_opts* opts, pl_job
     threads.reserve((size_t)opts->lanes);
     for (int l = 0; l < opts->lanes; ++l) threads.emplace_back(lane_main, std::ref(S), l);
     for (auto& t : threads) t.join();
+    const double wall = since(S);
+    // hand the lanes' cached blocks back to the device
+    cudaMemPool_t pool;
+    if (cudaDeviceGetDefaultMemPool(&pool, S.device) == cudaSuccess) {
+        cudaDeviceSynchronize();
+        cudaMemPoolTrimTo(pool, 0);
+    }
+    cudaGetLastError();
     if (stats) {
-        stats->wall_s = since(S);
+        stats->wall_s = wall;
         stats->peak_bytes = S.budget.peak;
         stats->budget_waits = S.budget.waits;
         stats->jobs_failed = S.failed.load();

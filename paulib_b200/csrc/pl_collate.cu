@@ -1448,10 +1448,10 @@ int run_collate(const Src& src, u32 n, int mode, const KeyLayout& L, const PassP
 // ---------------------------------------------------------------------------
 int DevArena::ensure(size_t need) {
     if (need <= bytes) return PL_OK;
-    if (ptr) dev_free(ptr);
+    if (ptr) dev_free(ptr, st);
     ptr = nullptr;
     bytes = 0;
-    if (dev_alloc(&ptr, need) != cudaSuccess) {
+    if (dev_alloc(&ptr, need, st) != cudaSuccess) {
         cudaGetLastError();
         return record_status(PL_ERR_OOM, "workspace allocation");
     }
@@ -1459,7 +1459,7 @@ int DevArena::ensure(size_t need) {
     return PL_OK;
 }
 DevArena::~DevArena() {
-    if (ptr) dev_free(ptr);
+    if (ptr) dev_free(ptr, st);
 }
 
 size_t collate_ws_bytes(int as, i64 n) { return ws_for(as, n, max_chunks(as)); }

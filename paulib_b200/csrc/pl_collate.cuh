@@ -31,10 +31,11 @@ struct SoAOut {
     i64 capacity = 0;  // plane stride and maximum term count
 };
 
-// Grow-only device arena.
+// Grow-only device arena, allocated in order on its owner's stream.
 struct DevArena {
     void* ptr = nullptr;
     size_t bytes = 0;
+    cudaStream_t st = nullptr;
     int ensure(size_t need);
     ~DevArena();
 };

@@ -121,11 +121,12 @@ int record_cuda(cudaError_t e);
 int record_status(int code, const char* what);
 // Measurement hooks (pl_profile_*): launch counter and event-timed passes.
 void note_launch();
-// Device allocation and release, serialised with CUDA graph capture: a
-// cudaFree synchronises the device, which a capture running on another
-// thread must not see.
-cudaError_t dev_alloc(void** p, size_t bytes);
-void dev_free(void* p);
+// Stream-ordered device allocation from the device's default memory pool
+// (freed blocks stay cached in the pool, so regrowing costs no device-wide
+// synchronisation and no fresh page mapping); calls are serialised with CUDA
+// graph capture on other threads.
+cudaError_t dev_alloc(void** p, size_t bytes, cudaStream_t st);
+void dev_free(void* p, cudaStream_t st);
 void capture_lock();
 void capture_unlock();
 void note_launches(unsigned long long n);

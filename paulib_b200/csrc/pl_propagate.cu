@@ -1203,7 +1203,7 @@ int state_alloc(pl_state* s, i64 cap, void** mem_out, Buf* S, Buf& R0, Buf& R1, 
                 size_t* small_off) {
     const size_t total = state_bytes(s->as, cap);
     void* mem = nullptr;
-    if (dev_alloc(&mem, total) != cudaSuccess) {
+    if (dev_alloc(&mem, total, s->st) != cudaSuccess) {
         cudaGetLastError();
         return record_status(PL_ERR_OOM, "pl_state buffers");
     }
@@ -1284,7 +1284,7 @@ int state_grow(pl_state* s, i64 need) {
         PL_CUDA_TRY(cudaMemcpyAsync(&status, s->d_status, sizeof(int), cudaMemcpyDeviceToHost,
                                     s->st));
         PL_CUDA_TRY(cudaStreamSynchronize(s->st));
-        dev_free(s->mem);
+        dev_free(s->mem, s->st);
     }
     s->mem = mem;
     s->held_bytes = nbytes;
@@ -1456,51 +1456,67 @@ int rotation_chain(pl_state* s, int in, int op, const pl_truncation& tr, bool ti
 }
 constexpr int kChainKernels = 6;
 
-// A run of len fast-path rotations starting at op first, replayed from a
-// CUDA graph captured once per (len, start buffer, truncation) and state
-// buffers.  The graph advances the device cursor itself.
+// A run of len fast-path rotations starting at op first.  Whole chunks of
+// kGraphChunk rotations replay one captured CUDA graph (captured once per
+// start buffer and truncation for the state's current buffers; an even
+// chunk ends on the buffer it started from, so the same graph serves every
+// chunk of every run); the graphs advance the device cursor themselves.
+// The rest of the run is launched kernel by kernel.
+constexpr int kGraphChunk = 8;
+
 template <int AS>
 int rotation_graph(pl_state* s, int first, int len, const pl_truncation& tr) {
     const double cut = tr.coefficient_cutoff > 0.0 ? tr.coefficient_cutoff : 0.0;
     u64 cut_bits;
     std::memcpy(&cut_bits, &cut, sizeof(cut_bits));
-    const auto key = std::make_tuple(len, s->cur, (uint64_t)tr.max_weight, (uint64_t)cut_bits);
-    auto it = s->graphs.find(key);
-    cudaGraphExec_t ex = nullptr;
-    if (it != s->graphs.end()) {
-        ex = it->second;
-    } else {
-        // Capture on a private stream (the caller's may be the legacy default
-        // stream, which cannot be captured); the graph then runs on s->st.
-        if (!s->cap_st)
-            PL_CUDA_TRY(cudaStreamCreateWithFlags(&s->cap_st, cudaStreamNonBlocking));
-        capture_lock();
-        const cudaError_t eb = cudaStreamBeginCapture(s->cap_st, cudaStreamCaptureModeThreadLocal);
-        if (eb != cudaSuccess) {
+    const int chunks = len / kGraphChunk;
+    if (chunks > 0) {
+        const auto key =
+            std::make_tuple(kGraphChunk, s->cur, (uint64_t)tr.max_weight, (uint64_t)cut_bits);
+        auto it = s->graphs.find(key);
+        cudaGraphExec_t ex = nullptr;
+        if (it != s->graphs.end()) {
+            ex = it->second;
+        } else {
+            // Capture on a private stream (the caller's may be the legacy
+            // default stream, which cannot be captured); the graph then runs
+            // on s->st.
+            if (!s->cap_st)
+                PL_CUDA_TRY(cudaStreamCreateWithFlags(&s->cap_st, cudaStreamNonBlocking));
+            capture_lock();
+            const cudaError_t eb =
+                cudaStreamBeginCapture(s->cap_st, cudaStreamCaptureModeThreadLocal);
+            if (eb != cudaSuccess) {
+                capture_unlock();
+                return record_cuda(eb);
+            }
+            const cudaStream_t user_st = s->st;
+            s->st = s->cap_st;
+            int in = s->cur;
+            for (int r = 0; r < kGraphChunk; ++r) {
+                rotation_chain<AS>(s, in, -1, tr, false);
+                in = 1 - in;
+            }
+            s->st = user_st;
+            cudaGraph_t g = nullptr;
+            const cudaError_t ec = cudaStreamEndCapture(s->cap_st, &g);
             capture_unlock();
-            return record_cuda(eb);
+            if (ec != cudaSuccess) return record_cuda(ec);
+            const cudaError_t ei = cudaGraphInstantiate(&ex, g, 0);
+            cudaGraphDestroy(g);
+            if (ei != cudaSuccess) return record_cuda(ei);
+            s->graphs[key] = ex;
         }
-        const cudaStream_t user_st = s->st;
-        s->st = s->cap_st;
-        int in = s->cur;
-        for (int r = 0; r < len; ++r) {
-            rotation_chain<AS>(s, in, -1, tr, false);
-            in = 1 - in;
-        }
-        s->st = user_st;
-        cudaGraph_t g = nullptr;
-        const cudaError_t ec = cudaStreamEndCapture(s->cap_st, &g);
-        capture_unlock();
-        if (ec != cudaSuccess) return record_cuda(ec);
-        const cudaError_t ei = cudaGraphInstantiate(&ex, g, 0);
-        cudaGraphDestroy(g);
-        if (ei != cudaSuccess) return record_cuda(ei);
-        s->graphs[key] = ex;
+        k_set_int<<<1, 1, 0, s->st>>>(s->d_cursor, first - 1);
+        pl::note_launch();
+        for (int c = 0; c < chunks; ++c) PL_CUDA_TRY(cudaGraphLaunch(ex, s->st));
+        pl::note_launches((unsigned long long)kChainKernels * kGraphChunk * chunks);
     }
-    k_set_int<<<1, 1, 0, s->st>>>(s->d_cursor, first - 1);
-    PL_CUDA_TRY(cudaGraphLaunch(ex, s->st));
-    pl::note_launches(1 + (unsigned long long)kChainKernels * len);
-    s->cur ^= (len & 1);
+    for (int r = chunks * kGraphChunk; r < len; ++r) {
+        const int rc = rotation_chain<AS>(s, s->cur, first + r, tr, true);
+        if (rc) return rc;
+        s->cur ^= 1;
+    }
     return PL_OK;
 }
 
@@ -1600,15 +1616,15 @@ int upload_tables(pl_state* s, const std::vector<GateRec<AS>>& recs,
     if (tb > s->table_bytes || pb > s->pairs_bytes) {
         PL_CUDA_TRY(cudaStreamSynchronize(s->st));
         drop_graphs(s);
-        if (s->d_table) dev_free(s->d_table);
-        if (s->d_pairs) dev_free(s->d_pairs);
+        if (s->d_table) dev_free(s->d_table, s->st);
+        if (s->d_pairs) dev_free(s->d_pairs, s->st);
         s->d_table = nullptr;
         s->d_pairs = nullptr;
         s->table_bytes = s->pairs_bytes = 0;
         const size_t tcap = std::max(tb, sizeof(GateRec<AS>) * 16384);
         const size_t pcap = std::max(pb, sizeof(int) * 2 * 16384);
-        PL_CUDA_TRY(dev_alloc(&s->d_table, tcap));
-        PL_CUDA_TRY(dev_alloc(reinterpret_cast<void**>(&s->d_pairs), pcap));
+        PL_CUDA_TRY(dev_alloc(&s->d_table, tcap, s->st));
+        PL_CUDA_TRY(dev_alloc(reinterpret_cast<void**>(&s->d_pairs), pcap, s->st));
         s->table_bytes = tcap;
         s->pairs_bytes = pcap;
     }
@@ -1797,6 +1813,7 @@ extern "C" int pl_state_create(pl_state** out, int array_size, int64_t capacity_
     pl_state* s = new pl_state();
     s->as = array_size;
     s->st = stream;
+    s->ws.st = stream;
     const int rc = state_grow(s, std::max<int64_t>(capacity_hint, 1 << 16));
     if (rc) {
         delete s;
@@ -1811,10 +1828,13 @@ extern "C" int pl_state_destroy(pl_state* s) {
     cudaStreamSynchronize(s->st);
     drop_graphs(s);
     if (s->cap_st) cudaStreamDestroy(s->cap_st);
-    if (s->mem) dev_free(s->mem);
-    if (s->d_table) dev_free(s->d_table);
-    if (s->d_pairs) dev_free(s->d_pairs);
+    if (s->mem) dev_free(s->mem, s->st);
+    if (s->d_table) dev_free(s->d_table, s->st);
+    if (s->d_pairs) dev_free(s->d_pairs, s->st);
     if (s->budget) s->budget->resize(s->held_bytes + s->ws.bytes, 0);
+    if (s->ws.ptr) dev_free(s->ws.ptr, s->st);
+    s->ws.ptr = nullptr;
+    cudaStreamSynchronize(s->st);
     delete s;
     return record_status(PL_OK, nullptr);
 }
@@ -1852,10 +1872,10 @@ int state_shrink(pl_state* s) {
     PL_CUDA_TRY(cudaStreamSynchronize(s->st));
     drop_graphs(s);
     const size_t before = s->held_bytes + s->ws.bytes;
-    if (s->ws.ptr) dev_free(s->ws.ptr);
+    if (s->ws.ptr) dev_free(s->ws.ptr, s->st);
     s->ws.ptr = nullptr;
     s->ws.bytes = 0;
-    if (s->mem) dev_free(s->mem);
+    if (s->mem) dev_free(s->mem, s->st);
     s->mem = nullptr;
     s->cap = 0;
     s->held_bytes = 0;

@@ -51,14 +51,31 @@ int record_cuda(cudaError_t e) {
 }
 
 static std::mutex g_alloc_mu;
-cudaError_t dev_alloc(void** p, size_t bytes) {
-    std::lock_guard<std::mutex> lock(g_alloc_mu);
-    return cudaMalloc(p, bytes);
+static void keep_pool_cached() {
+    static std::mutex mu;
+    static std::vector<bool> done;
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return;
+    std::lock_guard<std::mutex> lock(mu);
+    if ((int)done.size() <= dev) done.resize(dev + 1, false);
+    if (done[dev]) return;
+    cudaMemPool_t pool;
+    if (cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) {
+        uint64_t keep = ~0ull;
+        cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+    }
+    cudaGetLastError();
+    done[dev] = true;
 }
-void dev_free(void* p) {
+cudaError_t dev_alloc(void** p, size_t bytes, cudaStream_t st) {
+    keep_pool_cached();
+    std::lock_guard<std::mutex> lock(g_alloc_mu);
+    return cudaMallocAsync(p, bytes, st);
+}
+void dev_free(void* p, cudaStream_t st) {
     if (!p) return;
     std::lock_guard<std::mutex> lock(g_alloc_mu);
-    cudaFree(p);
+    cudaFreeAsync(p, st);
 }
 void capture_lock() { g_alloc_mu.lock(); }
 void capture_unlock() { g_alloc_mu.unlock(); }
