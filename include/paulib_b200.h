@@ -225,6 +225,14 @@ PL_API int pl_state_sort_and_combine(pl_state* state);
 PL_API int pl_state_cutoff(pl_state* state, double eps);
 PL_API int pl_state_truncate_weight(pl_state* state, uint64_t max_weight);
 PL_API int pl_state_apply_cnot(pl_state* state, int control, int target);
+/* trim(max_terms) (PauliSumUtils.h:331-345): keep the max_terms terms of
+ * largest |c| in their order; among equal |c| at the boundary the lower
+ * index survives (the reference leaves that choice to std::nth_element). */
+PL_API int pl_state_trim(pl_state* state, uint64_t max_terms);
+/* trim(max_terms, keep) (PauliSumUtils.h:347-375): terms whose (x, z)
+ * pattern occurs in `keep` are always kept and the others share what is
+ * left of max_terms. */
+PL_API int pl_state_trim_protected(pl_state* state, uint64_t max_terms, pl_state* keep);
 PL_API int pl_state_zero_state_expectation(pl_state* state, double* result);
 
 /* lhs := lhs * rhs, the outer product in the reference's i*n + j order

@@ -138,6 +138,7 @@ class Oracle(_Impl):
         L.or_cutoff.argtypes = [C.c_void_p, C.c_double]
         L.or_truncate_weight.argtypes = [C.c_void_p, C.c_uint64]
         L.or_trim.argtypes = [C.c_void_p, C.c_uint64]
+        L.or_trim_protected.argtypes = [C.c_void_p, C.c_uint64, C.c_void_p]
         L.or_apply_cnot.argtypes = [C.c_void_p, C.c_uint64, C.c_uint64]
         L.or_zero_state_expectation.restype = C.c_double
         L.or_zero_state_expectation.argtypes = [C.c_void_p]
@@ -162,6 +163,13 @@ class Oracle(_Impl):
 
     def trim(self, p, m):
         return self._inplace(p, self.lib.or_trim, int(m))
+
+    def trim_protected(self, p, m, keep):
+        hk = self._make(keep)
+        try:
+            return self._inplace(p, self.lib.or_trim_protected, int(m), hk)
+        finally:
+            self._free(hk)
 
     def apply_cnot(self, p, c, t):
         return self._inplace(p, self.lib.or_apply_cnot, int(c), int(t))
@@ -233,6 +241,7 @@ class Reference(_Impl):
         L.ref_cutoff.argtypes = [C.c_void_p, C.c_double]
         L.ref_truncate_weight.argtypes = [C.c_void_p, C.c_uint64]
         L.ref_trim.argtypes = [C.c_void_p, C.c_uint64]
+        L.ref_trim_protected.argtypes = [C.c_void_p, C.c_uint64, C.c_void_p]
         L.ref_apply_cnot.argtypes = [C.c_void_p, C.c_uint64, C.c_uint64]
         L.ref_zero_state_expectation.restype = C.c_double
         L.ref_zero_state_expectation.argtypes = [C.c_void_p]
@@ -269,6 +278,13 @@ class Reference(_Impl):
 
     def trim(self, p, m):
         return self._inplace(p, self.lib.ref_trim, int(m))
+
+    def trim_protected(self, p, m, keep):
+        hk = self._make(keep)
+        try:
+            return self._inplace(p, self.lib.ref_trim_protected, int(m), hk)
+        finally:
+            self._free(hk)
 
     def apply_cnot(self, p, c, t):
         return self._inplace(p, self.lib.ref_apply_cnot, int(c), int(t))

@@ -442,6 +442,38 @@ OR_EXPORT void or_trim(or_sum *s, u64 max_terms) {
     free(idx);
 }
 
+/* trim(max_terms, keep) (PauliSumUtils.h:347-375): terms whose (x, z)
+ * pattern occurs in keep are always kept (the reference's XZ hash set;
+ * here a linear scan of the small keep sum); the others compete for what
+ * is left of max_terms by |c|, ties to the lower index as in or_trim. */
+OR_EXPORT void or_trim_protected(or_sum *s, u64 max_terms, const or_sum *keep) {
+    if ((u64)s->n <= max_terms) return;
+    const int as = s->as;
+    u8 *mask = (u8 *)calloc((size_t)s->n, 1);
+    i64 *idx = (i64 *)malloc((size_t)s->n * sizeof(i64));
+    i64 m = 0;
+    for (i64 i = 0; i < s->n; ++i) {
+        int prot = 0;
+        for (i64 j = 0; j < keep->n && !prot; ++j) {
+            int same = 1;
+            for (int k = 0; k < as && same; ++k)
+                same = s->x[k * s->cap + i] == keep->x[k * keep->cap + j] &&
+                       s->z[k * s->cap + i] == keep->z[k * keep->cap + j];
+            prot = same;
+        }
+        if (prot) mask[i] = 1;
+        else idx[m++] = i;
+    }
+    const u64 protected_count = (u64)(s->n - m);
+    const u64 budget = max_terms > protected_count ? max_terms - protected_count : 0;
+    g_trim_v = s->v;
+    qsort(idx, (size_t)m, sizeof(i64), g_trim_cmp);
+    for (i64 i = 0; i < m && (u64)i < budget; ++i) mask[idx[i]] = 1;
+    compact(s, mask);
+    free(mask);
+    free(idx);
+}
+
 /* TruncationOptions (PauliPropagation.h:27-31); "disabled" mirrors the
  * reference's SIZE_MAX / 0 sentinels. */
 typedef struct {

@@ -46,6 +46,7 @@ struct SumBase {
     virtual void propagate(const SumBase* rot, const std::int32_t* ops, i64 n_ops,
                            u64 max_weight, double cutoff, u64 max_terms) = 0;
     virtual void trim(u64 max_terms) = 0;
+    virtual void trim_protected(u64 max_terms, const SumBase* keep) = 0;
 };
 
 template <std::size_t N>
@@ -98,6 +99,9 @@ struct Sum final : SumBase {
         return o;
     }
     void trim(u64 max_terms) override { s.trim((std::size_t)max_terms); }
+    void trim_protected(u64 max_terms, const SumBase* keep) override {
+        s.trim((std::size_t)max_terms, static_cast<const Sum*>(keep)->s);
+    }
     void propagate(const SumBase* rotb, const std::int32_t* ops, i64 n_ops, u64 max_weight,
                    double cutoff, u64 max_terms) override {
         const auto& rot = static_cast<const Sum*>(rotb)->s;
@@ -176,6 +180,9 @@ __attribute__((visibility("default"))) void ref_truncate_weight(void* h, u64 w) 
     ((SumBase*)h)->truncate_weight(w);
 }
 __attribute__((visibility("default"))) void ref_trim(void* h, u64 m) { ((SumBase*)h)->trim(m); }
+__attribute__((visibility("default"))) void ref_trim_protected(void* h, u64 m, const void* k) {
+    ((SumBase*)h)->trim_protected(m, (const SumBase*)k);
+}
 __attribute__((visibility("default"))) void ref_apply_cnot(void* h, u64 c, u64 t) {
     ((SumBase*)h)->apply_cnot(c, t);
 }

@@ -36,6 +36,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstddef>
 #include <cstring>
 #include <map>
 #include <tuple>
@@ -1122,6 +1123,382 @@ __global__ void __launch_bounds__(256) k_cnot_layer(Buf b, const i64* d_n, const
     }
 }
 
+// ---------------------------------------------------------------------------
+// trim(max_terms[, keep]) (PauliSumUtils.h:331-375): keep the max_terms terms
+// of largest |c| in their original order.  The reference's nth_element leaves
+// the choice among equal |c| at the boundary to the library; here (as in the
+// oracle) ties go to the lower index.  Terms whose (x, z) is in the protect
+// list are always kept and do not count against the rest's budget.
+//
+// The magnitude's bit pattern (sign cleared) orders like |c|, so the
+// threshold is a radix select over 64-bit keys: kTrimPasses histogram passes
+// of up to 11 bits, each followed by a one-block pick of the bin holding the
+// k-th largest.  Then per-tile counts of keys above / equal to the threshold,
+// one scan, and an order-preserving emit.  Every step reads the term count
+// from the device, so no host round trip is needed.
+// ---------------------------------------------------------------------------
+constexpr int kTrimBits = 11;
+constexpr int kTrimBins = 1 << kTrimBits;
+constexpr int kTrimPasses = (64 + kTrimBits - 1) / kTrimBits;  // 6
+constexpr int kTrimItems = 8;
+constexpr u32 kTrimTile = kPT * kTrimItems;
+
+struct TrimCtl {
+    u64 prefix;     // key bits decided so far
+    u64 k;          // how many still to select below the decided prefix
+    u64 T;          // threshold key (after the last pick)
+    u64 r;          // how many keys == T are kept
+    u64 protected_n;
+    int keep_all;   // n - protected <= budget: every term survives
+    int pad;
+    u32 hist[kTrimBins];
+};
+
+struct Protect {
+    const u64* x;  // sorted (x words, z words) of the protected strings
+    const u64* z;
+    i64 n;         // 0: nothing protected
+    i64 stride;
+};
+
+__device__ __forceinline__ u64 mag_key(double v) {
+    return (u64)__double_as_longlong(v) & 0x7fffffffffffffffull;
+}
+
+template <int AS>
+__device__ __forceinline__ bool is_protected(const Protect& P, const u64* x, const u64* z) {
+    i64 lo = 0, hi = P.n;
+    while (lo < hi) {
+        const i64 mid = (lo + hi) >> 1;
+        int c = 0;
+#pragma unroll
+        for (int w = 0; w < AS; ++w) {
+            const u64 a = P.x[w * P.stride + mid];
+            if (c == 0 && a != x[w]) c = a < x[w] ? -1 : 1;
+        }
+#pragma unroll
+        for (int w = 0; w < AS; ++w) {
+            const u64 a = P.z[w * P.stride + mid];
+            if (c == 0 && a != z[w]) c = a < z[w] ? -1 : 1;
+        }
+        if (c == 0) return true;
+        if (c < 0) lo = mid + 1;
+        else hi = mid;
+    }
+    return false;
+}
+
+template <int AS>
+__device__ __forceinline__ bool term_protected(const Buf& b, i64 i, const Protect& P) {
+    if (P.n == 0) return false;
+    u64 x[AS], z[AS];
+#pragma unroll
+    for (int w = 0; w < AS; ++w) {
+        x[w] = b.x[w * b.cap + i];
+        z[w] = b.z[w * b.cap + i];
+    }
+    return is_protected<AS>(P, x, z);
+}
+
+// Count the protected terms and set up the select.
+template <int AS>
+__global__ void __launch_bounds__(256) k_trim_init(Buf b, const i64* d_n, u64 max_terms,
+                                                   Protect P, TrimCtl* C, const int* status) {
+    if (status_set(status)) return;
+    const i64 n = *d_n;
+    u32 cnt = 0;
+    if (P.n > 0)
+        for (i64 i = (i64)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+             i += (i64)gridDim.x * blockDim.x)
+            cnt += term_protected<AS>(b, i, P) ? 1u : 0u;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) cnt += __shfl_xor_sync(0xffffffffu, cnt, o);
+    if ((threadIdx.x & 31) == 0 && cnt) atomicAdd((unsigned long long*)&C->protected_n, cnt);
+}
+
+__global__ void __launch_bounds__(256) k_trim_setup(const i64* d_n, u64 max_terms, TrimCtl* C) {
+    const i64 n = *d_n;
+    const u64 prot = C->protected_n;
+    const u64 rest = (u64)n - prot;
+    const u64 budget = max_terms > prot ? max_terms - prot : 0;
+    for (int i = threadIdx.x; i < kTrimBins; i += blockDim.x) C->hist[i] = 0;
+    if (threadIdx.x == 0) {
+        C->prefix = 0;
+        C->k = budget;
+        C->keep_all = (u64)n <= max_terms || rest <= budget;
+        C->T = 0;
+        C->r = 0;
+    }
+}
+
+// Histogram of key bits [shift, shift + bits) over unprotected keys whose
+// bits above shift + bits equal the decided prefix.
+template <int AS>
+__global__ void __launch_bounds__(256) k_trim_hist(Buf b, const i64* d_n, Protect P, TrimCtl* C,
+                                                   int shift, int bits) {
+    __shared__ u32 sh[kTrimBins];
+    if (C->keep_all || C->k == 0) return;
+    for (int i = threadIdx.x; i < kTrimBins; i += blockDim.x) sh[i] = 0;
+    __syncthreads();
+    const i64 n = *d_n;
+    const int hi = shift + bits;
+    const u64 pre = C->prefix;
+    const u32 dmask = (1u << bits) - 1u;
+    for (i64 i = (i64)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+         i += (i64)gridDim.x * blockDim.x) {
+        const u64 key = mag_key(b.v[i]);
+        if (hi < 64 && (key >> hi) != (pre >> hi)) continue;
+        if (term_protected<AS>(b, i, P)) continue;
+        atomicAdd(&sh[(u32)(key >> shift) & dmask], 1u);
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < kTrimBins; i += blockDim.x)
+        if (sh[i]) atomicAdd(&C->hist[i], sh[i]);
+}
+
+// One block: the bin (from the top) holding the k-th largest key.
+__global__ void __launch_bounds__(32) k_trim_pick(TrimCtl* C, int shift, int bits, int last) {
+    if (C->keep_all) return;
+    if (threadIdx.x == 0) {
+        u64 k = C->k;
+        if (k > 0) {
+            const int nb = 1 << bits;
+            u64 cum = 0;
+            int bin = 0;
+            for (int d = nb - 1; d >= 0; --d) {
+                const u64 c = C->hist[d];
+                if (cum + c >= k) {
+                    bin = d;
+                    break;
+                }
+                cum += c;
+            }
+            C->prefix |= (u64)bin << shift;
+            C->k = k - cum;
+        }
+        if (last) {
+            // k == 0 (nothing to select): no unprotected key survives
+            C->T = C->k == 0 ? ~0ull : C->prefix;
+            C->r = C->k;
+        }
+    }
+    __syncwarp();
+    for (int i = threadIdx.x; i < kTrimBins; i += 32) C->hist[i] = 0;
+}
+
+__device__ __forceinline__ bool trim_above(const TrimCtl& C, u64 key) {
+    return C.keep_all || (C.T != ~0ull && key > C.T);
+}
+__device__ __forceinline__ bool trim_tie(const TrimCtl& C, u64 key) {
+    return !C.keep_all && C.T != ~0ull && key == C.T;
+}
+
+// Per tile: terms kept for sure (above the threshold or protected) and ties.
+template <int AS>
+__global__ void __launch_bounds__(kPT) k_trim_count(Buf b, const i64* d_n, Protect P,
+                                                    const TrimCtl* Cp, u32* gt, u32* eq,
+                                                    const int* status) {
+    __shared__ u32 s_gt[kPT / 32], s_eq[kPT / 32];
+    if (status_set(status)) return;
+    const TrimCtl& C = *Cp;
+    const i64 n = *d_n;
+    const u32 ntiles = (u32)((n + kTrimTile - 1) / kTrimTile);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (u32 tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+        const i64 wbase = (i64)tile * kTrimTile + warp * (kTrimItems * 32);
+        u32 g = 0, e = 0;
+#pragma unroll
+        for (int t = 0; t < kTrimItems; ++t) {
+            const i64 i = wbase + t * 32 + lane;
+            if (i >= n) continue;
+            const u64 key = mag_key(b.v[i]);
+            if (trim_above(C, key) || term_protected<AS>(b, i, P)) ++g;
+            else if (trim_tie(C, key)) ++e;
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            g += __shfl_xor_sync(0xffffffffu, g, o);
+            e += __shfl_xor_sync(0xffffffffu, e, o);
+        }
+        if (lane == 0) {
+            s_gt[warp] = g;
+            s_eq[warp] = e;
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            u32 tg = 0, te = 0;
+            for (int w = 0; w < kPT / 32; ++w) {
+                tg += s_gt[w];
+                te += s_eq[w];
+            }
+            gt[tile] = tg;
+            eq[tile] = te;
+        }
+        __syncthreads();
+    }
+}
+
+// One block: tie offsets, kept counts and kept offsets per tile; the output
+// size.  eq[] is replaced by its exclusive scan, gt[] by the kept offsets.
+__global__ void __launch_bounds__(1024) k_trim_scan(const i64* d_n, const TrimCtl* Cp, u32* gt,
+                                                    u32* eq, i64* d_out, const int* status) {
+    __shared__ u32 sw[33];
+    __shared__ u64 s_carry[2];
+    if (status_set(status)) return;
+    const i64 n = *d_n;
+    const u32 ntiles = (u32)((n + kTrimTile - 1) / kTrimTile);
+    const u64 r = Cp->r;
+    if (threadIdx.x == 0) s_carry[0] = s_carry[1] = 0;
+    __syncthreads();
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (u32 base = 0; base < ntiles; base += 1024) {
+        const u32 t = base + threadIdx.x;
+        const u32 e = t < ntiles ? eq[t] : 0u;
+        const u32 g = t < ntiles ? gt[t] : 0u;
+        // scan of ties
+        u32 inc = e;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const u32 v = __shfl_up_sync(0xffffffffu, inc, o);
+            if (lane >= o) inc += v;
+        }
+        if (lane == 31) sw[warp] = inc;
+        __syncthreads();
+        if (warp == 0) {
+            u32 c = sw[lane], ci = c;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const u32 v = __shfl_up_sync(0xffffffffu, ci, o);
+                if (lane >= o) ci += v;
+            }
+            sw[lane] = ci - c;
+            if (lane == 31) sw[32] = ci;
+        }
+        __syncthreads();
+        const u64 eoff = s_carry[0] + sw[warp] + (inc - e);
+        const u32 etot = sw[32];
+        __syncthreads();
+        const u64 keep_ties = eoff >= r ? 0 : (r - eoff < e ? r - eoff : e);
+        const u32 kept = g + (u32)keep_ties;
+        // scan of kept
+        inc = kept;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const u32 v = __shfl_up_sync(0xffffffffu, inc, o);
+            if (lane >= o) inc += v;
+        }
+        if (lane == 31) sw[warp] = inc;
+        __syncthreads();
+        if (warp == 0) {
+            u32 c = sw[lane], ci = c;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const u32 v = __shfl_up_sync(0xffffffffu, ci, o);
+                if (lane >= o) ci += v;
+            }
+            sw[lane] = ci - c;
+            if (lane == 31) sw[32] = ci;
+        }
+        __syncthreads();
+        const u64 koff = s_carry[1] + sw[warp] + (inc - kept);
+        const u32 ktot = sw[32];
+        if (t < ntiles) {
+            eq[t] = (u32)eoff;
+            gt[t] = (u32)koff;
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            s_carry[0] += etot;
+            s_carry[1] += ktot;
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) *d_out = (i64)s_carry[1];
+}
+
+// Order-preserving emit of the survivors into out.
+template <int AS>
+__global__ void __launch_bounds__(kPT) k_trim_emit(Buf b, const i64* d_n, Protect P,
+                                                   const TrimCtl* Cp, const u32* koff,
+                                                   const u32* eoff, Buf out, int* status) {
+    __shared__ u32 s_k[kPT / 32], s_e[kPT / 32];
+    if (status_set(status)) return;
+    const TrimCtl& C = *Cp;
+    const i64 n = *d_n;
+    const u32 ntiles = (u32)((n + kTrimTile - 1) / kTrimTile);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (u32 tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+        const i64 wbase = (i64)tile * kTrimTile + warp * (kTrimItems * 32);
+        // warp prefix of ties and of sure survivors, in item order
+        u32 sure = 0, tie = 0;
+        u32 cs = 0, ce = 0;
+#pragma unroll
+        for (int t = 0; t < kTrimItems; ++t) {
+            const i64 i = wbase + t * 32 + lane;
+            bool s = false, e = false;
+            if (i < n) {
+                const u64 key = mag_key(b.v[i]);
+                s = trim_above(C, key) || term_protected<AS>(b, i, P);
+                e = !s && trim_tie(C, key);
+            }
+            const u32 bs = __ballot_sync(0xffffffffu, s), be = __ballot_sync(0xffffffffu, e);
+            if (s) sure |= 1u << t;
+            if (e) tie |= 1u << t;
+            cs += __popc(bs);
+            ce += __popc(be);
+        }
+        if (lane == 0) {
+            s_k[warp] = cs;
+            s_e[warp] = ce;
+        }
+        __syncthreads();
+        u32 we = 0;
+        for (int w = 0; w < warp; ++w) we += s_e[w];
+        // ties before this warp, then kept terms before this warp
+        const u64 tie0 = (u64)eoff[tile] + we;
+        u32 wk = 0;
+        {
+            // kept before this warp = sure before + ties kept before
+            u32 ties_before = 0, sure_before = 0;
+            for (int w = 0; w < warp; ++w) {
+                sure_before += s_k[w];
+                ties_before += s_e[w];
+            }
+            const u64 e0 = (u64)eoff[tile];
+            const u64 kt = e0 >= C.r ? 0 : (C.r - e0 < ties_before ? C.r - e0 : ties_before);
+            wk = sure_before + (u32)kt;
+        }
+        u64 o = (u64)koff[tile] + wk;
+        u64 tr = tie0;  // rank of the next tie
+#pragma unroll
+        for (int t = 0; t < kTrimItems; ++t) {
+            const i64 i = wbase + t * 32 + lane;
+            const bool s = (sure >> t) & 1u, e = (tie >> t) & 1u;
+            const u32 be = __ballot_sync(0xffffffffu, e);
+            const u64 my_rank = tr + __popc(be & lanemask_lt());
+            const bool keep = s || (e && my_rank < C.r);
+            const u32 bk = __ballot_sync(0xffffffffu, keep);
+            const u64 pos = o + __popc(bk & lanemask_lt());
+            if (keep) {
+                if ((i64)pos >= out.cap) {
+                    raise_status(status, PL_ERR_INTERNAL);
+                } else {
+#pragma unroll
+                    for (int w = 0; w < AS; ++w) {
+                        out.x[w * out.cap + pos] = b.x[w * b.cap + i];
+                        out.z[w * out.cap + pos] = b.z[w * b.cap + i];
+                    }
+                    out.f[pos] = b.f[i];
+                    out.v[pos] = b.v[i];
+                }
+            }
+            o += __popc(bk);
+            tr += __popc(be);
+        }
+        __syncthreads();
+    }
+}
+
 // isCloseOne (PauliSumOperations.h:19-21).
 bool close_one(double v) { return std::fabs(v - 1.0) <= 1e-14; }
 
@@ -1166,6 +1543,8 @@ struct pl_state {
     pl::MemBudget* budget = nullptr;
     size_t held_bytes = 0;    // device bytes of mem (counted against budget)
     cudaStream_t cap_st = nullptr;  // private stream the chains are captured on
+    void* trim_mem = nullptr;       // trim control block and per-tile counts
+    size_t trim_bytes = 0;
 };
 
 namespace pl {
@@ -1586,6 +1965,49 @@ int general_rotation(pl_state* s, const Rot& r, bool truncate, const pl_truncati
     return PL_OK;
 }
 
+// trim(max_terms[, protect]) of S[cur] into S[1-cur], all on the stream (the
+// term count stays on the device).  Terms kept in their original order.
+template <int AS>
+int trim_state(pl_state* s, u64 max_terms, const Protect& P) {
+    const size_t tiles = (size_t)(s->cap / kTrimTile) + 2;
+    const size_t need = a256(sizeof(TrimCtl)) + 2 * a256(4 * tiles);
+    if (need > s->trim_bytes) {
+        if (s->trim_mem) dev_free(s->trim_mem, s->st);
+        s->trim_mem = nullptr;
+        s->trim_bytes = 0;
+        PL_CUDA_TRY(dev_alloc(&s->trim_mem, need, s->st));
+        s->trim_bytes = need;
+    }
+    auto* C = static_cast<TrimCtl*>(s->trim_mem);
+    u32* gt = reinterpret_cast<u32*>(static_cast<unsigned char*>(s->trim_mem) +
+                                     a256(sizeof(TrimCtl)));
+    u32* eq = gt + a256(4 * tiles) / 4;
+    const int in = s->cur, outb = 1 - s->cur;
+    const i64* d_n = s->d_size + in;
+    PL_CUDA_TRY(cudaMemsetAsync(C, 0, offsetof(TrimCtl, hist), s->st));
+    if (P.n > 0)
+        k_trim_init<AS><<<grid_persistent(4), 256, 0, s->st>>>(s->S[in], d_n, max_terms, P, C,
+                                                               s->d_status), pl::note_launch();
+    k_trim_setup<<<1, 256, 0, s->st>>>(d_n, max_terms, C), pl::note_launch();
+    for (int p = 0; p < kTrimPasses; ++p) {
+        const int shift = std::max(0, 64 - kTrimBits * (p + 1));
+        const int bits = 64 - kTrimBits * p - shift;
+        k_trim_hist<AS><<<grid_persistent(4), 256, 0, s->st>>>(s->S[in], d_n, P, C, shift, bits),
+            pl::note_launch();
+        k_trim_pick<<<1, 32, 0, s->st>>>(C, shift, bits, p == kTrimPasses - 1), pl::note_launch();
+    }
+    k_trim_count<AS><<<grid_persistent(4), kPT, 0, s->st>>>(s->S[in], d_n, P, C, gt, eq,
+                                                           s->d_status), pl::note_launch();
+    k_trim_scan<<<1, 1024, 0, s->st>>>(d_n, C, gt, eq, s->d_size + outb, s->d_status),
+        pl::note_launch();
+    k_trim_emit<AS><<<grid_persistent(4), kPT, 0, s->st>>>(s->S[in], d_n, P, C, gt, eq,
+                                                          s->S[outb], s->d_status),
+        pl::note_launch();
+    PL_CUDA_TRY(cudaGetLastError());
+    s->cur = outb;
+    return PL_OK;
+}
+
 // Make a state of class 1 (distinct keys) canonical: sort by (x, z, phase),
 // folding signs (values then carry the sign; see the header comment).
 int state_canonical_sort(pl_state* s) {
@@ -1641,8 +2063,8 @@ constexpr int kGraphMin = 8;  // shortest run of rotations replayed from a graph
 template <int AS>
 int run_ops(pl_state* s, const std::vector<Rot>& rots, const std::vector<Op>& ops,
             const pl_truncation& tr) {
-    if (tr.max_terms != ~0ull)
-        return record_status(PL_ERR_UNSUPPORTED, "max_terms truncation (trim) is not built");
+    const bool trimming = tr.max_terms != ~0ull;
+    const Protect no_protect{nullptr, nullptr, 0, 0};
     int rc = set_smem_attrs<AS>();
     if (rc) return rc;
     // per-rotation parameters, then one record per op for the device
@@ -1737,7 +2159,7 @@ int run_ops(pl_state* s, const std::vector<Rot>& rots, const std::vector<Op>& op
                 size_t j = i;
                 while (j < ops.size() && ops[j].kind == 0 && singles[ops[j].a]) ++j;
                 const int len = (int)(j - i);
-                if (s->use_graphs && len >= kGraphMin && !timing_enabled()) {
+                if (s->use_graphs && !trimming && len >= kGraphMin && !timing_enabled()) {
                     for (int q = 0; q < len; ++q) in_buf[i + q] = s->cur ^ (q & 1);
                     rc = rotation_graph<AS>(s, (int)i, len, tr);
                     if (rc) return rc;
@@ -1754,11 +2176,21 @@ int run_ops(pl_state* s, const std::vector<Rot>& rots, const std::vector<Op>& op
                         if (rc) return rc;
                         s->cur ^= 1;
                     }
+                    if (trimming) {
+                        rc = trim_state<AS>(s, tr.max_terms, no_protect);
+                        if (rc) return rc;
+                    }
                     ++i;
                     ++since_sync;
                 }
                 pending = true;
             } else if (modes[r] == kSkip && s->cls == 2) {
+                if (trimming) {
+                    in_buf[i] = s->cur;
+                    rc = trim_state<AS>(s, tr.max_terms, no_protect);
+                    if (rc) return rc;
+                    pending = true;
+                }
                 ++i;
             } else {
                 // general path (synchronous)
@@ -1767,6 +2199,10 @@ int run_ops(pl_state* s, const std::vector<Rot>& rots, const std::vector<Op>& op
                 if (rewound) continue;
                 rc = general_rotation<AS>(s, rots[r], true, tr);
                 if (rc) return rc;
+                if (trimming) {
+                    rc = trim_state<AS>(s, tr.max_terms, no_protect);
+                    if (rc) return rc;
+                }
                 ++i;
             }
         }
@@ -1834,6 +2270,7 @@ extern "C" int pl_state_destroy(pl_state* s) {
     if (s->budget) s->budget->resize(s->held_bytes + s->ws.bytes, 0);
     if (s->ws.ptr) dev_free(s->ws.ptr, s->st);
     s->ws.ptr = nullptr;
+    if (s->trim_mem) dev_free(s->trim_mem, s->st);
     cudaStreamSynchronize(s->st);
     delete s;
     return record_status(PL_OK, nullptr);
@@ -1994,12 +2431,80 @@ extern "C" int pl_state_canonicalize(pl_state* s) {
 extern "C" int pl_state_sort_and_combine(pl_state* s) {
     return collate_state_api(s, kCombine, 0.0, ~0ull);
 }
+static int trim_api(pl_state* s, uint64_t max_terms, pl_state* keep) {
+    int rc = check_state(s);
+    if (rc) return rc;
+    Protect P{nullptr, nullptr, 0, 0};
+    void* prot = nullptr;
+    if (keep) {
+        rc = check_state(keep);
+        if (rc) return rc;
+        if (keep->as != s->as) return record_status(PL_ERR_INVALID_ARG, "trim: keep array_size");
+        // the protected (x, z) patterns, sorted on the host (the keep set is
+        // small: the observable at t = 0 in the reference's use)
+        i64 kn = 0;
+        rc = read_size(keep, &kn);
+        if (rc) return rc;
+        if (kn > 0) {
+            const int as = s->as;
+            std::vector<u64> kx((size_t)as * kn), kz((size_t)as * kn);
+            const Buf& b = keep->S[keep->cur];
+            PL_CUDA_TRY(cudaMemcpy2DAsync(kx.data(), 8 * kn, b.x, 8 * b.cap, 8 * kn, as,
+                                          cudaMemcpyDeviceToHost, keep->st));
+            PL_CUDA_TRY(cudaMemcpy2DAsync(kz.data(), 8 * kn, b.z, 8 * b.cap, 8 * kn, as,
+                                          cudaMemcpyDeviceToHost, keep->st));
+            PL_CUDA_TRY(cudaStreamSynchronize(keep->st));
+            std::vector<i64> idx((size_t)kn);
+            for (i64 i = 0; i < kn; ++i) idx[(size_t)i] = i;
+            auto key_less = [&](i64 a, i64 c) {
+                for (int w = 0; w < as; ++w)
+                    if (kx[(size_t)w * kn + a] != kx[(size_t)w * kn + c])
+                        return kx[(size_t)w * kn + a] < kx[(size_t)w * kn + c];
+                for (int w = 0; w < as; ++w)
+                    if (kz[(size_t)w * kn + a] != kz[(size_t)w * kn + c])
+                        return kz[(size_t)w * kn + a] < kz[(size_t)w * kn + c];
+                return false;
+            };
+            std::sort(idx.begin(), idx.end(), key_less);
+            std::vector<u64> sx((size_t)as * kn), sz((size_t)as * kn);
+            for (i64 i = 0; i < kn; ++i)
+                for (int w = 0; w < as; ++w) {
+                    sx[(size_t)w * kn + i] = kx[(size_t)w * kn + idx[(size_t)i]];
+                    sz[(size_t)w * kn + i] = kz[(size_t)w * kn + idx[(size_t)i]];
+                }
+            PL_CUDA_TRY(dev_alloc(&prot, 16 * (size_t)as * kn, s->st));
+            u64* px = static_cast<u64*>(prot);
+            PL_CUDA_TRY(cudaMemcpyAsync(px, sx.data(), 8 * (size_t)as * kn, cudaMemcpyHostToDevice,
+                                        s->st));
+            PL_CUDA_TRY(cudaMemcpyAsync(px + (size_t)as * kn, sz.data(), 8 * (size_t)as * kn,
+                                        cudaMemcpyHostToDevice, s->st));
+            P = Protect{px, px + (size_t)as * kn, kn, kn};
+        }
+    }
+    PL_DISPATCH_AS(s->as, rc = trim_state<AS>(s, max_terms, P));
+    if (prot) dev_free(prot, s->st);
+    if (rc) return rc;
+    int st = 0, fail = 0;
+    rc = read_status(s, &st, &fail);
+    if (rc) return rc;
+    if (st) return record_status(st, "trim");
+    return record_status(PL_OK, nullptr);
+}
+
+extern "C" int pl_state_trim(pl_state* s, uint64_t max_terms) {
+    return trim_api(s, max_terms, nullptr);
+}
+extern "C" int pl_state_trim_protected(pl_state* s, uint64_t max_terms, pl_state* keep) {
+    return trim_api(s, max_terms, keep);
+}
+
 extern "C" int pl_state_apply_truncation(pl_state* s, const pl_truncation* o) {
     if (!o) return record_status(PL_ERR_INVALID_ARG, "pl_state_apply_truncation");
-    if (o->max_terms != ~0ull)
-        return record_status(PL_ERR_UNSUPPORTED, "max_terms truncation (trim) is not built");
-    return collate_state_api(s, kCanon, o->coefficient_cutoff > 0 ? o->coefficient_cutoff : 0.0,
-                             o->max_weight);
+    const int rc = collate_state_api(s, kCanon,
+                                     o->coefficient_cutoff > 0 ? o->coefficient_cutoff : 0.0,
+                                     o->max_weight);
+    if (rc || o->max_terms == ~0ull) return rc;
+    return trim_api(s, o->max_terms, nullptr);
 }
 
 static int filter_state(pl_state* s, double eps, uint64_t max_weight) {

@@ -118,6 +118,13 @@ class State:
     def truncate_weight(self, w):
         _abi.check(self._lib.pl_state_truncate_weight(self._h, int(w)), "pl_state_truncate_weight")
 
+    def trim(self, max_terms, keep: "State | None" = None):
+        if keep is None:
+            _abi.check(self._lib.pl_state_trim(self._h, int(max_terms)), "pl_state_trim")
+        else:
+            _abi.check(self._lib.pl_state_trim_protected(self._h, int(max_terms), keep._h),
+                       "pl_state_trim_protected")
+
     def apply_cnot(self, c, t):
         _abi.check(self._lib.pl_state_apply_cnot(self._h, int(c), int(t)), "pl_state_apply_cnot")
 

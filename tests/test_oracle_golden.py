@@ -222,3 +222,22 @@ def test_commutator_values(impl):
     assert to_str(c, 1) == "6.000000 * -iY\n"
     ic = impl.commutator(planes([("X", 1.5)]), planes([("Z", 2.0)]), mul_i=True)
     assert to_str(ic, 1) == "6.000000 * Y\n"
+
+
+# PauliSumTests.cpp:1113-1137 -- trim keeps the largest |c|; a keep set
+# protects its patterns and the rest share what is left of the budget.
+def _terms(impl_out, nq):
+    from paulib_b200 import strings
+    return {strings.fmt(impl_out.x[:, i], impl_out.z[:, i], impl_out.flags[i], nq):
+            float(impl_out.val[i]) for i in range(impl_out.n)}
+
+
+def test_trim_keeps_largest(impl):
+    s = planes([("XI", 0.1), ("ZI", -5.0), ("IZ", 0.3), ("YI", 2.0)])
+    assert _terms(impl.trim(s, 2), 2) == {"ZI": -5.0, "YI": 2.0}
+
+
+def test_trim_protects_keep_patterns(impl):
+    s = planes([("XI", 0.001), ("ZI", -5.0), ("IZ", 0.3), ("YI", 2.0)])
+    keep = planes([("XI", 1.0)])
+    assert _terms(impl.trim_protected(s, 2, keep), 2) == {"XI": 0.001, "ZI": -5.0}

@@ -87,3 +87,22 @@ def test_propagation_rotation_only(oracle, reference):
     r = reference.propagate(obs, rot, None, max_weight=6, cutoff=1e-3)
     assert_keys_equal(o, r)
     assert bit_identical(o, r)
+
+
+@pytest.mark.parametrize("words,n,m", [(1, 3000, 1000), (2, 2000, 1999), (4, 500, 10)])
+def test_trim(oracle, reference, words, n, m):
+    # N(0,1) coefficients: no ties at the boundary, so nth_element's choice
+    # and the restatement's lower-index rule pick the same terms
+    s = random_sum(n, words, 31 + words, None, "normal")
+    o, r = oracle.trim(s, m), reference.trim(s, m)
+    assert_keys_equal(o, r)
+    assert bit_identical(o, r)
+
+
+def test_trim_protected(oracle, reference):
+    s = random_sum(2000, 1, 41, 30, "normal")
+    keep = Planes(s.x[:, ::97].copy(), s.z[:, ::97].copy(), s.flags[::97].copy(),
+                  np.ones(s.x[:, ::97].shape[1]))
+    o, r = oracle.trim_protected(s, 300, keep), reference.trim_protected(s, 300, keep)
+    assert_keys_equal(o, r)
+    assert bit_identical(o, r)
