@@ -246,6 +246,10 @@ PL_API int pl_state_multiply_canonicalize(pl_state* lhs, pl_state* rhs);
  * reference's single-threaded CPU order (commutator / i_commutator,
  * PauliSumOperations.h:316-356). */
 PL_API int pl_state_commutator(pl_state* out, pl_state* a, pl_state* b, int multiply_by_i);
+/* dst := dst followed by the terms of src (PauliSum::add, PauliSumCore.h:
+ * 210-237, before its merge); the reference's `+=` is this followed by
+ * pl_state_sort_and_combine. */
+PL_API int pl_state_append(pl_state* dst, pl_state* src);
 
 /* propagate (PauliPropagation.h:54-63): ops walked in reverse; a rotation
  * is evolve + apply_truncation, a CNOT is apply_CNOT.  ops == NULL means

@@ -43,7 +43,7 @@ EXPORTS = (
     "pl_profile_reset", "pl_profile_read", "pl_state_multiply",
     "pl_state_multiply_canonicalize", "pl_state_commutator", "pl_profile_report",
     "pl_commutator_noalloc", "pl_state_set_option", "pl_state_memory", "pl_batch_propagate",
-    "pl_serve", "pl_state_trim", "pl_state_trim_protected",
+    "pl_serve", "pl_state_trim", "pl_state_trim_protected", "pl_state_append",
 )
 PL_OPT_GRAPHS = 1
 PL_ORDER_GIVEN = 0
@@ -144,6 +144,7 @@ def lib():
         "pl_state_commutator": (I32, [VP, VP, VP, I32]),
         "pl_state_set_option": (I32, [VP, I32, I64]),
         "pl_state_trim": (I32, [VP, C.c_uint64]),
+        "pl_state_append": (I32, [VP, VP]),
         "pl_state_trim_protected": (I32, [VP, C.c_uint64, VP]),
         "pl_state_memory": (I32, [VP, C.POINTER(C.c_uint64)]),
         "pl_batch_propagate": (I32, [C.POINTER(Job), I64, C.POINTER(BatchOpts),

@@ -2686,6 +2686,40 @@ extern "C" int pl_state_multiply_canonicalize(pl_state* lhs, pl_state* rhs) {
     return record_status(PL_ERR_INTERNAL, "pl_state_multiply_canonicalize");
 }
 
+// dst := dst followed by src's terms (PauliSum::add without the merge,
+// PauliSumCore.h:210-237); `+=` is this then pl_state_sort_and_combine.
+extern "C" int pl_state_append(pl_state* dst, pl_state* src) {
+    int rc = check_state(dst);
+    if (rc) return rc;
+    if ((rc = check_state(src))) return rc;
+    if (dst == src || dst->as != src->as)
+        return record_status(PL_ERR_INVALID_ARG, "pl_state_append: operands");
+    i64 n = 0, m = 0;
+    if ((rc = read_size(dst, &n)) || (rc = read_size(src, &m))) return rc;
+    if (src->st != dst->st) PL_CUDA_TRY(cudaStreamSynchronize(src->st));
+    if (n + m >= (1ll << 30)) return record_status(PL_ERR_INVALID_ARG, "pl_state_append: size");
+    if (n + m > dst->cap) {
+        rc = state_grow(dst, n + m);
+        if (rc) return rc;
+    }
+    const Buf& d = dst->S[dst->cur];
+    const Buf& b = src->S[src->cur];
+    if (m > 0) {
+        PL_CUDA_TRY(cudaMemcpy2DAsync(d.x + n, 8 * d.cap, b.x, 8 * b.cap, 8 * m, dst->as,
+                                      cudaMemcpyDeviceToDevice, dst->st));
+        PL_CUDA_TRY(cudaMemcpy2DAsync(d.z + n, 8 * d.cap, b.z, 8 * b.cap, 8 * m, dst->as,
+                                      cudaMemcpyDeviceToDevice, dst->st));
+        PL_CUDA_TRY(cudaMemcpyAsync(d.f + n, b.f, m, cudaMemcpyDeviceToDevice, dst->st));
+        PL_CUDA_TRY(cudaMemcpyAsync(d.v + n, b.v, 8 * m, cudaMemcpyDeviceToDevice, dst->st));
+    }
+    const i64 nm = n + m;
+    PL_CUDA_TRY(cudaMemcpyAsync(dst->d_size + dst->cur, &nm, sizeof(i64), cudaMemcpyHostToDevice,
+                                dst->st));
+    PL_CUDA_TRY(cudaStreamSynchronize(dst->st));
+    dst->cls = 0;
+    return record_status(PL_OK, nullptr);
+}
+
 extern "C" int pl_state_commutator(pl_state* out, pl_state* a, pl_state* b, int multiply_by_i) {
     int rc = check_state(out);
     if (rc) return rc;

@@ -1,0 +1,223 @@
+"""The reference's Python surface (python/paulib/__init__.py:64-159 and the
+PauliSum_<N> bindings, python/bindings.cpp:138-298) for the hot path, on
+device-resident sums.
+
+    from paulib_b200.paulib import PauliSum, TruncationOptions, commutator
+    soa = PauliSum([("XYZZ", 0.5), ("ZZZY", 1.2)])
+    soa.canonicalize()
+
+Same names, argument meanings and exception types (ValueError for bad
+input, IndexError for a bad term index).  Every method runs on the GPU
+through the C ABI; there is no CPU path.
+"""
+from __future__ import annotations
+
+from typing import Sequence, Tuple, Union
+
+import numpy as np
+
+from . import _abi
+from . import strings
+from .propagation import State
+
+MAX_QUBITS = 64 * 16
+
+
+class TruncationOptions:
+    """TruncationOptions<double> (PauliPropagation.h:27-31)."""
+
+    def __init__(self, max_weight=None, coefficient_cutoff=0.0, max_terms=None):
+        self.max_weight = max_weight
+        self.coefficient_cutoff = coefficient_cutoff
+        self.max_terms = max_terms
+
+
+def _capacity_words(n: int) -> int:
+    if n < 1:
+        raise ValueError("Qubit count must be at least 1.")
+    if n > MAX_QUBITS:
+        raise ValueError(f"Qubit count {n} exceeds the maximum of {MAX_QUBITS} qubits.")
+    return (n + 63) // 64
+
+
+def _count_qubits(s: str) -> int:
+    i = 0
+    if i < len(s) and s[i] in "+-":
+        i += 1
+    if i < len(s) and s[i] == "i":
+        i += 1
+    return len(s) - i
+
+
+def _checked(fn, *args):
+    try:
+        return fn(*args)
+    except _abi.PLError as e:
+        if e.status == _abi.PL_ERR_INVALID_ARG:
+            raise ValueError(str(e)) from None
+        raise
+
+
+class _PauliSum:
+    """A Pauli sum with FP64 coefficients kept in device memory."""
+
+    def __init__(self, num_qubits: int, x=None, z=None, f=None, v=None, state=None):
+        self._nq = int(num_qubits)
+        self._aw = _capacity_words(self._nq)
+        self._st = state if state is not None else State(self._aw)
+        if v is not None:
+            self._st.upload(x, z, f, v)
+
+    # -- accessors -------------------------------------------------------
+    def num_qubits(self) -> int:
+        return self._nq
+
+    def __len__(self) -> int:
+        return self._st.size()
+
+    @property
+    def coefficients(self):
+        return list(self._st.download()[3])
+
+    def planes(self):
+        """(x (AS, n), z (AS, n), flags, values) copied to the host."""
+        return self._st.download()
+
+    def get_str(self) -> str:
+        x, z, f, v = self._st.download()
+        return strings.get_str(x, z, f, v, self._nq)
+
+    __str__ = get_str
+    __repr__ = get_str
+
+    def __getitem__(self, i: int):
+        x, z, f, v = self._st.download()
+        if not 0 <= i < v.shape[0]:
+            raise IndexError("term index out of range")
+        return strings.fmt(x[:, i], z[:, i], f[i], self._nq), float(v[i])
+
+    def _check_same(self, other):
+        if not isinstance(other, _PauliSum):
+            raise TypeError("expected a PauliSum")
+        if other._nq != self._nq:
+            raise ValueError("Pauli sums have different qubit counts")
+
+    def _copy(self) -> "_PauliSum":
+        out = _PauliSum(self._nq)
+        _checked(out._st._lib.pl_state_append, out._st._h, self._st._h)
+        return out
+
+    # -- hot-path methods (reference names) ------------------------------
+    def collate(self):
+        """sort_and_combine (PauliSumOperations.h:369-461)."""
+        self._st.sort_and_combine()
+
+    def canonicalize(self):
+        self._st.canonicalize()
+
+    def cutoff(self, eps: float):
+        self._st.cutoff(eps)
+
+    def truncate_weight(self, max_weight: int):
+        self._st.truncate_weight(max_weight)
+
+    def trim(self, max_terms: int, keep: "_PauliSum | None" = None):
+        if keep is not None:
+            self._check_same(keep)
+        self._st.trim(max_terms, None if keep is None else keep._st)
+
+    def multiply(self, rhs: "_PauliSum"):
+        """self := self * rhs (polynomial product, PauliSumOperations.h:256-306)."""
+        self._check_same(rhs)
+        _checked(_abi.check, self._st._lib.pl_state_multiply(self._st._h, rhs._st._h),
+                 "pl_state_multiply")
+
+    def evolve(self, rotations: "_PauliSum"):
+        """Apply the rotations (generator = term, angle = coefficient) in order."""
+        self._check_same(rotations)
+        x, z, f, v = rotations._st.download()
+        self._st.evolve(x, z, f, v)
+
+    def apply_CNOT(self, control: int, target: int):
+        if not (0 <= control < self._nq and 0 <= target < self._nq):
+            raise IndexError("qubit index out of range")
+        _checked(self._st.apply_cnot, control, target)
+
+    def zero_state_expectation(self) -> float:
+        return self._st.zero_state_expectation()
+
+    # -- operators ---------------------------------------------------------
+    def __mul__(self, other):
+        out = self._copy()
+        out.multiply(other)
+        return out
+
+    def __imul__(self, other):
+        self.multiply(other)
+        return self
+
+    def __iadd__(self, other):
+        """append, then sort_and_combine (PauliSumCore.h:210-237)."""
+        self._check_same(other)
+        _checked(_abi.check, self._st._lib.pl_state_append(self._st._h, other._st._h),
+                 "pl_state_append")
+        self._st.sort_and_combine()
+        return self
+
+    def __add__(self, other):
+        out = self._copy()
+        out += other
+        return out
+
+
+def PauliSum(terms: Union[str, Sequence[str], Sequence[Tuple[str, float]]],
+             coefficient: float = 1.0):
+    """A device-resident Pauli sum from strings, as the reference's factory."""
+    if isinstance(terms, str):
+        terms = [(terms, coefficient)]
+    terms = list(terms)
+    if not terms:
+        raise ValueError("Cannot infer qubit count from an empty list. "
+                         "Use a non-empty list or pass a single string.")
+    nq = max(_count_qubits(t if isinstance(t, str) else t[0]) for t in terms)
+    aw = _capacity_words(nq)
+    try:
+        x, z, f, v, _ = strings.planes_from_terms(terms, aw)
+    except ValueError:
+        raise
+    return _PauliSum(nq, x, z, f, v)
+
+
+def commutator(a: _PauliSum, b: _PauliSum) -> _PauliSum:
+    """[A, B], canonicalized."""
+    return _comm(a, b, 0)
+
+
+def i_commutator(a: _PauliSum, b: _PauliSum) -> _PauliSum:
+    """i[A, B], canonicalized (Hermitian for Hermitian inputs)."""
+    return _comm(a, b, 1)
+
+
+def _comm(a, b, mul_i):
+    a._check_same(b)
+    out = _PauliSum(a._nq)
+    _abi.check(out._st._lib.pl_state_commutator(out._st._h, a._st._h, b._st._h, mul_i),
+               "pl_state_commutator")
+    out.canonicalize()
+    return out
+
+
+def propagate_expectation(observable: _PauliSum, rotations: _PauliSum,
+                          options: TruncationOptions | None = None) -> float:
+    """Pauli propagation: <0|U^dagger O U|0> for the rotation circuit U
+    (generator = term, angle = coefficient; PauliPropagation.h:65-71)."""
+    observable._check_same(rotations)
+    o = options or TruncationOptions()
+    out = observable._copy()
+    x, z, f, v = rotations._st.download()
+    out._st.propagate(x, z, f, v, None, o.max_weight, o.coefficient_cutoff, o.max_terms)
+    return out.zero_state_expectation()
+
+
+__all__ = ["PauliSum", "TruncationOptions", "commutator", "i_commutator",
+           "propagate_expectation", "MAX_QUBITS"]
