@@ -205,6 +205,33 @@ def run_product_collate(args, rank, local, ws):
         n_out = step()
     torch.cuda.synchronize()
 
+    # ---- autotune: keys per thread of the digit pass -------------------
+    tune_trials = []
+    for items in (8, 12, 16):
+        _abi.check(L.pl_set_tuning(_abi.PL_TUNE_RADIX_ITEMS, items), "pl_set_tuning")
+        step()
+        torch.cuda.synchronize()
+        t0 = torch.cuda.Event(enable_timing=True)
+        t1 = torch.cuda.Event(enable_timing=True)
+        t0.record(stream)
+        for _ in range(3):
+            step()
+        t1.record(stream)
+        torch.cuda.synchronize()
+        tune_trials.append({"radix_items": items, "ms_per_step": t0.elapsed_time(t1) / 3})
+    best = min(tune_trials, key=lambda t: t["ms_per_step"])
+    tune_ms = [t["ms_per_step"] for t in tune_trials]
+    best_items = best["radix_items"]
+    if ws > 1:  # every rank uses rank 0's choice
+        import torch.distributed as dist
+        t = torch.tensor([best_items], device="cuda")
+        dist.broadcast(t, 0)
+        best_items = int(t.item())
+    _abi.check(L.pl_set_tuning(_abi.PL_TUNE_RADIX_ITEMS, best_items), "pl_set_tuning")
+    for _ in range(args.warmup):
+        n_out = step()
+    torch.cuda.synchronize()
+
     # ---- device-resident timing ---------------------------------------
     _abi.profile_reset(timing=True)
     evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
@@ -295,7 +322,9 @@ def run_product_collate(args, rank, local, ws):
                    "terms_lhs": n, "terms_rhs": m, "products_per_step": total,
                    "terms_out": n_out, "array_size": 1, "parallelism": f"replicas x{ws}",
                    "l2": "flushed between steps (256 MB write outside the step events); "
-                         "step working set 0.6 GB > 126 MB L2"},
+                         "step working set 0.6 GB > 126 MB L2",
+                   "tuned": {"radix_items": best_items,
+                             "trials_ms_per_step": dict(zip(("8", "12", "16"), tune_ms))}},
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d,
                 "d2h_bytes_per_step": int(statistics.mean(d2h)),
                 "path": "pinned host planes -> H2D -> pl_multiply_collate (C ABI) -> D2H of "

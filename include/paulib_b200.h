@@ -331,6 +331,14 @@ PL_API int pl_batch_propagate(const pl_job* jobs, int64_t count, const pl_batch_
 PL_API int pl_serve(const pl_job* jobs, int64_t count, const pl_batch_opts* opts,
                     pl_job_result* results, pl_batch_stats* stats);
 
+/* ---- tuning ------------------------------------------------------------- */
+
+/* Keys per thread of the collate engine's onesweep digit pass: 8 (default),
+ * 12 or 16 (tiles of 2048, 3072 or 4096 keys).  Process-wide. */
+#define PL_TUNE_RADIX_ITEMS 1
+PL_API int pl_set_tuning(int key, int64_t value);
+PL_API int pl_get_tuning(int key, int64_t* value);
+
 /* ---- measurement hooks ------------------------------------------------ */
 
 /* Reset the library's counters.  With enable_timing != 0, every kernel of

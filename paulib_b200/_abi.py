@@ -44,7 +44,9 @@ EXPORTS = (
     "pl_state_multiply_canonicalize", "pl_state_commutator", "pl_profile_report",
     "pl_commutator_noalloc", "pl_state_set_option", "pl_state_memory", "pl_batch_propagate",
     "pl_serve", "pl_state_trim", "pl_state_trim_protected", "pl_state_append",
+    "pl_set_tuning", "pl_get_tuning",
 )
+PL_TUNE_RADIX_ITEMS = 1
 PL_OPT_GRAPHS = 1
 PL_ORDER_GIVEN = 0
 PL_ORDER_LONGEST_FIRST = 1
@@ -145,6 +147,8 @@ def lib():
         "pl_state_set_option": (I32, [VP, I32, I64]),
         "pl_state_trim": (I32, [VP, C.c_uint64]),
         "pl_state_append": (I32, [VP, VP]),
+        "pl_set_tuning": (I32, [I32, I64]),
+        "pl_get_tuning": (I32, [I32, C.POINTER(I64)]),
         "pl_state_trim_protected": (I32, [VP, C.c_uint64, VP]),
         "pl_state_memory": (I32, [VP, C.POINTER(C.c_uint64)]),
         "pl_batch_propagate": (I32, [C.POINTER(Job), I64, C.POINTER(BatchOpts),

@@ -40,8 +40,7 @@ namespace pl {
 namespace {
 
 constexpr int kThreads = 256;
-constexpr int kRItems = 8;
-constexpr int kRTile = kThreads * kRItems;  // 2048 keys per radix tile
+constexpr int kRTileMin = kThreads * 8;  // smallest radix tile (8 keys per thread)
 constexpr int kRadix = 256;
 constexpr int kWarps = kThreads / 32;
 constexpr u32 kIdxMask = 0x7fffffffu;
@@ -462,30 +461,30 @@ struct RadixSmem {
 
 // LAST: the final pass also fetches each term's coefficient from the source
 // and writes it in sorted order, so the segment sums read contiguous values.
-template <class Src, bool LAST>
-__global__ void __launch_bounds__(kThreads, 4)
+template <class Src, bool LAST, int ITEMS>
+__global__ void __launch_bounds__(kThreads, ITEMS <= 8 ? 4 : (ITEMS <= 12 ? 3 : 2))
     k_radix_pass(const u64* __restrict__ kin, const u32* __restrict__ vin, u64* __restrict__ kout,
                  u32* __restrict__ vout, u32 n, int shift, int bits,
                  const u32* __restrict__ bstart, u32* lb, u32* tile_ctr, int* status, Src src,
                  double* __restrict__ val_out) {
     extern __shared__ __align__(16) unsigned char dsm[];
     u64* skeys = reinterpret_cast<u64*>(dsm);
-    u32* svals = reinterpret_cast<u32*>(dsm + sizeof(u64) * kRTile);
+    u32* svals = reinterpret_cast<u32*>(dsm + sizeof(u64) * (kThreads * ITEMS));
     __shared__ RadixSmem S;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     if (tid == 0) S.tile = atomicAdd(tile_ctr, 1u);
     for (int i = tid; i < kWarps * kRadix; i += kThreads) S.whist[i] = 0;
     __syncthreads();
     const u32 tile = S.tile;
-    const u32 base = tile * (u32)kRTile;
+    const u32 base = tile * (u32)(kThreads * ITEMS);
     const u32 dmask = (1u << bits) - 1u;
 
-    u64 keys[kRItems];
-    u32 vals[kRItems];
-    u32 rank[kRItems];
-    const u32 wbase = base + (u32)warp * (kRItems * 32);
+    u64 keys[ITEMS];
+    u32 vals[ITEMS];
+    u32 rank[ITEMS];
+    const u32 wbase = base + (u32)warp * (ITEMS * 32);
 #pragma unroll
-    for (int t = 0; t < kRItems; ++t) {
+    for (int t = 0; t < ITEMS; ++t) {
         const u32 idx = wbase + t * 32 + lane;
         if (idx < n) {
             keys[t] = kin[idx];
@@ -497,7 +496,7 @@ __global__ void __launch_bounds__(kThreads, 4)
     }
     u32* wh = S.whist + warp * kRadix;
 #pragma unroll
-    for (int t = 0; t < kRItems; ++t) {
+    for (int t = 0; t < ITEMS; ++t) {
         const bool valid = (wbase + t * 32 + lane) < n;
         const u32 d = valid ? ((u32)(keys[t] >> shift) & dmask) : kSentinel;
         const u32 peers = __match_any_sync(0xffffffffu, d);
@@ -528,7 +527,7 @@ __global__ void __launch_bounds__(kThreads, 4)
     S.gofs[d] = bstart[d] + excl;
     __syncthreads();
 #pragma unroll
-    for (int t = 0; t < kRItems; ++t) {
+    for (int t = 0; t < ITEMS; ++t) {
         if (wbase + t * 32 + lane < n) {
             const u32 dd = (u32)(keys[t] >> shift) & dmask;
             const u32 pos = S.bloc[dd] + S.whist[warp * kRadix + dd] + rank[t];
@@ -537,7 +536,7 @@ __global__ void __launch_bounds__(kThreads, 4)
         }
     }
     __syncthreads();
-    const u32 tile_n = min((u32)kRTile, n - base);
+    const u32 tile_n = min((u32)(kThreads * ITEMS), n - base);
     for (u32 p = tid; p < tile_n; p += kThreads) {
         const u64 k = skeys[p];
         const u32 dd = (u32)(k >> shift) & dmask;
@@ -553,7 +552,7 @@ __global__ void __launch_bounds__(kThreads, 4)
     }
 }
 
-constexpr size_t kRadixDynSmem = sizeof(u64) * kRTile + sizeof(u32) * kRTile;
+constexpr size_t radix_smem(int items) { return (sizeof(u64) + sizeof(u32)) * kThreads * items; }
 
 // ---------------------------------------------------------------------------
 // 4. Segments: equal-key runs of the sorted order.
@@ -1211,7 +1210,7 @@ struct Bufs {
 };
 
 void carve_all(Carve& c, i64 n, int nch, Bufs& B) {
-    const i64 rtiles = (n + kRTile - 1) / kRTile + 1;
+    const i64 rtiles = (n + kRTileMin - 1) / kRTileMin + 1;
     const i64 etiles = (n + kETile - 1) / kETile + 1;
     const i64 ngw = (n + kFoldSpan - 1) / kFoldSpan + 16;  // fold warps; also bounds long runs
     const i64 npieces = n / kPiece + ngw;
@@ -1350,11 +1349,41 @@ u32 derive_histograms(const ProdSrc<AS>& src, const KeyLayout& L, const PassPlan
     return mask;
 }
 
+// Keys per thread of a digit pass (8, 12 or 16; PL_TUNE_RADIX_ITEMS).
+int radix_items() {
+    const long long v = tuning(PL_TUNE_RADIX_ITEMS);
+    return v == 12 || v == 16 ? (int)v : 8;
+}
+
+template <class Src, int ITEMS>
+int radix_pass(bool last, const u64* kin, const u32* vin, u64* kout, u32* vout, u32 n, int shift,
+               int bits, const u32* bstart, Bufs& B, u32* ctr, const Src& src, cudaStream_t st) {
+    const u32 tiles = (n + kThreads * ITEMS - 1) / (kThreads * ITEMS);
+    const SoASrc<1> nosrc{nullptr, nullptr, nullptr, nullptr, 0};
+    if (last) {
+        PL_CUDA_TRY(cudaFuncSetAttribute(k_radix_pass<Src, true, ITEMS>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)radix_smem(ITEMS)));
+        k_radix_pass<Src, true, ITEMS><<<tiles, kThreads, radix_smem(ITEMS), st>>>(
+            kin, vin, kout, vout, n, shift, bits, bstart, B.lb, ctr, B.d_status, src, B.sv),
+            pl::note_launch();
+    } else {
+        PL_CUDA_TRY(cudaFuncSetAttribute(k_radix_pass<SoASrc<1>, false, ITEMS>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)radix_smem(ITEMS)));
+        k_radix_pass<SoASrc<1>, false, ITEMS><<<tiles, kThreads, radix_smem(ITEMS), st>>>(
+            kin, vin, kout, vout, n, shift, bits, bstart, B.lb, ctr, B.d_status, nosrc, nullptr),
+            pl::note_launch();
+    }
+    return PL_OK;
+}
+
 template <int AS, class Src>
 int run_collate(const Src& src, u32 n, int mode, const KeyLayout& L, const PassPlan& P,
                 const CollateArgs& a, const SoAOut& out, i64* out_count, Bufs& B,
                 cudaStream_t st) {
-    const u32 rtiles = (n + kRTile - 1) / kRTile;
+    const int items = radix_items();
+    const u32 rtiles = (n + kThreads * items - 1) / (kThreads * items);
     const int nsm = sm_count();
     PL_CUDA_TRY(cudaMemsetAsync(B.hist, 0, sizeof(u32) * kMaxPasses * kRadix, st));
     PL_CUDA_TRY(cudaMemsetAsync(B.counters, 0, sizeof(u32) * (kMaxPasses + 8), st));
@@ -1386,14 +1415,19 @@ int run_collate(const Src& src, u32 n, int mode, const KeyLayout& L, const PassP
             PL_CUDA_TRY(cudaMemsetAsync(B.lb, 0, sizeof(u32) * (size_t)rtiles * kRadix, st));
             cudaEvent_t ev0 = timed_begin(st);
             const bool last = (p == P.npasses - 1);
-            if (last)
-                k_radix_pass<Src, true><<<rtiles, kThreads, kRadixDynSmem, st>>>(
-                    kin, vin, kout, vout, n, P.shift[p], P.bits[p], B.hist + (size_t)p * kRadix,
-                    B.lb, B.counters + 8 + p, B.d_status, src, B.sv), pl::note_launch();
+            const u32* bs = B.hist + (size_t)p * kRadix;
+            u32* ctr = B.counters + 8 + p;
+            int rc = PL_OK;
+            if (items == 16)
+                rc = radix_pass<Src, 16>(last, kin, vin, kout, vout, n, P.shift[p], P.bits[p], bs,
+                                         B, ctr, src, st);
+            else if (items == 12)
+                rc = radix_pass<Src, 12>(last, kin, vin, kout, vout, n, P.shift[p], P.bits[p], bs,
+                                         B, ctr, src, st);
             else
-                k_radix_pass<SoASrc<1>, false><<<rtiles, kThreads, kRadixDynSmem, st>>>(
-                    kin, vin, kout, vout, n, P.shift[p], P.bits[p], B.hist + (size_t)p * kRadix,
-                    B.lb, B.counters + 8 + p, B.d_status, nosrc, nullptr), pl::note_launch();
+                rc = radix_pass<Src, 8>(last, kin, vin, kout, vout, n, P.shift[p], P.bits[p], bs,
+                                        B, ctr, src, st);
+            if (rc) return rc;
             // algorithmic bytes: read and write one u64 key + one u32 payload per
             // term (+ the u64 coefficient written by the last pass)
             timed_end(ev0, st, "k_radix_pass", 24ull * n + (last ? 8ull * n : 0ull));

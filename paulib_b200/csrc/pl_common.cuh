@@ -120,6 +120,8 @@ namespace pl {
 int record_cuda(cudaError_t e);
 int record_status(int code, const char* what);
 // Measurement hooks (pl_profile_*): launch counter and event-timed passes.
+// Process-wide tuning values set through pl_set_tuning (0 = default).
+long long tuning(int key);
 void note_launch();
 // Stream-ordered device allocation from the device's default memory pool
 // (freed blocks stay cached in the pool, so regrowing costs no device-wide

@@ -80,6 +80,9 @@ void dev_free(void* p, cudaStream_t st) {
 void capture_lock() { g_alloc_mu.lock(); }
 void capture_unlock() { g_alloc_mu.unlock(); }
 
+static std::atomic<long long> g_tuning[8] = {};
+long long tuning(int key) { return key >= 0 && key < 8 ? g_tuning[key].load() : 0; }
+
 void note_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
 void note_launches(unsigned long long n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
 bool timing_enabled() { return g_timing.load(std::memory_order_relaxed); }
@@ -214,4 +217,18 @@ extern "C" int pl_profile_report(char* buf, size_t cap) {
     if (!buf || cap == 0) return pl::record_status(PL_ERR_INVALID_ARG, "pl_profile_report");
     snprintf(buf, cap, "%s", out.c_str());
     return pl::record_status(out.size() < cap ? PL_OK : PL_ERR_CAPACITY, nullptr);
+}
+
+extern "C" int pl_set_tuning(int key, int64_t value) {
+    if (key == PL_TUNE_RADIX_ITEMS && (value == 0 || value == 8 || value == 12 || value == 16)) {
+        pl::g_tuning[key].store(value);
+        return pl::record_status(PL_OK, nullptr);
+    }
+    return pl::record_status(PL_ERR_INVALID_ARG, "pl_set_tuning");
+}
+
+extern "C" int pl_get_tuning(int key, int64_t* value) {
+    if (!value || key < 1 || key >= 8) return pl::record_status(PL_ERR_INVALID_ARG, "pl_get_tuning");
+    *value = pl::g_tuning[key].load();
+    return pl::record_status(PL_OK, nullptr);
 }
