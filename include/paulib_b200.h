@@ -194,9 +194,35 @@ typedef struct {
     uint64_t max_terms;           /* UINT64_MAX = disabled */
 } pl_truncation;
 
+/* Bulk Clifford gates (PauliSumClifford.h:44-501).  One-qubit gates act on
+ * qubit a; two-qubit gates on control / first qubit a and target / second
+ * qubit b (a != b). */
+#define PL_GATE_H 1
+#define PL_GATE_S 2
+#define PL_GATE_H_YZ 3
+#define PL_GATE_H_XY 4
+#define PL_GATE_SQRT_X 5
+#define PL_GATE_SQRT_Y 6
+#define PL_GATE_X 7
+#define PL_GATE_Y 8
+#define PL_GATE_Z 9
+#define PL_GATE_I 10
+#define PL_GATE_CNOT 11
+#define PL_GATE_CZ 12
+#define PL_GATE_CY 13
+#define PL_GATE_XC_X 14
+#define PL_GATE_XC_Y 15
+#define PL_GATE_XC_Z 16
+#define PL_GATE_YC_X 17
+#define PL_GATE_YC_Y 18
+#define PL_GATE_YC_Z 19
+#define PL_GATE_SWAP 20
+#define PL_GATE_ISWAP 21
+
 /* Circuit ops, rows of int32 (kind, a, b) in application order. */
 #define PL_OP_ROTATION 0   /* rotation number a of the rotation table */
 #define PL_OP_CNOT 1       /* CNOT control a, target b */
+#define PL_OP_CLIFFORD 100 /* kind PL_OP_CLIFFORD + g: Clifford gate PL_GATE_g on a (, b) */
 
 typedef struct pl_state pl_state;
 
@@ -225,6 +251,13 @@ PL_API int pl_state_sort_and_combine(pl_state* state);
 PL_API int pl_state_cutoff(pl_state* state, double eps);
 PL_API int pl_state_truncate_weight(pl_state* state, uint64_t max_weight);
 PL_API int pl_state_apply_cnot(pl_state* state, int control, int target);
+/* apply_H, apply_S, ..., apply_iSWAP (PauliSumClifford.h:44-501): gate
+ * PL_GATE_* on qubit q1 (and q2 for two-qubit gates), every term in place. */
+PL_API int pl_state_apply_clifford(pl_state* state, int gate, int q1, int q2);
+/* apply_RX / apply_RY / apply_RZ (PauliSumOperations.h:29-104): the gate
+ * exp(-i angle/2 P) on `qubit`, P = X (axis 1), Y (2) or Z (3), followed by
+ * the reference's `+=` merge (sort_and_combine). */
+PL_API int pl_state_apply_rotation_gate(pl_state* state, int axis, int qubit, double angle);
 /* trim(max_terms) (PauliSumUtils.h:331-345): keep the max_terms terms of
  * largest |c| in their order; among equal |c| at the boundary the lower
  * index survives (the reference leaves that choice to std::nth_element). */

@@ -257,6 +257,32 @@ public:
     void apply_CNOT(std::size_t control, std::size_t target) {
         check(pl_state_apply_cnot(s_, (int)control, (int)target), "apply_CNOT");
     }
+    // Bulk Clifford gates (PauliSumClifford.h:44-501).
+    void apply_H(std::size_t q) { gate1(PL_GATE_H, q); }
+    void apply_S(std::size_t q) { gate1(PL_GATE_S, q); }
+    void apply_H_YZ(std::size_t q) { gate1(PL_GATE_H_YZ, q); }
+    void apply_H_XY(std::size_t q) { gate1(PL_GATE_H_XY, q); }
+    void apply_sqrt_X(std::size_t q) { gate1(PL_GATE_SQRT_X, q); }
+    void apply_sqrt_Y(std::size_t q) { gate1(PL_GATE_SQRT_Y, q); }
+    void apply_X(std::size_t q) { gate1(PL_GATE_X, q); }
+    void apply_Y(std::size_t q) { gate1(PL_GATE_Y, q); }
+    void apply_Z(std::size_t q) { gate1(PL_GATE_Z, q); }
+    void apply_I(std::size_t q) { gate1(PL_GATE_I, q); }
+    void apply_CZ(std::size_t c, std::size_t t) { gate2(PL_GATE_CZ, c, t); }
+    void apply_CY(std::size_t c, std::size_t t) { gate2(PL_GATE_CY, c, t); }
+    void apply_XC_X(std::size_t c, std::size_t t) { gate2(PL_GATE_XC_X, c, t); }
+    void apply_XC_Y(std::size_t c, std::size_t t) { gate2(PL_GATE_XC_Y, c, t); }
+    void apply_XC_Z(std::size_t c, std::size_t t) { gate2(PL_GATE_XC_Z, c, t); }
+    void apply_YC_X(std::size_t c, std::size_t t) { gate2(PL_GATE_YC_X, c, t); }
+    void apply_YC_Y(std::size_t c, std::size_t t) { gate2(PL_GATE_YC_Y, c, t); }
+    void apply_YC_Z(std::size_t c, std::size_t t) { gate2(PL_GATE_YC_Z, c, t); }
+    void apply_SWAP(std::size_t a, std::size_t b) { gate2(PL_GATE_SWAP, a, b); }
+    void apply_iSWAP(std::size_t a, std::size_t b) { gate2(PL_GATE_ISWAP, a, b); }
+    // apply_RX / RY / RZ (PauliSumOperations.h:29-104): exp(-i angle/2 P).
+    void apply_RX(std::size_t q, T angle) { rgate(1, q, angle); }
+    void apply_RY(std::size_t q, T angle) { rgate(2, q, angle); }
+    void apply_RZ(std::size_t q, T angle) { rgate(3, q, angle); }
+
     // PauliSumUtils.h:163-177.
     T zero_state_expectation() const {
         double r = 0.0;
@@ -284,6 +310,15 @@ public:
     }
 
 private:
+    void gate1(int g, std::size_t q) {
+        check(pl_state_apply_clifford(s_, g, (int)q, (int)q), "apply gate");
+    }
+    void gate2(int g, std::size_t a, std::size_t b) {
+        check(pl_state_apply_clifford(s_, g, (int)a, (int)b), "apply gate");
+    }
+    void rgate(int axis, std::size_t q, T angle) {
+        check(pl_state_apply_rotation_gate(s_, axis, (int)q, (double)angle), "apply rotation");
+    }
     static std::vector<std::pair<std::string, T>> with_unit(const std::vector<std::string>& v) {
         std::vector<std::pair<std::string, T>> out;
         for (const auto& s : v) out.emplace_back(s, T(1));

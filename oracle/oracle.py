@@ -121,6 +121,16 @@ class _Impl:
         fn(h, *args)
         return self._take(h, p.array_size)
 
+    def apply_clifford(self, p, gate: int, c: int, t: int = 0):
+        """Bulk Clifford gate number `gate` (the library's PL_GATE_* values)."""
+        return self._inplace(p, getattr(self.lib, self.prefix + "apply_clifford"), int(gate),
+                             int(c), int(t))
+
+    def apply_rgate(self, p, axis: int, c: int, angle: float):
+        """apply_RX / RY / RZ (axis 1 / 2 / 3)."""
+        return self._inplace(p, getattr(self.lib, self.prefix + "apply_rgate"), int(axis),
+                             int(c), float(angle))
+
 
 class Oracle(_Impl):
     """The C restatement (oracle/paulib_oracle.c)."""
@@ -139,6 +149,8 @@ class Oracle(_Impl):
         L.or_truncate_weight.argtypes = [C.c_void_p, C.c_uint64]
         L.or_trim.argtypes = [C.c_void_p, C.c_uint64]
         L.or_trim_protected.argtypes = [C.c_void_p, C.c_uint64, C.c_void_p]
+        L.or_apply_clifford.argtypes = [C.c_void_p, C.c_int, C.c_uint64, C.c_uint64]
+        L.or_apply_rgate.argtypes = [C.c_void_p, C.c_int, C.c_uint64, C.c_double]
         L.or_apply_cnot.argtypes = [C.c_void_p, C.c_uint64, C.c_uint64]
         L.or_zero_state_expectation.restype = C.c_double
         L.or_zero_state_expectation.argtypes = [C.c_void_p]
@@ -242,6 +254,8 @@ class Reference(_Impl):
         L.ref_truncate_weight.argtypes = [C.c_void_p, C.c_uint64]
         L.ref_trim.argtypes = [C.c_void_p, C.c_uint64]
         L.ref_trim_protected.argtypes = [C.c_void_p, C.c_uint64, C.c_void_p]
+        L.ref_apply_clifford.argtypes = [C.c_void_p, C.c_int, C.c_uint64, C.c_uint64]
+        L.ref_apply_rgate.argtypes = [C.c_void_p, C.c_int, C.c_uint64, C.c_double]
         L.ref_apply_cnot.argtypes = [C.c_void_p, C.c_uint64, C.c_uint64]
         L.ref_zero_state_expectation.restype = C.c_double
         L.ref_zero_state_expectation.argtypes = [C.c_void_p]

@@ -336,6 +336,131 @@ OR_EXPORT void or_apply_cnot(or_sum *s, u64 c, u64 t) {
     }
 }
 
+/* Bulk Clifford gates (PauliSumClifford.h:44-501): a per-term update of the
+ * Pauli bits of qubit c (and t) and of the sign bit, from the bits before
+ * the update.  Gate numbers are the library's PL_GATE_* values. */
+enum {
+    OG_H = 1, OG_S, OG_H_YZ, OG_H_XY, OG_SQRT_X, OG_SQRT_Y, OG_X, OG_Y, OG_Z, OG_I,
+    OG_CNOT, OG_CZ, OG_CY, OG_XC_X, OG_XC_Y, OG_XC_Z, OG_YC_X, OG_YC_Y, OG_YC_Z, OG_SWAP,
+    OG_ISWAP
+};
+
+/* Returns the sign flip; updates the bits in place (b[0..3] = xc, zc, xt, zt). */
+static unsigned gate_bits(int g, unsigned *b) {
+    const unsigned xc = b[0], zc = b[1], xt = b[2], zt = b[3];
+    unsigned sg = 0;
+    switch (g) {
+    case OG_H:      sg = xc & zc;        b[0] = zc; b[1] = xc; break;          /* :44-62 */
+    case OG_S:      sg = xc & zc;        b[1] = zc ^ xc; break;                /* :65-81 */
+    case OG_H_YZ:   sg = xc & !zc;       b[0] = xc ^ zc; break;                /* :84-100 */
+    case OG_H_XY:   sg = !xc & zc;       b[1] = zc ^ xc; break;                /* :103-119 */
+    case OG_SQRT_X: sg = !xc & zc;       b[0] = xc ^ zc; break;                /* :122-138 */
+    case OG_SQRT_Y: sg = xc & !zc;       b[0] = zc; b[1] = xc; break;          /* :141-159 */
+    case OG_X:      sg = zc; break;                                            /* :162-174 */
+    case OG_Y:      sg = xc ^ zc; break;                                       /* :177-190 */
+    case OG_Z:      sg = xc; break;                                            /* :193-205 */
+    case OG_I:      break;                                                     /* :208-210 */
+    case OG_CNOT:   /* :213-239 */
+        sg = xc & zt & (1 ^ xt ^ zc); b[2] = xt ^ xc; b[1] = zc ^ zt; break;
+    case OG_CZ:     /* :242-267 */
+        sg = xc & xt & (zc ^ zt);     b[3] = zt ^ xc; b[1] = zc ^ xt; break;
+    case OG_CY: /* :269-295 */
+        sg = (xc & zc & zt & !xt) | (xc & xt & !zc & !zt);
+        b[1] = zc ^ xt ^ zt; b[2] = xt ^ xc; b[3] = zt ^ xc; break;
+    case OG_XC_X: /* :297-322 */
+        sg = (xc & zc & zt & !xt) | (xt & zc & zt & !xc);
+        b[0] = xc ^ zt; b[2] = xt ^ zc; break;
+    case OG_XC_Z: /* :324-349 */
+        sg = (xc & xt & zc & zt) | (xt & zc & !xc & !zt);
+        b[0] = xc ^ xt; b[3] = zt ^ zc; break;
+    case OG_XC_Y: /* :351-377 */
+        sg = (xc & xt & zc & !zt) | (zc & zt & !xc & !xt);
+        b[0] = xc ^ xt ^ zt; b[2] = xt ^ zc; b[3] = zt ^ zc; break;
+    case OG_YC_X: /* :379-405 */
+        sg = (xc & xt & zt & !zc) | (zc & zt & !xc & !xt);
+        b[0] = xc ^ zt; b[1] = zc ^ zt; b[2] = xt ^ xc ^ zc; break;
+    case OG_YC_Z: /* :407-433 */
+        sg = (xt & zc & zt & !xc) | (xc & xt & !zc & !zt);
+        b[0] = xc ^ xt; b[1] = zc ^ xt; b[3] = zt ^ xc ^ zc; break;
+    case OG_YC_Y: /* :435-463 */
+        sg = (xc & zt & !xt & !zc) | (xt & zc & !xc & !zt);
+        b[0] = xc ^ xt ^ zt; b[1] = zc ^ xt ^ zt; b[2] = xt ^ xc ^ zc; b[3] = zt ^ xc ^ zc;
+        break;
+    case OG_SWAP:   b[0] = xt; b[1] = zt; b[2] = xc; b[3] = zc; break;        /* :465-490 */
+    case OG_ISWAP: {                                      /* :493-499: SWAP, CZ, S(c), S(t) */
+        unsigned f = gate_bits(OG_SWAP, b);
+        f ^= gate_bits(OG_CZ, b);
+        f ^= gate_bits(OG_S, b);
+        unsigned u[4] = {b[2], b[3], 0, 0};
+        f ^= gate_bits(OG_S, u);
+        b[2] = u[0]; b[3] = u[1];
+        sg = f; break;
+    }
+    default: break;
+    }
+    return sg & 1u;
+}
+
+OR_EXPORT int or_apply_clifford(or_sum *s, int gate, u64 c, u64 t) {
+    if (gate < OG_H || gate > OG_ISWAP) return -1;
+    const int two = gate >= OG_CNOT;
+    if (two && c == t) return -1;
+    const int wc = (int)(c / 64), wt = (int)(t / 64);
+    const u64 mc = 1ull << (c % 64), mt = 1ull << (t % 64);
+    for (i64 i = 0; i < s->n; ++i) {
+        unsigned b[4] = {(SX(s, wc, i) & mc) != 0, (SZ(s, wc, i) & mc) != 0, 0, 0};
+        if (two) { b[2] = (SX(s, wt, i) & mt) != 0; b[3] = (SZ(s, wt, i) & mt) != 0; }
+        const unsigned sg = gate_bits(gate, b);
+        s->f[i] ^= (u8)(sg << 1);
+        SX(s, wc, i) = (SX(s, wc, i) & ~mc) | (b[0] ? mc : 0);
+        SZ(s, wc, i) = (SZ(s, wc, i) & ~mc) | (b[1] ? mc : 0);
+        if (two) {
+            SX(s, wt, i) = (SX(s, wt, i) & ~mt) | (b[2] ? mt : 0);
+            SZ(s, wt, i) = (SZ(s, wt, i) & ~mt) | (b[3] ? mt : 0);
+        }
+    }
+    return 0;
+}
+
+/* apply_RZ / apply_RX / apply_RY (PauliSumOperations.h:29-104), the gate
+ * exp(-i theta/2 P): every term that anticommutes with P_c keeps
+ * cos(theta/2) of its value and emits a copy left-multiplied by i P_c
+ * (multiply_iZ / iX / iY, PauliSumClifford.h:13-40) with sin(theta/2) of
+ * the original value; then `+=` (append + sort_and_combine).  axis: 1 X,
+ * 2 Y, 3 Z. */
+OR_EXPORT int or_apply_rgate(or_sum *s, int axis, u64 c, double angle) {
+    if (axis < 1 || axis > 3) return -1;
+    const double ch = cos(angle / 2), sh = sin(angle / 2);
+    const int w = (int)(c / 64);
+    const u64 mk = 1ull << (c % 64);
+    const i64 m = s->n;
+    i64 kc = 0;
+    for (i64 j = 0; j < m; ++j) {
+        const u64 xc = (SX(s, w, j) & mk) != 0, zc = (SZ(s, w, j) & mk) != 0;
+        kc += axis == 3 ? xc : axis == 1 ? zc : (xc ^ zc);
+    }
+    sum_reserve(s, m + kc);
+    i64 t = m;
+    for (i64 j = 0; j < m; ++j) {
+        const u64 xc = (SX(s, w, j) & mk) != 0, zc = (SZ(s, w, j) & mk) != 0;
+        const u64 anti = axis == 3 ? xc : axis == 1 ? zc : (xc ^ zc);
+        if (!anti) continue;
+        const double tv = s->v[j] * sh;
+        s->v[j] *= ch;
+        for (int k = 0; k < s->as; ++k) { SX(s, k, t) = SX(s, k, j); SZ(s, k, t) = SZ(s, k, j); }
+        u8 f = s->f[j];
+        if (axis == 3) { f ^= (u8)((!zc) << 1); SZ(s, w, t) ^= mk; }
+        else if (axis == 1) { f ^= (u8)(xc << 1); SX(s, w, t) ^= mk; }
+        else { f ^= (u8)((!xc) << 1); SX(s, w, t) ^= mk; SZ(s, w, t) ^= mk; }
+        s->f[t] = f;
+        s->v[t] = tv;
+        ++t;
+    }
+    s->n = t;
+    or_sort_and_combine(s);
+    return 0;
+}
+
 /* zero_state_expectation (PauliSumUtils.h:163-177): terms with no X bit and
  * a real phase contribute +-value, summed in term order. */
 OR_EXPORT double or_zero_state_expectation(const or_sum *s) {
@@ -507,6 +632,10 @@ OR_EXPORT void or_propagate(or_sum *s, const or_sum *rot, const int32_t *ops, i6
         i64 a = ops ? ops[3 * l + 1] : l;
         if (kind == 1) {
             or_apply_cnot(s, (u64)a, (u64)ops[3 * l + 2]);
+            continue;
+        }
+        if (kind >= 100) { /* Clifford gate kind - 100 on (a, b), no truncation */
+            or_apply_clifford(s, kind - 100, (u64)a, (u64)ops[3 * l + 2]);
             continue;
         }
         for (int k = 0; k < rot->as; ++k) { px[k] = SX(rot, k, a); pz[k] = SZ(rot, k, a); }

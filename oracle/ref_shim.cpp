@@ -47,6 +47,8 @@ struct SumBase {
                            u64 max_weight, double cutoff, u64 max_terms) = 0;
     virtual void trim(u64 max_terms) = 0;
     virtual void trim_protected(u64 max_terms, const SumBase* keep) = 0;
+    virtual int apply_clifford(int gate, u64 c, u64 t) = 0;
+    virtual int apply_rgate(int axis, u64 c, double angle) = 0;
 };
 
 template <std::size_t N>
@@ -101,6 +103,42 @@ struct Sum final : SumBase {
     void trim(u64 max_terms) override { s.trim((std::size_t)max_terms); }
     void trim_protected(u64 max_terms, const SumBase* keep) override {
         s.trim((std::size_t)max_terms, static_cast<const Sum*>(keep)->s);
+    }
+    // gate numbers: the library's PL_GATE_* values
+    int apply_clifford(int gate, u64 c, u64 t) override {
+        const std::size_t a = (std::size_t)c, b = (std::size_t)t;
+        switch (gate) {
+            case 1: s.apply_H(a); break;
+            case 2: s.apply_S(a); break;
+            case 3: s.apply_H_YZ(a); break;
+            case 4: s.apply_H_XY(a); break;
+            case 5: s.apply_sqrt_X(a); break;
+            case 6: s.apply_sqrt_Y(a); break;
+            case 7: s.apply_X(a); break;
+            case 8: s.apply_Y(a); break;
+            case 9: s.apply_Z(a); break;
+            case 10: s.apply_I(a); break;
+            case 11: s.apply_CNOT(a, b); break;
+            case 12: s.apply_CZ(a, b); break;
+            case 13: s.apply_CY(a, b); break;
+            case 14: s.apply_XC_X(a, b); break;
+            case 15: s.apply_XC_Y(a, b); break;
+            case 16: s.apply_XC_Z(a, b); break;
+            case 17: s.apply_YC_X(a, b); break;
+            case 18: s.apply_YC_Y(a, b); break;
+            case 19: s.apply_YC_Z(a, b); break;
+            case 20: s.apply_SWAP(a, b); break;
+            case 21: s.apply_iSWAP(a, b); break;
+            default: return -1;
+        }
+        return 0;
+    }
+    int apply_rgate(int axis, u64 c, double angle) override {
+        if (axis == 1) s.apply_RX((std::size_t)c, angle);
+        else if (axis == 2) s.apply_RY((std::size_t)c, angle);
+        else if (axis == 3) s.apply_RZ((std::size_t)c, angle);
+        else return -1;
+        return 0;
     }
     void propagate(const SumBase* rotb, const std::int32_t* ops, i64 n_ops, u64 max_weight,
                    double cutoff, u64 max_terms) override {
@@ -180,6 +218,12 @@ __attribute__((visibility("default"))) void ref_truncate_weight(void* h, u64 w) 
     ((SumBase*)h)->truncate_weight(w);
 }
 __attribute__((visibility("default"))) void ref_trim(void* h, u64 m) { ((SumBase*)h)->trim(m); }
+__attribute__((visibility("default"))) int ref_apply_clifford(void* h, int g, u64 c, u64 t) {
+    return ((SumBase*)h)->apply_clifford(g, c, t);
+}
+__attribute__((visibility("default"))) int ref_apply_rgate(void* h, int axis, u64 c, double a) {
+    return ((SumBase*)h)->apply_rgate(axis, c, a);
+}
 __attribute__((visibility("default"))) void ref_trim_protected(void* h, u64 m, const void* k) {
     ((SumBase*)h)->trim_protected(m, (const SumBase*)k);
 }

@@ -44,8 +44,12 @@ EXPORTS = (
     "pl_state_multiply_canonicalize", "pl_state_commutator", "pl_profile_report",
     "pl_commutator_noalloc", "pl_state_set_option", "pl_state_memory", "pl_batch_propagate",
     "pl_serve", "pl_state_trim", "pl_state_trim_protected", "pl_state_append",
-    "pl_set_tuning", "pl_get_tuning",
+    "pl_set_tuning", "pl_get_tuning", "pl_state_apply_clifford", "pl_state_apply_rotation_gate",
 )
+PL_OP_CLIFFORD = 100
+GATES = {"H": 1, "S": 2, "H_YZ": 3, "H_XY": 4, "SQRT_X": 5, "SQRT_Y": 6, "X": 7, "Y": 8,
+         "Z": 9, "I": 10, "CNOT": 11, "CZ": 12, "CY": 13, "XC_X": 14, "XC_Y": 15, "XC_Z": 16,
+         "YC_X": 17, "YC_Y": 18, "YC_Z": 19, "SWAP": 20, "ISWAP": 21}
 PL_TUNE_RADIX_ITEMS = 1
 PL_OPT_GRAPHS = 1
 PL_ORDER_GIVEN = 0
@@ -147,6 +151,8 @@ def lib():
         "pl_state_set_option": (I32, [VP, I32, I64]),
         "pl_state_trim": (I32, [VP, C.c_uint64]),
         "pl_state_append": (I32, [VP, VP]),
+        "pl_state_apply_clifford": (I32, [VP, I32, I32, I32]),
+        "pl_state_apply_rotation_gate": (I32, [VP, I32, I32, C.c_double]),
         "pl_set_tuning": (I32, [I32, I64]),
         "pl_get_tuning": (I32, [I32, C.POINTER(I64)]),
         "pl_state_trim_protected": (I32, [VP, C.c_uint64, VP]),

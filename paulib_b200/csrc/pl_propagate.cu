@@ -983,6 +983,141 @@ __global__ void __launch_bounds__(kPT)
     }
 }
 
+// ---------------------------------------------------------------------------
+// Bulk Clifford gates (PauliSumClifford.h:44-501) as a 16-entry table over
+// the Pauli bits (xc, zc, xt, zt) of the gate's qubits: entry e holds the
+// new bits (tbits, 4 per entry) and whether the sign flips (tsign bit e).
+// The tables are built on the host from each gate's images of X and Z.
+// ---------------------------------------------------------------------------
+template <int AS>
+__global__ void __launch_bounds__(256) k_clifford(Buf b, const i64* d_n, int wc, u64 mc, int wt,
+                                                  u64 mt, int two, u64 tbits, u32 tsign,
+                                                  const int* status) {
+    if (status_set(status)) return;
+    const i64 n = *d_n;
+    for (i64 i = (i64)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+         i += (i64)gridDim.x * blockDim.x) {
+        u64 xa = b.x[wc * b.cap + i], za = b.z[wc * b.cap + i];
+        u64 xb = xa, zb = za;
+        if (two && wt != wc) {
+            xb = b.x[wt * b.cap + i];
+            zb = b.z[wt * b.cap + i];
+        }
+        const u32 e = (u32)((xa & mc) != 0) | ((u32)((za & mc) != 0) << 1) |
+                      (two ? ((u32)((xb & mt) != 0) << 2) | ((u32)((zb & mt) != 0) << 3) : 0u);
+        const u32 o = (u32)(tbits >> (4 * e)) & 15u;
+        xa = (xa & ~mc) | ((o & 1u) ? mc : 0ull);
+        za = (za & ~mc) | ((o & 2u) ? mc : 0ull);
+        if (two) {
+            if (wt == wc) {
+                xa = (xa & ~mt) | ((o & 4u) ? mt : 0ull);
+                za = (za & ~mt) | ((o & 8u) ? mt : 0ull);
+            } else {
+                b.x[wt * b.cap + i] = (xb & ~mt) | ((o & 4u) ? mt : 0ull);
+                b.z[wt * b.cap + i] = (zb & ~mt) | ((o & 8u) ? mt : 0ull);
+            }
+        }
+        b.x[wc * b.cap + i] = xa;
+        b.z[wc * b.cap + i] = za;
+        b.f[i] ^= (u8)(((tsign >> e) & 1u) << 1);
+    }
+}
+
+// apply_RX / RY / RZ (PauliSumOperations.h:29-104) materialised:
+// out[0, m) = old terms, those anticommuting with P_c scaled by cos(theta/2);
+// out[m + r] = the r-th anticommuting term left-multiplied by i P_c
+// (multiply_iX / iY / iZ, PauliSumClifford.h:13-40) with sin(theta/2) of its
+// original value -- the array the reference's `+=` sorts.  axis 1 X, 2 Y, 3 Z.
+template <int AS>
+__global__ void __launch_bounds__(kPT)
+    k_materialize_rgate(Buf old, i64 m, int w, u64 mk, int axis, double ch, double sh, Buf out,
+                        i64* d_total, u64* lb, u32* ctr, int* status) {
+    __shared__ u32 s_tile;
+    __shared__ u64 s_warp[kPT / 32];
+    __shared__ u64 s_base;
+    const u32 ntiles = (u32)((m + kExpTile - 1) / kExpTile);
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    for (;;) {
+        if (tid == 0) s_tile = atomicAdd(ctr, 1u);
+        __syncthreads();
+        const u32 tile = s_tile;
+        __syncthreads();
+        if (tile >= ntiles) break;
+        const i64 wbase = (i64)tile * kExpTile + warp * (kExpItems * 32);
+        u32 amask = 0, cnt = 0;
+        u32 off[kExpItems];
+#pragma unroll
+        for (int t = 0; t < kExpItems; ++t) {
+            const i64 j = wbase + t * 32 + lane;
+            bool a = false;
+            if (j < m) {
+#pragma unroll
+                for (int k = 0; k < AS; ++k) {
+                    out.x[k * out.cap + j] = old.x[k * old.cap + j];
+                    out.z[k * out.cap + j] = old.z[k * old.cap + j];
+                }
+                const bool xc = (old.x[w * old.cap + j] & mk) != 0;
+                const bool zc = (old.z[w * old.cap + j] & mk) != 0;
+                a = axis == 3 ? xc : (axis == 1 ? zc : (xc != zc));
+                out.f[j] = old.f[j];
+                out.v[j] = a ? dmul(old.v[j], ch) : old.v[j];
+            }
+            const u32 bal = __ballot_sync(0xffffffffu, a);
+            off[t] = cnt + __popc(bal & lanemask_lt());
+            cnt += __popc(bal);
+            if (a) amask |= 1u << t;
+        }
+        if (lane == 0) s_warp[warp] = cnt;
+        __syncthreads();
+        u64 wpre = 0, tot = 0;
+#pragma unroll
+        for (int q = 0; q < kPT / 32; ++q) {
+            const u64 v = s_warp[q];
+            if (q < warp) wpre += v;
+            tot += v;
+        }
+        if (warp == 0) {
+            const u64 ex = warp_lookback2(lb, tile, tot, status);
+            if (lane == 0) s_base = ex;
+        }
+        __syncthreads();
+        const i64 base = (i64)(u32)(s_base + wpre);
+#pragma unroll
+        for (int t = 0; t < kExpItems; ++t) {
+            if (!((amask >> t) & 1u)) continue;
+            const i64 j = wbase + t * 32 + lane;
+            const i64 pos = m + base + off[t];
+            if (pos >= out.cap) {
+                raise_status(status, PL_ERR_CAPACITY);
+                continue;
+            }
+#pragma unroll
+            for (int k = 0; k < AS; ++k) {
+                out.x[k * out.cap + pos] = old.x[k * old.cap + j];
+                out.z[k * out.cap + pos] = old.z[k * old.cap + j];
+            }
+            const bool xc = (old.x[w * old.cap + j] & mk) != 0;
+            const bool zc = (old.z[w * old.cap + j] & mk) != 0;
+            u32 f = old.f[j];
+            if (axis == 3) {
+                f ^= (u32)(!zc) << 1;
+                out.z[w * out.cap + pos] ^= mk;
+            } else if (axis == 1) {
+                f ^= (u32)xc << 1;
+                out.x[w * out.cap + pos] ^= mk;
+            } else {
+                f ^= (u32)(!xc) << 1;
+                out.x[w * out.cap + pos] ^= mk;
+                out.z[w * out.cap + pos] ^= mk;
+            }
+            out.f[pos] = (u8)f;
+            out.v[pos] = dmul(old.v[j], sh);
+        }
+        if (tile == ntiles - 1 && tid == 0) *d_total = m + (i64)(u32)(s_base + tot);
+        __syncthreads();
+    }
+}
+
 // Order-preserving filters cutoff / truncate_weight (PauliSumUtils.h:378-393).
 template <int AS>
 __global__ void __launch_bounds__(kPT) k_filter(Buf in, i64 n, Buf out, double eps,
@@ -1496,6 +1631,115 @@ __global__ void __launch_bounds__(kPT) k_trim_emit(Buf b, const i64* d_n, Protec
             tr += __popc(be);
         }
         __syncthreads();
+    }
+}
+
+// ---- Clifford gate tables ------------------------------------------------
+// A Clifford gate maps each generator X_c, Z_c, X_t, Z_t to a signed Pauli
+// (its image); conjugation is multiplicative, so the image of any Pauli is
+// the product of its generators' images.  Paulis are kept in product form
+// i^k X_c^x0 Z_c^z0 X_t^x1 Z_t^z1; a term's bits (Y = (1,1)) read as
+// i^{#Y} X^x Z^z since Y = i X Z.
+struct P2 {
+    unsigned x[2], z[2], k;
+};
+
+P2 p2_mul(const P2& a, const P2& b) {
+    P2 r;
+    r.k = (a.k + b.k) & 3u;
+    for (int q = 0; q < 2; ++q) {
+        r.k = (r.k + 2u * (a.z[q] & b.x[q])) & 3u;  // Z X = -X Z
+        r.x[q] = a.x[q] ^ b.x[q];
+        r.z[q] = a.z[q] ^ b.z[q];
+    }
+    return r;
+}
+
+// Signed string "[-]PQ" (P on c, Q on t) in product form.
+P2 p2_of(const char* s) {
+    P2 r{{0, 0}, {0, 0}, 0};
+    unsigned sign = 0;
+    if (*s == '-') {
+        sign = 1;
+        ++s;
+    }
+    unsigned ny = 0;
+    for (int q = 0; q < 2 && s[q]; ++q) {
+        r.x[q] = s[q] == 'X' || s[q] == 'Y';
+        r.z[q] = s[q] == 'Z' || s[q] == 'Y';
+        ny += s[q] == 'Y';
+    }
+    r.k = (ny + 2u * sign) & 3u;
+    return r;
+}
+
+struct GateImages {
+    const char* img[4];  // images of X_c, Z_c, X_t, Z_t
+};
+
+// Generator images of PL_GATE_1 .. PL_GATE_SWAP, read off the reference's
+// gate definitions (PauliSumClifford.h:44-490) and its truth-table tests.
+const GateImages kGateImages[] = {
+    {{"XI", "ZI", "IX", "IZ"}},      // unused (0)
+    {{"ZI", "XI", "IX", "IZ"}},      // H
+    {{"YI", "ZI", "IX", "IZ"}},      // S
+    {{"-XI", "YI", "IX", "IZ"}},     // H_YZ
+    {{"YI", "-ZI", "IX", "IZ"}},     // H_XY
+    {{"XI", "-YI", "IX", "IZ"}},     // sqrt(X)
+    {{"-ZI", "XI", "IX", "IZ"}},     // sqrt(Y)
+    {{"XI", "-ZI", "IX", "IZ"}},     // X
+    {{"-XI", "-ZI", "IX", "IZ"}},    // Y
+    {{"-XI", "ZI", "IX", "IZ"}},     // Z
+    {{"XI", "ZI", "IX", "IZ"}},      // I
+    {{"XX", "ZI", "IX", "ZZ"}},      // CNOT
+    {{"XZ", "ZI", "ZX", "IZ"}},      // CZ
+    {{"XY", "ZI", "ZX", "ZZ"}},      // CY
+    {{"XI", "ZX", "IX", "XZ"}},      // XC_X
+    {{"XI", "ZY", "XX", "XZ"}},      // XC_Y
+    {{"XI", "ZZ", "XX", "IZ"}},      // XC_Z
+    {{"XX", "ZX", "IX", "YZ"}},      // YC_X
+    {{"XY", "ZY", "YX", "YZ"}},      // YC_Y
+    {{"XZ", "ZZ", "YX", "IZ"}},      // YC_Z
+    {{"IX", "IZ", "XI", "ZI"}},      // SWAP
+};
+
+// Image of the term bits e = xc | zc << 1 | xt << 2 | zt << 3 under gate g:
+// new bits and sign flip.
+void gate_apply(int g, unsigned e, unsigned* out_bits, unsigned* sign) {
+    const GateImages& G = kGateImages[g];
+    const unsigned b[4] = {e & 1u, (e >> 1) & 1u, (e >> 2) & 1u, (e >> 3) & 1u};
+    P2 r{{0, 0}, {0, 0}, (b[0] & b[1]) + (b[2] & b[3])};  // i^{#Y}
+    for (int k = 0; k < 4; ++k)
+        if (b[k]) r = p2_mul(r, p2_of(G.img[k]));
+    const unsigned ny = (r.x[0] & r.z[0]) + (r.x[1] & r.z[1]);
+    *out_bits = r.x[0] | (r.z[0] << 1) | (r.x[1] << 2) | (r.z[1] << 3);
+    *sign = ((r.k + 4u - ny) & 3u) >> 1;  // a Clifford image of a Hermitian Pauli: 0 or 2
+}
+
+// Packed table of gate g (iSWAP = SWAP, CZ, S on c, S on t;
+// PauliSumClifford.h:493-499).
+void gate_table(int g, u64* tbits, u32* tsign) {
+    *tbits = 0;
+    *tsign = 0;
+    for (unsigned e = 0; e < 16; ++e) {
+        unsigned bits = e, sg = 0;
+        if (g == PL_GATE_ISWAP) {
+            unsigned s1;
+            gate_apply(PL_GATE_SWAP, bits, &bits, &s1);
+            sg ^= s1;
+            gate_apply(PL_GATE_CZ, bits, &bits, &s1);
+            sg ^= s1;
+            gate_apply(PL_GATE_S, bits, &bits, &s1);
+            sg ^= s1;
+            unsigned hi = bits >> 2, nb;
+            gate_apply(PL_GATE_S, hi, &nb, &s1);
+            bits = (bits & 3u) | ((nb & 3u) << 2);
+            sg ^= s1;
+        } else {
+            gate_apply(g, bits, &bits, &sg);
+        }
+        *tbits |= (u64)bits << (4 * e);
+        *tsign |= (sg & 1u) << e;
     }
 }
 
@@ -2023,8 +2267,9 @@ int state_canonical_sort(pl_state* s) {
 }
 
 struct Op {
-    int kind;  // 0 rotation, 1 CNOT
+    int kind;  // 0 rotation, 1 CNOT, 2 Clifford gate `gate`
     int a, b;
+    int gate;
 };
 
 // Device copies of the op tables (gate records, CNOT pairs), grow-only with
@@ -2086,7 +2331,7 @@ int run_ops(pl_state* s, const std::vector<Rot>& rots, const std::vector<Op>& op
             if (ops[q].kind == 1) {
                 pairs[2 * q] = ops[q].a;
                 pairs[2 * q + 1] = ops[q].b;
-            } else {
+            } else if (ops[q].kind == 0) {
                 const int r = ops[q].a;
                 recs[q].g = gates[r];
                 recs[q].mode = modes[r];
@@ -2131,7 +2376,22 @@ int run_ops(pl_state* s, const std::vector<Rot>& rots, const std::vector<Op>& op
     while (i < ops.size()) {
         const Op& op = ops[i];
         bool rewound = false;
-        if (op.kind == 1) {
+        if (op.kind == 2) {
+            // a bulk Clifford gate: a bijection of the strings, in place
+            in_buf[i] = s->cur;
+            if (s->cls == 2) s->cls = 1;
+            const bool two = op.gate >= PL_GATE_CNOT;
+            const int q2 = two ? op.b : op.a;
+            u64 tb;
+            u32 ts;
+            gate_table(op.gate, &tb, &ts);
+            k_clifford<AS><<<grid_persistent(8), 256, 0, s->st>>>(
+                s->S[s->cur], s->d_size + s->cur, op.a / 64, 1ull << (op.a % 64), q2 / 64,
+                1ull << (q2 % 64), two ? 1 : 0, tb, ts, s->d_status), pl::note_launch();
+            pending = true;
+            ++since_sync;
+            ++i;
+        } else if (op.kind == 1) {
             // consecutive CNOTs (one brickwork layer) in one pass
             size_t j = i;
             while (j < ops.size() && ops[j].kind == 1) in_buf[j++] = s->cur;
@@ -2554,6 +2814,61 @@ extern "C" int pl_state_apply_cnot(pl_state* s, int control, int target) {
     return record_status(PL_OK, nullptr);
 }
 
+extern "C" int pl_state_apply_clifford(pl_state* s, int gate, int q1, int q2) {
+    int rc = check_state(s);
+    if (rc) return rc;
+    const bool two = gate >= PL_GATE_CNOT;
+    if (gate < PL_GATE_H || gate > PL_GATE_ISWAP || q1 < 0 || q1 >= 64 * s->as ||
+        (two && (q2 < 0 || q2 >= 64 * s->as || q2 == q1)))
+        return record_status(PL_ERR_INVALID_ARG, "pl_state_apply_clifford");
+    if (!two) q2 = q1;
+    u64 tb;
+    u32 ts;
+    gate_table(gate, &tb, &ts);
+    PL_DISPATCH_AS(s->as, k_clifford<AS><<<grid_persistent(8), 256, 0, s->st>>>(
+                              s->S[s->cur], s->d_size + s->cur, q1 / 64, 1ull << (q1 % 64),
+                              q2 / 64, 1ull << (q2 % 64), two ? 1 : 0, tb, ts, s->d_status),
+                          pl::note_launch());
+    PL_CUDA_TRY(cudaGetLastError());
+    if (s->cls == 2) s->cls = 1;
+    return record_status(PL_OK, nullptr);
+}
+
+extern "C" int pl_state_apply_rotation_gate(pl_state* s, int axis, int qubit, double angle) {
+    int rc = check_state(s);
+    if (rc) return rc;
+    if (axis < 1 || axis > 3 || qubit < 0 || qubit >= 64 * s->as || !std::isfinite(angle))
+        return record_status(PL_ERR_INVALID_ARG, "pl_state_apply_rotation_gate");
+    i64 n = 0;
+    rc = read_size(s, &n);
+    if (rc) return rc;
+    if (n == 0) return record_status(PL_OK, nullptr);
+    if (2 * n > s->cap) {
+        rc = state_grow(s, 2 * n);
+        if (rc) return rc;
+    }
+    const double ch = std::cos(angle / 2), sh = std::sin(angle / 2);
+    PL_CUDA_TRY(cudaMemsetAsync(s->lbA, 0, s->zero_bytes, s->st));
+    const int other = 1 - s->cur;
+    PL_DISPATCH_AS(s->as, k_materialize_rgate<AS><<<grid_persistent(4), kPT, 0, s->st>>>(
+                              s->S[s->cur], n, qubit / 64, 1ull << (qubit % 64), axis, ch, sh,
+                              s->S[other], s->d_tmp, s->lbA, s->ctr + 0, s->d_status),
+                          pl::note_launch());
+    i64 total = 0;
+    int st[2];
+    PL_CUDA_TRY(cudaMemcpyAsync(&total, s->d_tmp, sizeof(i64), cudaMemcpyDeviceToHost, s->st));
+    PL_CUDA_TRY(cudaMemcpyAsync(st, s->d_status, sizeof(st), cudaMemcpyDeviceToHost, s->st));
+    PL_CUDA_TRY(cudaStreamSynchronize(s->st));
+    if (st[0]) return record_status(st[0], "apply_rotation_gate: materialise");
+    s->cur = other;
+    CollateArgs a;
+    a.mode = kCombine;
+    rc = state_collate(s, total, a);
+    if (rc) return rc;
+    s->cls = 0;
+    return record_status(PL_OK, nullptr);
+}
+
 extern "C" int pl_state_zero_state_expectation(pl_state* s, double* result) {
     int rc = check_state(s);
     if (rc) return rc;
@@ -2592,13 +2907,21 @@ extern "C" int pl_propagate(pl_state* s, const uint64_t* rot_x, const uint64_t* 
             } else if (kind == PL_OP_CNOT) {
                 if (a < 0 || b < 0 || a >= 64 * s->as || b >= 64 * s->as || a == b)
                     return record_status(PL_ERR_INVALID_ARG, "pl_propagate: CNOT qubits");
+            } else if (kind > PL_OP_CLIFFORD && kind <= PL_OP_CLIFFORD + PL_GATE_ISWAP) {
+                const bool two = kind - PL_OP_CLIFFORD >= PL_GATE_CNOT;
+                if (a < 0 || a >= 64 * s->as ||
+                    (two && (b < 0 || b >= 64 * s->as || a == b)))
+                    return record_status(PL_ERR_INVALID_ARG, "pl_propagate: gate qubits");
             } else {
                 return record_status(PL_ERR_INVALID_ARG, "pl_propagate: op kind");
             }
-            list.push_back(Op{kind == PL_OP_CNOT ? 1 : 0, a, b});
+            if (kind >= PL_OP_CLIFFORD)
+                list.push_back(Op{2, a, b, kind - PL_OP_CLIFFORD});
+            else
+                list.push_back(Op{kind == PL_OP_CNOT ? 1 : 0, a, b, 0});
         }
     } else {
-        for (i64 l = n_rot; l-- > 0;) list.push_back(Op{0, (int)l, 0});
+        for (i64 l = n_rot; l-- > 0;) list.push_back(Op{0, (int)l, 0, 0});
     }
     PL_DISPATCH_AS(s->as, rc = run_ops<AS>(s, rots, list, *opts));
     if (rc) return rc;

@@ -146,6 +146,55 @@ class _PauliSum:
     def zero_state_expectation(self) -> float:
         return self._st.zero_state_expectation()
 
+    # -- Clifford and rotation gates (PauliSumClifford.h, PauliSumOperations.h:29-104)
+    def _q(self, *qs):
+        for q in qs:
+            if not 0 <= q < self._nq:
+                raise IndexError("qubit index out of range")
+
+    def _g1(self, name, qubit):
+        self._q(qubit)
+        _checked(self._st.apply_clifford, name, qubit, 0)
+
+    def _g2(self, name, a, b):
+        self._q(a, b)
+        if a == b:
+            raise ValueError("two-qubit gate needs two different qubits")
+        _checked(self._st.apply_clifford, name, a, b)
+
+    def apply_H(self, qubit): self._g1("H", qubit)
+    def apply_H_YZ(self, qubit): self._g1("H_YZ", qubit)
+    def apply_H_XY(self, qubit): self._g1("H_XY", qubit)
+    def apply_S(self, qubit): self._g1("S", qubit)
+    def apply_SX(self, qubit): self._g1("SQRT_X", qubit)
+    def apply_SY(self, qubit): self._g1("SQRT_Y", qubit)
+    def apply_X(self, qubit): self._g1("X", qubit)
+    def apply_Y(self, qubit): self._g1("Y", qubit)
+    def apply_Z(self, qubit): self._g1("Z", qubit)
+    def apply_I(self, qubit): self._g1("I", qubit)
+    def apply_CZ(self, control, target): self._g2("CZ", control, target)
+    def apply_CY(self, control, target): self._g2("CY", control, target)
+    def apply_XC_X(self, control, target): self._g2("XC_X", control, target)
+    def apply_XC_Y(self, control, target): self._g2("XC_Y", control, target)
+    def apply_XC_Z(self, control, target): self._g2("XC_Z", control, target)
+    def apply_YC_X(self, control, target): self._g2("YC_X", control, target)
+    def apply_YC_Y(self, control, target): self._g2("YC_Y", control, target)
+    def apply_YC_Z(self, control, target): self._g2("YC_Z", control, target)
+    def apply_SWAP(self, qubit1, qubit2): self._g2("SWAP", qubit1, qubit2)
+    def apply_iSWAP(self, qubit1, qubit2): self._g2("ISWAP", qubit1, qubit2)
+
+    def apply_RX(self, qubit, angle):
+        self._q(qubit)
+        self._st.apply_rotation_gate("X", qubit, angle)
+
+    def apply_RY(self, qubit, angle):
+        self._q(qubit)
+        self._st.apply_rotation_gate("Y", qubit, angle)
+
+    def apply_RZ(self, qubit, angle):
+        self._q(qubit)
+        self._st.apply_rotation_gate("Z", qubit, angle)
+
     # -- operators ---------------------------------------------------------
     def __mul__(self, other):
         out = self._copy()

@@ -125,6 +125,19 @@ class State:
             _abi.check(self._lib.pl_state_trim_protected(self._h, int(max_terms), keep._h),
                        "pl_state_trim_protected")
 
+    def apply_clifford(self, gate, q1, q2=0):
+        """Bulk Clifford gate (name from _abi.GATES or its PL_GATE_* number)."""
+        g = _abi.GATES[gate] if isinstance(gate, str) else int(gate)
+        _abi.check(self._lib.pl_state_apply_clifford(self._h, g, int(q1), int(q2)),
+                   "pl_state_apply_clifford")
+
+    def apply_rotation_gate(self, axis, qubit, angle):
+        """apply_RX / RY / RZ: axis "X"/"Y"/"Z" (or 1/2/3), exp(-i angle/2 P)."""
+        a = {"X": 1, "Y": 2, "Z": 3}.get(axis, axis)
+        _abi.check(self._lib.pl_state_apply_rotation_gate(self._h, int(a), int(qubit),
+                                                          float(angle)),
+                   "pl_state_apply_rotation_gate")
+
     def apply_cnot(self, c, t):
         _abi.check(self._lib.pl_state_apply_cnot(self._h, int(c), int(t)), "pl_state_apply_cnot")
 

@@ -155,6 +155,18 @@ int main() {
         }
         EXPECT(std::fabs(h.zero_state_expectation() - e) <= 1e-12);
     }
+    // PauliSumTests.cpp:313-325 and 243-256: H gates and apply_RZ
+    {
+        PauliSum<4> s(Terms{{"IZXY", 1.0}});
+        for (std::size_t q = 0; q < 4; ++q) s.apply_H(q);
+        EXPECT(s.get_str() == "1.000000 * -IXZY\n");
+        PauliSum<1> r(Terms{{"Z", 2.0}, {"X", 1.0}});
+        r.apply_RZ(0, M_PI / 3.0);
+        EXPECT(r.get_str() == "2.000000 * Z\n0.866025 * X\n0.500000 * -Y\n");
+        PauliSum<2> c(Terms{{"XI", 1.0}});
+        c.apply_iSWAP(0, 1);
+        EXPECT(c.get_str() == "1.000000 * ZY\n");
+    }
     // errors map to the reference's exception types
     {
         bool threw = false;
