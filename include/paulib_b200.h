@@ -267,6 +267,24 @@ PL_API int pl_state_trim(pl_state* state, uint64_t max_terms);
  * left of max_terms. */
 PL_API int pl_state_trim_protected(pl_state* state, uint64_t max_terms, pl_state* keep);
 PL_API int pl_state_zero_state_expectation(pl_state* state, double* result);
+/* basis_state_expectation (PauliSumUtils.h:178-220): <x| sum |x> for the
+ * basis state whose bit q (word q/64, bit q%64 of bit_words[0..AS)) is
+ * qubit q's value. */
+PL_API int pl_state_basis_state_expectation(pl_state* state, const uint64_t* bit_words,
+                                            double* result);
+/* trace (PauliSumUtils.h:226-245): 2^num_qubits times the signed sum of the
+ * real-phase identity terms. */
+PL_API int pl_state_trace(pl_state* state, int num_qubits, double* result);
+/* frobenius_norm2 (PauliSumUtils.h:400-410): sum of squared coefficients
+ * (tr(O^dagger O) / 2^n of a canonical sum). */
+PL_API int pl_state_frobenius_norm2(pl_state* state, double* result);
+/* lookup (PauliSumUtils.h:246-268): coefficient of the string (x, z words,
+ * flags), phases relative to the query, +-i terms skipped. */
+PL_API int pl_state_lookup(pl_state* state, const uint64_t* x, const uint64_t* z,
+                           uint8_t flags, double* result);
+/* trace_product (PauliSumUtils.h:412-447): Re tr(A B) = 2^num_qubits times the
+ * sum over shared patterns of Re(w_A * w_B). */
+PL_API int pl_state_trace_product(pl_state* a, pl_state* b, int num_qubits, double* result);
 
 /* lhs := lhs * rhs, the outer product in the reference's i*n + j order
  * (PauliSum::multiply, PauliSumOperations.h:256-306).  lhs and rhs may be

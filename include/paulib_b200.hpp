@@ -289,6 +289,40 @@ public:
         check(pl_state_zero_state_expectation(s_, &r), "zero_state_expectation");
         return r;
     }
+    // PauliSumUtils.h:178-268, 400-410.
+    T basis_state_expectation(const std::string& bits) const {
+        if (bits.size() != nq_)
+            throw std::invalid_argument("basis_state_expectation: bit string length " +
+                                        std::to_string(bits.size()) + " does not match " +
+                                        std::to_string(nq_) + " qubits");
+        std::vector<uint64_t> w(ArraySize, 0);
+        for (std::size_t q = 0; q < bits.size(); ++q) {
+            if (bits[q] != '0' && bits[q] != '1')
+                throw std::invalid_argument(
+                    "basis_state_expectation: bit string must contain only '0'/'1'");
+            if (bits[q] == '1') w[q / 64] |= 1ull << (q % 64);
+        }
+        double r = 0.0;
+        check(pl_state_basis_state_expectation(s_, w.data(), &r), "basis_state_expectation");
+        return r;
+    }
+    T trace() const {
+        double r = 0.0;
+        check(pl_state_trace(s_, (int)nq_, &r), "trace");
+        return r;
+    }
+    T frobenius_norm2() const {
+        double r = 0.0;
+        check(pl_state_frobenius_norm2(s_, &r), "frobenius_norm2");
+        return r;
+    }
+    T lookup(const std::string& pauli_string) const {
+        const ParsedString p = parse_pauli(pauli_string, ArraySize);
+        double r = 0.0;
+        check(pl_state_lookup(s_, p.x.data(), p.z.data(), p.flags, &r), "lookup");
+        return r;
+    }
+
     // PauliSumUtils.h:19-33: "%f * <string>" per term.
     std::string get_str() {
         download();
@@ -349,6 +383,17 @@ PauliSum<N, T> i_commutator(const PauliSum<N, T>& a, const PauliSum<N, T>& b) {
     PauliSum<N, T> out(a.num_qubits());
     check(pl_state_commutator(out.handle(), a.handle(), b.handle(), 1), "i_commutator");
     return out;
+}
+
+// trace_product (PauliSumUtils.h:412-447): Re tr(A B).
+template <std::size_t N, typename T>
+T trace_product(const PauliSum<N, T>& a, const PauliSum<N, T>& b) {
+    if (a.num_qubits() != b.num_qubits())
+        throw std::invalid_argument("trace_product: qubit-count mismatch");
+    double r = 0.0;
+    check(pl_state_trace_product(a.handle(), b.handle(), (int)a.num_qubits(), &r),
+          "trace_product");
+    return r;
 }
 
 // propagate (PauliPropagation.h:54-63): the rotations (generator = term,

@@ -121,6 +121,22 @@ class _Impl:
         fn(h, *args)
         return self._take(h, p.array_size)
 
+    def _scalar(self, p, fn, *args):
+        h = self._make(p)
+        try:
+            return fn(h, *args)
+        finally:
+            self._free(h)
+
+    def frobenius_norm2(self, p) -> float:
+        return self._scalar(p, getattr(self.lib, self.prefix + "frobenius_norm2"))
+
+    def lookup(self, p, x, z, f) -> float:
+        x = np.ascontiguousarray(x, np.uint64)
+        z = np.ascontiguousarray(z, np.uint64)
+        return self._scalar(p, getattr(self.lib, self.prefix + "lookup"), _c(x, U64P),
+                            _c(z, U64P), int(f))
+
     def apply_clifford(self, p, gate: int, c: int, t: int = 0):
         """Bulk Clifford gate number `gate` (the library's PL_GATE_* values)."""
         return self._inplace(p, getattr(self.lib, self.prefix + "apply_clifford"), int(gate),
@@ -151,6 +167,13 @@ class Oracle(_Impl):
         L.or_trim_protected.argtypes = [C.c_void_p, C.c_uint64, C.c_void_p]
         L.or_apply_clifford.argtypes = [C.c_void_p, C.c_int, C.c_uint64, C.c_uint64]
         L.or_apply_rgate.argtypes = [C.c_void_p, C.c_int, C.c_uint64, C.c_double]
+        for name, args in (("or_basis_state_expectation", [C.c_void_p, U64P]),
+                           ("or_trace", [C.c_void_p, C.c_int]),
+                           ("or_frobenius_norm2", [C.c_void_p]),
+                           ("or_lookup", [C.c_void_p, U64P, U64P, C.c_uint8]),
+                           ("or_trace_product", [C.c_void_p, C.c_void_p, C.c_int])):
+            getattr(L, name).restype = C.c_double
+            getattr(L, name).argtypes = args
         L.or_apply_cnot.argtypes = [C.c_void_p, C.c_uint64, C.c_uint64]
         L.or_zero_state_expectation.restype = C.c_double
         L.or_zero_state_expectation.argtypes = [C.c_void_p]
@@ -175,6 +198,20 @@ class Oracle(_Impl):
 
     def trim(self, p, m):
         return self._inplace(p, self.lib.or_trim, int(m))
+
+    def basis_state_expectation(self, p, bit_words) -> float:
+        w = np.ascontiguousarray(bit_words, np.uint64)
+        return self._scalar(p, self.lib.or_basis_state_expectation, _c(w, U64P))
+
+    def trace(self, p, num_qubits: int) -> float:
+        return self._scalar(p, self.lib.or_trace, int(num_qubits))
+
+    def trace_product(self, a, b, num_qubits: int) -> float:
+        hb = self._make(b)
+        try:
+            return self._scalar(a, self.lib.or_trace_product, hb, int(num_qubits))
+        finally:
+            self._free(hb)
 
     def trim_protected(self, p, m, keep):
         hk = self._make(keep)
@@ -256,6 +293,13 @@ class Reference(_Impl):
         L.ref_trim_protected.argtypes = [C.c_void_p, C.c_uint64, C.c_void_p]
         L.ref_apply_clifford.argtypes = [C.c_void_p, C.c_int, C.c_uint64, C.c_uint64]
         L.ref_apply_rgate.argtypes = [C.c_void_p, C.c_int, C.c_uint64, C.c_double]
+        for name, args in (("ref_basis_state_expectation", [C.c_void_p, C.c_char_p]),
+                           ("ref_trace", [C.c_void_p]),
+                           ("ref_frobenius_norm2", [C.c_void_p]),
+                           ("ref_lookup", [C.c_void_p, U64P, U64P, C.c_uint8]),
+                           ("ref_trace_product", [C.c_void_p, C.c_void_p])):
+            getattr(L, name).restype = C.c_double
+            getattr(L, name).argtypes = args
         L.ref_apply_cnot.argtypes = [C.c_void_p, C.c_uint64, C.c_uint64]
         L.ref_zero_state_expectation.restype = C.c_double
         L.ref_zero_state_expectation.argtypes = [C.c_void_p]
@@ -292,6 +336,25 @@ class Reference(_Impl):
 
     def trim(self, p, m):
         return self._inplace(p, self.lib.ref_trim, int(m))
+
+    # the reference build's sums have num_qubits = 64 * array_size
+    def basis_state_expectation(self, p, bit_words) -> float:
+        nq = 64 * p.array_size
+        bits = "".join("1" if (int(bit_words[q // 64]) >> (q % 64)) & 1 else "0"
+                       for q in range(nq))
+        return self._scalar(p, self.lib.ref_basis_state_expectation, bits.encode())
+
+    def trace(self, p, num_qubits: int) -> float:
+        assert num_qubits == 64 * p.array_size
+        return self._scalar(p, self.lib.ref_trace)
+
+    def trace_product(self, a, b, num_qubits: int) -> float:
+        assert num_qubits == 64 * a.array_size
+        hb = self._make(b)
+        try:
+            return self._scalar(a, self.lib.ref_trace_product, hb)
+        finally:
+            self._free(hb)
 
     def trim_protected(self, p, m, keep):
         hk = self._make(keep)

@@ -461,6 +461,93 @@ OR_EXPORT int or_apply_rgate(or_sum *s, int axis, u64 c, double angle) {
     return 0;
 }
 
+/* basis_state_expectation(bits) (PauliSumUtils.h:178-220): terms with no X
+ * bit and a real phase contribute +-value, negated once more per set bit of
+ * the basis state under a Z; summed in term order.  bits: AS words. */
+OR_EXPORT double or_basis_state_expectation(const or_sum *s, const u64 *bits) {
+    double r = 0.0;
+    for (i64 i = 0; i < s->n; ++i) {
+        int has_x = 0, par = 0;
+        for (int k = 0; k < s->as; ++k) {
+            has_x |= SX(s, k, i) != 0;
+            par ^= __builtin_popcountll(SZ(s, k, i) & bits[k]) & 1;
+        }
+        if (has_x || (s->f[i] & 1)) continue;
+        const double sg = ((s->f[i] & 2) ? -1.0 : 1.0) * (par ? -1.0 : 1.0);
+        r += sg * s->v[i];
+    }
+    return r;
+}
+
+/* trace() (PauliSumUtils.h:226-245): 2^nq times the signed sum of the
+ * identity terms with a real phase. */
+OR_EXPORT double or_trace(const or_sum *s, int nq) {
+    double r = 0.0;
+    for (i64 i = 0; i < s->n; ++i) {
+        int id = 1;
+        for (int k = 0; k < s->as; ++k) id &= (SX(s, k, i) | SZ(s, k, i)) == 0;
+        if (!id || (s->f[i] & 1)) continue;
+        r += ((s->f[i] & 2) ? -1.0 : 1.0) * s->v[i];
+    }
+    return ldexp(r, nq);
+}
+
+/* lookup(ps) (PauliSumUtils.h:246-268): signed sum of the values of the
+ * terms with ps's (x, z), phase taken relative to ps's; terms off by +-i
+ * are skipped. */
+OR_EXPORT double or_lookup(const or_sum *s, const u64 *x, const u64 *z, u8 f) {
+    double r = 0.0;
+    for (i64 i = 0; i < s->n; ++i) {
+        int match = 1;
+        for (int k = 0; k < s->as; ++k) match &= SX(s, k, i) == x[k] && SZ(s, k, i) == z[k];
+        if (!match) continue;
+        const u8 rel = (u8)((s->f[i] - f) & 3);
+        if (rel & 1) continue;
+        r += (rel & 2) ? -s->v[i] : s->v[i];
+    }
+    return r;
+}
+
+/* frobenius_norm2() (PauliSumUtils.h:400-410): sum of squared values. */
+OR_EXPORT double or_frobenius_norm2(const or_sum *s) {
+    double r = 0.0;
+    for (i64 i = 0; i < s->n; ++i) r += s->v[i] * s->v[i];
+    return r;
+}
+
+/* trace_product(a, b) (PauliSumUtils.h:412-447): Re tr(A B).  Per (x, z)
+ * pattern of A the complex weight sum c i^k is accumulated in A's term
+ * order; every term of B with that pattern adds 2^nq Re(w * c_b i^k_b), in
+ * B's order (the reference's hash map, restated as a scan). */
+OR_EXPORT double or_trace_product(const or_sum *a, const or_sum *b, int nq) {
+    double r = 0.0;
+    for (i64 j = 0; j < b->n; ++j) {
+        double re = 0.0, im = 0.0;
+        int found = 0;
+        for (i64 i = 0; i < a->n; ++i) {
+            int match = 1;
+            for (int k = 0; k < a->as; ++k)
+                match &= SX(a, k, i) == SX(b, k, j) && SZ(a, k, i) == SZ(b, k, j);
+            if (!match) continue;
+            found = 1;
+            switch (a->f[i] & 3) {
+            case 0: re += a->v[i]; break;
+            case 1: im += a->v[i]; break;
+            case 2: re -= a->v[i]; break;
+            default: im -= a->v[i]; break;
+            }
+        }
+        if (!found) continue;
+        switch (b->f[j] & 3) {
+        case 0: r += re * b->v[j]; break;
+        case 1: r -= im * b->v[j]; break;
+        case 2: r -= re * b->v[j]; break;
+        default: r += im * b->v[j]; break;
+        }
+    }
+    return ldexp(r, nq);
+}
+
 /* zero_state_expectation (PauliSumUtils.h:163-177): terms with no X bit and
  * a real phase contribute +-value, summed in term order. */
 OR_EXPORT double or_zero_state_expectation(const or_sum *s) {

@@ -49,6 +49,11 @@ struct SumBase {
     virtual void trim_protected(u64 max_terms, const SumBase* keep) = 0;
     virtual int apply_clifford(int gate, u64 c, u64 t) = 0;
     virtual int apply_rgate(int axis, u64 c, double angle) = 0;
+    virtual double basis_state_expectation(const char* bits) const = 0;
+    virtual double trace() const = 0;
+    virtual double frobenius_norm2() const = 0;
+    virtual double lookup(const u64* x, const u64* z, u8 f) const = 0;
+    virtual double trace_product(const SumBase* b) const = 0;
 };
 
 template <std::size_t N>
@@ -132,6 +137,24 @@ struct Sum final : SumBase {
             default: return -1;
         }
         return 0;
+    }
+    // num_qubits_ of these sums is the capacity N = 64 * AS
+    double basis_state_expectation(const char* bits) const override {
+        return s.basis_state_expectation(std::string(bits));
+    }
+    double trace() const override { return s.trace(); }
+    double frobenius_norm2() const override { return s.frobenius_norm2(); }
+    double lookup(const u64* x, const u64* z, u8 f) const override {
+        paulib::PauliString<N> ps;
+        for (int k = 0; k < AS; ++k) {
+            ps.x[k] = (std::size_t)x[k];
+            ps.z[k] = (std::size_t)z[k];
+        }
+        ps.flags = f;
+        return s.lookup(ps);
+    }
+    double trace_product(const SumBase* b) const override {
+        return paulib::trace_product(s, static_cast<const Sum*>(b)->s);
     }
     int apply_rgate(int axis, u64 c, double angle) override {
         if (axis == 1) s.apply_RX((std::size_t)c, angle);
@@ -223,6 +246,23 @@ __attribute__((visibility("default"))) int ref_apply_clifford(void* h, int g, u6
 }
 __attribute__((visibility("default"))) int ref_apply_rgate(void* h, int axis, u64 c, double a) {
     return ((SumBase*)h)->apply_rgate(axis, c, a);
+}
+__attribute__((visibility("default"))) double ref_basis_state_expectation(const void* h,
+                                                                         const char* bits) {
+    return ((const SumBase*)h)->basis_state_expectation(bits);
+}
+__attribute__((visibility("default"))) double ref_trace(const void* h) {
+    return ((const SumBase*)h)->trace();
+}
+__attribute__((visibility("default"))) double ref_frobenius_norm2(const void* h) {
+    return ((const SumBase*)h)->frobenius_norm2();
+}
+__attribute__((visibility("default"))) double ref_lookup(const void* h, const u64* x,
+                                                         const u64* z, u8 f) {
+    return ((const SumBase*)h)->lookup(x, z, f);
+}
+__attribute__((visibility("default"))) double ref_trace_product(const void* a, const void* b) {
+    return ((const SumBase*)a)->trace_product((const SumBase*)b);
 }
 __attribute__((visibility("default"))) void ref_trim_protected(void* h, u64 m, const void* k) {
     ((SumBase*)h)->trim_protected(m, (const SumBase*)k);

@@ -1118,6 +1118,147 @@ __global__ void __launch_bounds__(kPT)
     }
 }
 
+// ---------------------------------------------------------------------------
+// Reductions over a sum's terms: basis_state_expectation, trace, lookup and
+// frobenius_norm2 (PauliSumUtils.h:178-268, 400-410), and the join of
+// trace_product (PauliSumUtils.h:412-447).  Each thread sums its strided
+// terms in order, blocks reduce with a fixed tree and one block adds the
+// block sums in order: a deterministic order (not the reference's term
+// order, so results agree within rounding).
+// ---------------------------------------------------------------------------
+enum RedKind : int { kRedBasis = 0, kRedTrace = 1, kRedFrob = 2, kRedLookup = 3 };
+constexpr int kRedBlocks = 296;
+
+struct RedArgs {
+    int kind;
+    u32 qf;             // lookup: flags of the query
+    u64 bits[kMaxAS];   // basis state, one bit per qubit
+    u64 qx[kMaxAS];     // lookup: the query string
+    u64 qz[kMaxAS];
+};
+
+template <int AS>
+__device__ __forceinline__ double red_term(const Buf& b, i64 i, const RedArgs& R) {
+    const u32 f = b.f[i];
+    const double v = b.v[i];
+    if (R.kind == kRedFrob) return dmul(v, v);
+    if (R.kind == kRedLookup) {
+        bool match = true;
+#pragma unroll
+        for (int k = 0; k < AS; ++k)
+            match = match && b.x[k * b.cap + i] == R.qx[k] && b.z[k * b.cap + i] == R.qz[k];
+        if (!match) return 0.0;
+        const u32 rel = (f - R.qf) & 3u;
+        if (rel & 1u) return 0.0;
+        return (rel & 2u) ? -v : v;
+    }
+    // basis state / trace: real-phase terms without X (and, for trace, without Z)
+    u64 xs = 0, zs = 0;
+    u32 par = 0;
+#pragma unroll
+    for (int k = 0; k < AS; ++k) {
+        const u64 z = b.z[k * b.cap + i];
+        xs |= b.x[k * b.cap + i];
+        zs |= z;
+        par ^= (u32)__popcll(z & R.bits[k]);
+    }
+    if (xs != 0 || (f & 1u)) return 0.0;
+    if (R.kind == kRedTrace && zs != 0) return 0.0;
+    const bool neg = ((f >> 1) & 1u) ^ (R.kind == kRedBasis ? (par & 1u) : 0u);
+    return neg ? -v : v;
+}
+
+__device__ __forceinline__ double block_tree_sum(double a, double* sm) {
+    sm[threadIdx.x] = a;
+    __syncthreads();
+    for (int st = blockDim.x / 2; st > 0; st >>= 1) {
+        if ((int)threadIdx.x < st) sm[threadIdx.x] = dadd(sm[threadIdx.x], sm[threadIdx.x + st]);
+        __syncthreads();
+    }
+    return sm[0];
+}
+
+template <int AS>
+__global__ void __launch_bounds__(256) k_reduce_terms(Buf b, const i64* d_n, RedArgs R,
+                                                      double* partial) {
+    __shared__ double sm[256];
+    const i64 n = *d_n;
+    double acc = 0.0;
+    for (i64 i = (i64)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+         i += (i64)gridDim.x * blockDim.x)
+        acc = dadd(acc, red_term<AS>(b, i, R));
+    const double s = block_tree_sum(acc, sm);
+    if (threadIdx.x == 0) partial[blockIdx.x] = s;
+}
+
+// The block sums in order, times 2^exp2.
+__global__ void __launch_bounds__(256) k_sum_partials(const double* partial, int np, int exp2,
+                                                      double* out) {
+    __shared__ double sm[256];
+    double acc = 0.0;
+    for (int i = threadIdx.x; i < np; i += blockDim.x) acc = dadd(acc, partial[i]);
+    const double s = block_tree_sum(acc, sm);
+    if (threadIdx.x == 0) *out = scalbn(s, exp2);
+}
+
+// trace_product join: A canonical (sorted by (x, z, phase), sign folded into
+// the value), so the complex weight of a pattern is (value of its phase-0
+// entry, value of its phase-1 entry).  Each term of B finds its pattern by
+// binary search and adds Re(w * c_b * i^k_b).
+template <int AS>
+__device__ __forceinline__ int xz_cmp(const Buf& a, i64 i, const u64* x, const u64* z) {
+#pragma unroll
+    for (int k = 0; k < AS; ++k) {
+        const u64 v = a.x[k * a.cap + i];
+        if (v != x[k]) return v < x[k] ? -1 : 1;
+    }
+#pragma unroll
+    for (int k = 0; k < AS; ++k) {
+        const u64 v = a.z[k * a.cap + i];
+        if (v != z[k]) return v < z[k] ? -1 : 1;
+    }
+    return 0;
+}
+
+template <int AS>
+__global__ void __launch_bounds__(256) k_trace_join(Buf A, const i64* d_na, Buf B,
+                                                    const i64* d_nb, double* partial) {
+    __shared__ double sm[256];
+    const i64 na = *d_na, nb = *d_nb;
+    double acc = 0.0;
+    for (i64 j = (i64)blockIdx.x * blockDim.x + threadIdx.x; j < nb;
+         j += (i64)gridDim.x * blockDim.x) {
+        u64 x[AS], z[AS];
+#pragma unroll
+        for (int k = 0; k < AS; ++k) {
+            x[k] = B.x[k * B.cap + j];
+            z[k] = B.z[k * B.cap + j];
+        }
+        i64 lo = 0, hi = na;  // first entry of A with (x, z) >= the pattern
+        while (lo < hi) {
+            const i64 mid = (lo + hi) >> 1;
+            if (xz_cmp<AS>(A, mid, x, z) < 0) lo = mid + 1;
+            else hi = mid;
+        }
+        double re = 0.0, im = 0.0;
+        for (i64 i = lo; i < na && i < lo + 2 && xz_cmp<AS>(A, i, x, z) == 0; ++i) {
+            if (A.f[i] & 1u) im = A.v[i];
+            else re = A.v[i];
+        }
+        const double v = B.v[j];
+        double c;
+        switch (B.f[j] & 3u) {
+            case 0: c = dmul(re, v); break;
+            case 1: c = -dmul(im, v); break;
+            case 2: c = -dmul(re, v); break;
+            default: c = dmul(im, v); break;
+        }
+        acc = dadd(acc, c);
+    }
+    const double s = block_tree_sum(acc, sm);
+    if (threadIdx.x == 0) partial[blockIdx.x] = s;
+}
+
 // Order-preserving filters cutoff / truncate_weight (PauliSumUtils.h:378-393).
 template <int AS>
 __global__ void __launch_bounds__(kPT) k_filter(Buf in, i64 n, Buf out, double eps,
@@ -1789,6 +1930,7 @@ struct pl_state {
     cudaStream_t cap_st = nullptr;  // private stream the chains are captured on
     void* trim_mem = nullptr;       // trim control block and per-tile counts
     size_t trim_bytes = 0;
+    double* red = nullptr;          // block sums and the result of a reduction
 };
 
 namespace pl {
@@ -2531,6 +2673,7 @@ extern "C" int pl_state_destroy(pl_state* s) {
     if (s->ws.ptr) dev_free(s->ws.ptr, s->st);
     s->ws.ptr = nullptr;
     if (s->trim_mem) dev_free(s->trim_mem, s->st);
+    if (s->red) dev_free(s->red, s->st);
     cudaStreamSynchronize(s->st);
     delete s;
     return record_status(PL_OK, nullptr);
@@ -2867,6 +3010,106 @@ extern "C" int pl_state_apply_rotation_gate(pl_state* s, int axis, int qubit, do
     if (rc) return rc;
     s->cls = 0;
     return record_status(PL_OK, nullptr);
+}
+
+namespace pl {
+namespace {
+int ensure_red(pl_state* s) {
+    if (!s->red) PL_CUDA_TRY(dev_alloc(reinterpret_cast<void**>(&s->red),
+                                       sizeof(double) * (kRedBlocks + 1), s->st));
+    return PL_OK;
+}
+
+int finish_red(pl_state* s, int exp2, double* result) {
+    k_sum_partials<<<1, 256, 0, s->st>>>(s->red, kRedBlocks, exp2, s->red + kRedBlocks),
+        pl::note_launch();
+    PL_CUDA_TRY(cudaMemcpyAsync(result, s->red + kRedBlocks, sizeof(double),
+                                cudaMemcpyDeviceToHost, s->st));
+    PL_CUDA_TRY(cudaStreamSynchronize(s->st));
+    return record_status(PL_OK, nullptr);
+}
+
+int reduce_state(pl_state* s, const RedArgs& R, int exp2, double* result) {
+    int rc = ensure_red(s);
+    if (rc) return rc;
+    PL_DISPATCH_AS(s->as, k_reduce_terms<AS><<<kRedBlocks, 256, 0, s->st>>>(
+                              s->S[s->cur], s->d_size + s->cur, R, s->red),
+                          pl::note_launch());
+    return finish_red(s, exp2, result);
+}
+}  // namespace
+}  // namespace pl
+
+extern "C" int pl_state_basis_state_expectation(pl_state* s, const uint64_t* bit_words,
+                                                double* result) {
+    int rc = check_state(s);
+    if (rc) return rc;
+    if (!bit_words || !result)
+        return record_status(PL_ERR_INVALID_ARG, "pl_state_basis_state_expectation");
+    RedArgs R{};
+    R.kind = kRedBasis;
+    for (int k = 0; k < s->as; ++k) R.bits[k] = bit_words[k];
+    return reduce_state(s, R, 0, result);
+}
+
+extern "C" int pl_state_trace(pl_state* s, int num_qubits, double* result) {
+    int rc = check_state(s);
+    if (rc) return rc;
+    if (!result || num_qubits < 0 || num_qubits > 64 * s->as)
+        return record_status(PL_ERR_INVALID_ARG, "pl_state_trace");
+    RedArgs R{};
+    R.kind = kRedTrace;
+    return reduce_state(s, R, num_qubits, result);
+}
+
+extern "C" int pl_state_frobenius_norm2(pl_state* s, double* result) {
+    int rc = check_state(s);
+    if (rc) return rc;
+    if (!result) return record_status(PL_ERR_INVALID_ARG, "pl_state_frobenius_norm2");
+    RedArgs R{};
+    R.kind = kRedFrob;
+    return reduce_state(s, R, 0, result);
+}
+
+extern "C" int pl_state_lookup(pl_state* s, const uint64_t* x, const uint64_t* z,
+                               uint8_t flags, double* result) {
+    int rc = check_state(s);
+    if (rc) return rc;
+    if (!x || !z || !result) return record_status(PL_ERR_INVALID_ARG, "pl_state_lookup");
+    RedArgs R{};
+    R.kind = kRedLookup;
+    R.qf = flags & 3u;
+    for (int k = 0; k < s->as; ++k) {
+        R.qx[k] = x[k];
+        R.qz[k] = z[k];
+    }
+    return reduce_state(s, R, 0, result);
+}
+
+extern "C" int pl_state_trace_product(pl_state* a, pl_state* b, int num_qubits,
+                                      double* result) {
+    int rc = check_state(a);
+    if (rc) return rc;
+    if ((rc = check_state(b))) return rc;
+    if (!result || a->as != b->as || num_qubits < 0 || num_qubits > 64 * a->as)
+        return record_status(PL_ERR_INVALID_ARG, "pl_state_trace_product");
+    if (b->st != a->st) PL_CUDA_TRY(cudaStreamSynchronize(b->st));
+    // A's complex weight per pattern: a canonicalized copy
+    pl_state* t = nullptr;
+    rc = pl_state_create(&t, a->as, 1 << 16, a->st);
+    if (rc) return rc;
+    rc = pl_state_append(t, a);
+    if (!rc) rc = pl_state_canonicalize(t);
+    if (!rc) rc = ensure_red(a);
+    if (!rc) {
+        PL_DISPATCH_AS(a->as, k_trace_join<AS><<<kRedBlocks, 256, 0, a->st>>>(
+                                  t->S[t->cur], t->d_size + t->cur, b->S[b->cur],
+                                  b->d_size + b->cur, a->red),
+                              pl::note_launch());
+        rc = finish_red(a, num_qubits, result);
+    }
+    pl_state_destroy(t);
+    return rc ? rc : record_status(PL_OK, nullptr);
 }
 
 extern "C" int pl_state_zero_state_expectation(pl_state* s, double* result) {

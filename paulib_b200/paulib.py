@@ -146,6 +146,31 @@ class _PauliSum:
     def zero_state_expectation(self) -> float:
         return self._st.zero_state_expectation()
 
+    # -- reductions (PauliSumUtils.h:178-268, 400-410) ---------------------
+    def basis_state_expectation(self, bits: str) -> float:
+        if len(bits) != self._nq:
+            raise ValueError(f"basis_state_expectation: bit string length {len(bits)} does "
+                             f"not match {self._nq} qubits")
+        if any(c not in "01" for c in bits):
+            raise ValueError("basis_state_expectation: bit string must contain only '0'/'1'")
+        w = np.zeros(self._aw, np.uint64)
+        for q, c in enumerate(bits):
+            if c == "1":
+                w[q // 64] |= np.uint64(1) << np.uint64(q % 64)
+        return self._st.basis_state_expectation(w)
+
+    def trace(self) -> float:
+        return self._st.trace(self._nq)
+
+    def frobenius_norm2(self) -> float:
+        return self._st.frobenius_norm2()
+
+    def lookup(self, pauli_string: str) -> float:
+        x, z, f, nq = strings.parse(pauli_string, self._aw)
+        if nq > self._nq:
+            raise ValueError("Pauli string has more qubits than the sum")
+        return self._st.lookup(np.array(x, np.uint64), np.array(z, np.uint64), f)
+
     # -- Clifford and rotation gates (PauliSumClifford.h, PauliSumOperations.h:29-104)
     def _q(self, *qs):
         for q in qs:
@@ -256,6 +281,13 @@ def _comm(a, b, mul_i):
     return out
 
 
+def trace_product(a: _PauliSum, b: _PauliSum) -> float:
+    """Re tr(A*B), computed without forming the product."""
+    if a._nq != b._nq:
+        raise ValueError("trace_product: qubit-count mismatch")
+    return a._st.trace_product(b._st, a._nq)
+
+
 def propagate_expectation(observable: _PauliSum, rotations: _PauliSum,
                           options: TruncationOptions | None = None) -> float:
     """Pauli propagation: <0|U^dagger O U|0> for the rotation circuit U
@@ -268,5 +300,5 @@ def propagate_expectation(observable: _PauliSum, rotations: _PauliSum,
     return out.zero_state_expectation()
 
 
-__all__ = ["PauliSum", "TruncationOptions", "commutator", "i_commutator",
+__all__ = ["PauliSum", "TruncationOptions", "commutator", "i_commutator", "trace_product",
            "propagate_expectation", "MAX_QUBITS"]

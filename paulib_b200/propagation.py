@@ -125,6 +125,33 @@ class State:
             _abi.check(self._lib.pl_state_trim_protected(self._h, int(max_terms), keep._h),
                        "pl_state_trim_protected")
 
+    # -- reductions (PauliSumUtils.h:178-268, 400-447) --------------------
+    def _scalar(self, fn, *args, what=""):
+        r = C.c_double()
+        _abi.check(fn(self._h, *args, C.byref(r)), what)
+        return r.value
+
+    def basis_state_expectation(self, bit_words):
+        w = np.ascontiguousarray(bit_words, np.uint64)
+        return self._scalar(self._lib.pl_state_basis_state_expectation, _ptr(w),
+                            what="pl_state_basis_state_expectation")
+
+    def trace(self, num_qubits):
+        return self._scalar(self._lib.pl_state_trace, int(num_qubits), what="pl_state_trace")
+
+    def frobenius_norm2(self):
+        return self._scalar(self._lib.pl_state_frobenius_norm2, what="pl_state_frobenius_norm2")
+
+    def lookup(self, x_words, z_words, flags):
+        x = np.ascontiguousarray(x_words, np.uint64)
+        z = np.ascontiguousarray(z_words, np.uint64)
+        return self._scalar(self._lib.pl_state_lookup, _ptr(x), _ptr(z), int(flags) & 3,
+                            what="pl_state_lookup")
+
+    def trace_product(self, other: "State", num_qubits):
+        return self._scalar(self._lib.pl_state_trace_product, other._h, int(num_qubits),
+                            what="pl_state_trace_product")
+
     def apply_clifford(self, gate, q1, q2=0):
         """Bulk Clifford gate (name from _abi.GATES or its PL_GATE_* number)."""
         g = _abi.GATES[gate] if isinstance(gate, str) else int(gate)

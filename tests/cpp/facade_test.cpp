@@ -167,6 +167,26 @@ int main() {
         c.apply_iSWAP(0, 1);
         EXPECT(c.get_str() == "1.000000 * ZY\n");
     }
+    // PauliSumTests.cpp:715-760, 764-816, 1041-1070: reductions
+    {
+        PauliSum<2> s(Terms{{"ZI", 2.0}, {"IZ", 3.0}, {"ZZ", 4.0}});
+        s.canonicalize();
+        PauliSum<2> t(Terms{{"ZI", 2.0}, {"IZ", 3.0}, {"ZZ", 4.0}});
+        EXPECT(t.basis_state_expectation("10") == -2.0 + 3.0 - 4.0);
+        bool threw = false;
+        try {
+            t.basis_state_expectation("000");
+        } catch (const std::invalid_argument&) {
+            threw = true;
+        }
+        EXPECT(threw);
+        PauliSum<1> l(Terms{{"X", 1.0}, {"-X", 0.25}, {"iY", 2.0}});
+        EXPECT(l.lookup("X") == 0.75 && l.lookup("-iY") == -2.0);
+        PauliSum<4> tr(Terms{{"IIII", 2.5}, {"XIZI", 7.0}, {"-IIII", 1.0}, {"iIIII", 3.0}});
+        EXPECT(tr.trace() == 16.0 * 1.5);
+        PauliSum<3> a(3, "XYZ", 1.0), b(3, "XYI", 1.0);
+        EXPECT(paulib_b200::trace_product(a, a) == 8.0 && paulib_b200::trace_product(a, b) == 0.0);
+    }
     // errors map to the reference's exception types
     {
         bool threw = false;
