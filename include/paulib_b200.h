@@ -317,6 +317,24 @@ PL_API int pl_state_set_option(pl_state* state, int option, int64_t value);
 /* Device bytes the state's buffers and workspace hold. */
 PL_API int pl_state_memory(pl_state* state, uint64_t* bytes);
 
+/* ---- sharded sums: hash-owned collate across ranks ---------------------
+ *
+ * MpiPauliSum::exchange_and_combine (MpiPauliSum.h:101-181): every term is
+ * owned by rank FNV-1a(x, z) mod ranks (the phase is excluded, so P, -P and
+ * iP meet on one rank).  pl_state_shard_pack writes the state's terms as
+ * term-major records (x[0..AS), z[0..AS), flags, value bits: 2*AS+2 u64 words
+ * each) into `records` (device memory, >= n records), grouped by owner in
+ * term order, and the per-owner counts into counts[0..ranks); the caller
+ * exchanges the buckets (one all-to-all, e.g. NCCL), and the receiver loads
+ * what it got with pl_state_shard_unpack and canonicalizes.  ranks <= 64. */
+PL_API int pl_state_shard_pack(pl_state* state, int ranks, uint64_t* records, int64_t capacity,
+                               int64_t* counts);
+PL_API int pl_state_shard_unpack(pl_state* state, const uint64_t* records, int64_t n);
+/* For the global trim of a sharded sum (MpiPauliSum.h:187-210): the number
+ * of terms with |c| >= threshold, and the largest |c| (0 for an empty sum). */
+PL_API int pl_state_count_above(pl_state* state, double threshold, int64_t* count);
+PL_API int pl_state_max_abs(pl_state* state, double* result);
+
 /* ---- many propagations on one device: batch and serving ---------------
  *
  * A job is one propagate_expectation (PauliPropagation.h:65-71): the

@@ -46,7 +46,8 @@ EXPORTS = (
     "pl_serve", "pl_state_trim", "pl_state_trim_protected", "pl_state_append",
     "pl_set_tuning", "pl_get_tuning", "pl_state_apply_clifford", "pl_state_apply_rotation_gate",
     "pl_state_basis_state_expectation", "pl_state_trace", "pl_state_frobenius_norm2",
-    "pl_state_lookup", "pl_state_trace_product",
+    "pl_state_lookup", "pl_state_trace_product", "pl_state_shard_pack", "pl_state_shard_unpack",
+    "pl_state_count_above", "pl_state_max_abs",
 )
 PL_OP_CLIFFORD = 100
 GATES = {"H": 1, "S": 2, "H_YZ": 3, "H_XY": 4, "SQRT_X": 5, "SQRT_Y": 6, "X": 7, "Y": 8,
@@ -159,6 +160,10 @@ def lib():
         "pl_state_frobenius_norm2": (I32, [VP, C.POINTER(C.c_double)]),
         "pl_state_lookup": (I32, [VP, VP, VP, C.c_uint8, C.POINTER(C.c_double)]),
         "pl_state_trace_product": (I32, [VP, VP, I32, C.POINTER(C.c_double)]),
+        "pl_state_shard_pack": (I32, [VP, I32, VP, I64, C.POINTER(I64)]),
+        "pl_state_shard_unpack": (I32, [VP, VP, I64]),
+        "pl_state_count_above": (I32, [VP, C.c_double, C.POINTER(I64)]),
+        "pl_state_max_abs": (I32, [VP, C.POINTER(C.c_double)]),
         "pl_state_apply_rotation_gate": (I32, [VP, I32, I32, C.c_double]),
         "pl_set_tuning": (I32, [I32, I64]),
         "pl_get_tuning": (I32, [I32, C.POINTER(I64)]),

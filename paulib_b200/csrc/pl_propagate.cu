@@ -1126,7 +1126,14 @@ __global__ void __launch_bounds__(kPT)
 // block sums in order: a deterministic order (not the reference's term
 // order, so results agree within rounding).
 // ---------------------------------------------------------------------------
-enum RedKind : int { kRedBasis = 0, kRedTrace = 1, kRedFrob = 2, kRedLookup = 3 };
+enum RedKind : int {
+    kRedBasis = 0,
+    kRedTrace = 1,
+    kRedFrob = 2,
+    kRedLookup = 3,
+    kRedCountAbove = 4,  // terms with |c| >= threshold (exact below 2^53)
+    kRedMaxAbs = 5       // largest |c| (combined with max, not +)
+};
 constexpr int kRedBlocks = 296;
 
 struct RedArgs {
@@ -1135,6 +1142,7 @@ struct RedArgs {
     u64 bits[kMaxAS];   // basis state, one bit per qubit
     u64 qx[kMaxAS];     // lookup: the query string
     u64 qz[kMaxAS];
+    double threshold;   // count above
 };
 
 template <int AS>
@@ -1142,6 +1150,8 @@ __device__ __forceinline__ double red_term(const Buf& b, i64 i, const RedArgs& R
     const u32 f = b.f[i];
     const double v = b.v[i];
     if (R.kind == kRedFrob) return dmul(v, v);
+    if (R.kind == kRedCountAbove) return fabs(v) >= R.threshold ? 1.0 : 0.0;
+    if (R.kind == kRedMaxAbs) return fabs(v);
     if (R.kind == kRedLookup) {
         bool match = true;
 #pragma unroll
@@ -1168,11 +1178,16 @@ __device__ __forceinline__ double red_term(const Buf& b, i64 i, const RedArgs& R
     return neg ? -v : v;
 }
 
-__device__ __forceinline__ double block_tree_sum(double a, double* sm) {
+__device__ __forceinline__ double red_op(double a, double b, bool use_max) {
+    return use_max ? fmax(a, b) : dadd(a, b);
+}
+
+__device__ __forceinline__ double block_tree_sum(double a, double* sm, bool use_max = false) {
     sm[threadIdx.x] = a;
     __syncthreads();
     for (int st = blockDim.x / 2; st > 0; st >>= 1) {
-        if ((int)threadIdx.x < st) sm[threadIdx.x] = dadd(sm[threadIdx.x], sm[threadIdx.x + st]);
+        if ((int)threadIdx.x < st)
+            sm[threadIdx.x] = red_op(sm[threadIdx.x], sm[threadIdx.x + st], use_max);
         __syncthreads();
     }
     return sm[0];
@@ -1183,21 +1198,22 @@ __global__ void __launch_bounds__(256) k_reduce_terms(Buf b, const i64* d_n, Red
                                                       double* partial) {
     __shared__ double sm[256];
     const i64 n = *d_n;
+    const bool mx = R.kind == kRedMaxAbs;
     double acc = 0.0;
     for (i64 i = (i64)blockIdx.x * blockDim.x + threadIdx.x; i < n;
          i += (i64)gridDim.x * blockDim.x)
-        acc = dadd(acc, red_term<AS>(b, i, R));
-    const double s = block_tree_sum(acc, sm);
+        acc = red_op(acc, red_term<AS>(b, i, R), mx);
+    const double s = block_tree_sum(acc, sm, mx);
     if (threadIdx.x == 0) partial[blockIdx.x] = s;
 }
 
 // The block sums in order, times 2^exp2.
 __global__ void __launch_bounds__(256) k_sum_partials(const double* partial, int np, int exp2,
-                                                      double* out) {
+                                                      double* out, int use_max) {
     __shared__ double sm[256];
     double acc = 0.0;
-    for (int i = threadIdx.x; i < np; i += blockDim.x) acc = dadd(acc, partial[i]);
-    const double s = block_tree_sum(acc, sm);
+    for (int i = threadIdx.x; i < np; i += blockDim.x) acc = red_op(acc, partial[i], use_max);
+    const double s = block_tree_sum(acc, sm, use_max != 0);
     if (threadIdx.x == 0) *out = scalbn(s, exp2);
 }
 
@@ -2699,6 +2715,32 @@ extern "C" int pl_state_memory(pl_state* s, uint64_t* bytes) {
 }
 
 namespace pl {
+// Internal hooks of the sharded collate (pl_shard.cu): the current planes of
+// a state, and making room for / setting its term count.
+int state_planes(pl_state* s, u64** x, u64** z, u8** f, double** v, i64* cap, i64* n) {
+    i64 m = 0;
+    const int rc = read_size(s, &m);
+    if (rc) return rc;
+    const Buf& b = s->S[s->cur];
+    *x = b.x;
+    *z = b.z;
+    *f = b.f;
+    *v = b.v;
+    *cap = b.cap;
+    *n = m;
+    return PL_OK;
+}
+int state_reserve(pl_state* s, i64 n) { return n > s->cap ? state_grow(s, n) : PL_OK; }
+int state_set_size(pl_state* s, i64 n) {
+    PL_CUDA_TRY(cudaMemcpyAsync(s->d_size + s->cur, &n, sizeof(i64), cudaMemcpyHostToDevice,
+                                s->st));
+    PL_CUDA_TRY(cudaStreamSynchronize(s->st));
+    s->cls = 0;
+    return PL_OK;
+}
+cudaStream_t state_stream(pl_state* s) { return s->st; }
+int state_array_size(pl_state* s) { return s->as; }
+
 // Internal hooks of the batch executor (pl_batch.cu).
 void state_attach_budget(pl_state* s, MemBudget* b) {
     if (s->budget == b) return;
@@ -3020,8 +3062,8 @@ int ensure_red(pl_state* s) {
     return PL_OK;
 }
 
-int finish_red(pl_state* s, int exp2, double* result) {
-    k_sum_partials<<<1, 256, 0, s->st>>>(s->red, kRedBlocks, exp2, s->red + kRedBlocks),
+int finish_red(pl_state* s, int exp2, double* result, int use_max = 0) {
+    k_sum_partials<<<1, 256, 0, s->st>>>(s->red, kRedBlocks, exp2, s->red + kRedBlocks, use_max),
         pl::note_launch();
     PL_CUDA_TRY(cudaMemcpyAsync(result, s->red + kRedBlocks, sizeof(double),
                                 cudaMemcpyDeviceToHost, s->st));
@@ -3035,7 +3077,7 @@ int reduce_state(pl_state* s, const RedArgs& R, int exp2, double* result) {
     PL_DISPATCH_AS(s->as, k_reduce_terms<AS><<<kRedBlocks, 256, 0, s->st>>>(
                               s->S[s->cur], s->d_size + s->cur, R, s->red),
                           pl::note_launch());
-    return finish_red(s, exp2, result);
+    return finish_red(s, exp2, result, R.kind == kRedMaxAbs ? 1 : 0);
 }
 }  // namespace
 }  // namespace pl
@@ -3068,6 +3110,30 @@ extern "C" int pl_state_frobenius_norm2(pl_state* s, double* result) {
     if (!result) return record_status(PL_ERR_INVALID_ARG, "pl_state_frobenius_norm2");
     RedArgs R{};
     R.kind = kRedFrob;
+    return reduce_state(s, R, 0, result);
+}
+
+// The magnitude statistics the global trim of a sharded sum needs
+// (MpiPauliSum.h:187-210): how many |c| >= threshold, and the largest |c|.
+extern "C" int pl_state_count_above(pl_state* s, double threshold, int64_t* count) {
+    int rc = check_state(s);
+    if (rc) return rc;
+    if (!count) return record_status(PL_ERR_INVALID_ARG, "pl_state_count_above");
+    RedArgs R{};
+    R.kind = kRedCountAbove;
+    R.threshold = threshold;
+    double r = 0.0;
+    rc = reduce_state(s, R, 0, &r);
+    *count = (int64_t)r;
+    return rc;
+}
+
+extern "C" int pl_state_max_abs(pl_state* s, double* result) {
+    int rc = check_state(s);
+    if (rc) return rc;
+    if (!result) return record_status(PL_ERR_INVALID_ARG, "pl_state_max_abs");
+    RedArgs R{};
+    R.kind = kRedMaxAbs;
     return reduce_state(s, R, 0, result);
 }
 
