@@ -405,6 +405,12 @@ PL_API int pl_serve(const pl_job* jobs, int64_t count, const pl_batch_opts* opts
 /* Keys per thread of the collate engine's onesweep digit pass: 8 (default),
  * 12 or 16 (tiles of 2048, 3072 or 4096 keys).  Process-wide. */
 #define PL_TUNE_RADIX_ITEMS 1
+/* canonicalize() of a sum (or of a product) whose varying x / z bits and
+ * term index fit one 64-bit word sorts index-packed keys: 8 bytes per key
+ * and digit pass, digits over the x / z bits only, the phase split in the
+ * segment sums.  0 (default) or 1: used where it fits; -1: never (the
+ * general key + payload sort).  Results are identical either way. */
+#define PL_TUNE_INDEX_KEYS 2
 PL_API int pl_set_tuning(int key, int64_t value);
 PL_API int pl_get_tuning(int key, int64_t* value);
 

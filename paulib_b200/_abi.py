@@ -54,6 +54,7 @@ GATES = {"H": 1, "S": 2, "H_YZ": 3, "H_XY": 4, "SQRT_X": 5, "SQRT_Y": 6, "X": 7,
          "Z": 9, "I": 10, "CNOT": 11, "CZ": 12, "CY": 13, "XC_X": 14, "XC_Y": 15, "XC_Z": 16,
          "YC_X": 17, "YC_Y": 18, "YC_Z": 19, "SWAP": 20, "ISWAP": 21}
 PL_TUNE_RADIX_ITEMS = 1
+PL_TUNE_INDEX_KEYS = 2
 PL_OPT_GRAPHS = 1
 PL_ORDER_GIVEN = 0
 PL_ORDER_LONGEST_FIRST = 1

@@ -286,6 +286,44 @@ __global__ void __launch_bounds__(256) k_pack(Src src, u32 n, int mode, KeyLayou
         if (sh[i]) atomicAdd(&hist[i], sh[i]);
 }
 
+// Pack for index-packed keys (kCanonSplit): key = packed (x, z) << index
+// bits | index, the phase / sign byte (flags & 3) of each term by index, and
+// the digit histograms of the passes not derived from operand histograms.
+template <int AS, class Src>
+__global__ void __launch_bounds__(256) k_pack_split(Src src, u32 n, KeyLayout L, PassPlan P,
+                                                    u32 count_mask, u64* keys, u8* phs,
+                                                    u32* hist) {
+    __shared__ u32 sh[8 * kRadix];
+    const int np = P.npasses;
+    for (int i = threadIdx.x; i < np * kRadix; i += blockDim.x) sh[i] = 0;
+    __syncthreads();
+    const int lane = threadIdx.x & 31;
+    const u32 wstride = gridDim.x * blockDim.x;
+    for (u32 w0 = (blockIdx.x * blockDim.x + threadIdx.x) & ~31u; w0 < n; w0 += wstride) {
+        const u32 i = w0 + lane;
+        const bool valid = i < n;
+        u64 k0 = 0;
+        if (valid) {
+            u64 xw[AS], zw[AS];
+            u32 fl;
+            src.key(i, xw, zw, fl);
+            k0 = pack_chunk<AS>(L, xw, zw, 0u, 0) | (u64)i;
+            keys[i] = k0;
+            phs[i] = (u8)(fl & 3u);
+        }
+        if (!count_mask) continue;
+        for (int p = 0; p < np; ++p) {
+            if (!((count_mask >> p) & 1u)) continue;
+            const u32 d = valid ? ((u32)(k0 >> P.shift[p]) & ((1u << P.bits[p]) - 1u)) : kSentinel;
+            const u32 peers = __match_any_sync(0xffffffffu, d);
+            if (valid && lane == __ffs(peers) - 1) atomicAdd(&sh[p * kRadix + d], __popc(peers));
+        }
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < np * kRadix; i += blockDim.x)
+        if (sh[i]) atomicAdd(&hist[i], sh[i]);
+}
+
 // Digit histograms of the operands of a product.  For a digit made only of
 // x / z bits, the product's digit is the XOR of the operands' digits
 // (x = ax ^ bx, z = az ^ bz), so the histogram over all n*m products is the
@@ -461,12 +499,17 @@ struct RadixSmem {
 
 // LAST: the final pass also fetches each term's coefficient from the source
 // and writes it in sorted order, so the segment sums read contiguous values.
-template <class Src, bool LAST, int ITEMS>
-__global__ void __launch_bounds__(kThreads, ITEMS <= 8 ? 4 : (ITEMS <= 12 ? 3 : 2))
+// KONLY: index-packed keys (the term index in the bits below the digits) and
+// no payload; the last pass then reads the term's phase / sign byte phs[idx],
+// writes the coefficient with its sign folded and replaces the index bits of
+// the key by the phase bit.
+template <class Src, bool LAST, int ITEMS, bool KONLY>
+__global__ void __launch_bounds__(kThreads, KONLY ? (ITEMS <= 12 ? 4 : 3)
+                                                  : (ITEMS <= 8 ? 4 : (ITEMS <= 12 ? 3 : 2)))
     k_radix_pass(const u64* __restrict__ kin, const u32* __restrict__ vin, u64* __restrict__ kout,
                  u32* __restrict__ vout, u32 n, int shift, int bits,
                  const u32* __restrict__ bstart, u32* lb, u32* tile_ctr, int* status, Src src,
-                 double* __restrict__ val_out) {
+                 double* __restrict__ val_out, const u8* __restrict__ phs, u64 imask) {
     extern __shared__ __align__(16) unsigned char dsm[];
     u64* skeys = reinterpret_cast<u64*>(dsm);
     u32* svals = reinterpret_cast<u32*>(dsm + sizeof(u64) * (kThreads * ITEMS));
@@ -480,19 +523,14 @@ __global__ void __launch_bounds__(kThreads, ITEMS <= 8 ? 4 : (ITEMS <= 12 ? 3 : 
     const u32 dmask = (1u << bits) - 1u;
 
     u64 keys[ITEMS];
-    u32 vals[ITEMS];
+    u32 vals[KONLY ? 1 : ITEMS];
     u32 rank[ITEMS];
     const u32 wbase = base + (u32)warp * (ITEMS * 32);
 #pragma unroll
     for (int t = 0; t < ITEMS; ++t) {
         const u32 idx = wbase + t * 32 + lane;
-        if (idx < n) {
-            keys[t] = kin[idx];
-            vals[t] = vin[idx];
-        } else {
-            keys[t] = 0;
-            vals[t] = kSentinel;
-        }
+        keys[t] = idx < n ? kin[idx] : 0ull;
+        if constexpr (!KONLY) vals[t] = idx < n ? vin[idx] : kSentinel;
     }
     u32* wh = S.whist + warp * kRadix;
 #pragma unroll
@@ -532,27 +570,71 @@ __global__ void __launch_bounds__(kThreads, ITEMS <= 8 ? 4 : (ITEMS <= 12 ? 3 : 
             const u32 dd = (u32)(keys[t] >> shift) & dmask;
             const u32 pos = S.bloc[dd] + S.whist[warp * kRadix + dd] + rank[t];
             skeys[pos] = keys[t];
-            svals[pos] = vals[t];
+            if constexpr (!KONLY) svals[pos] = vals[t];
         }
     }
     __syncthreads();
     const u32 tile_n = min((u32)(kThreads * ITEMS), n - base);
+    if constexpr (KONLY && LAST) {
+        // kGather terms per thread at a time: all their gathers (phase byte,
+        // coefficient) are issued before the first one is used.
+        constexpr int kGather = 8;
+        for (u32 p0 = 0; p0 < tile_n; p0 += kGather * kThreads) {
+            u64 kk[kGather];
+            u32 gg[kGather], ph[kGather];
+            double vv[kGather];
+#pragma unroll
+            for (int b = 0; b < kGather; ++b) {
+                const u32 p = p0 + (u32)b * kThreads + tid;
+                gg[b] = 0xffffffffu;
+                kk[b] = 0;
+                ph[b] = 0;
+                vv[b] = 0.0;
+                if (p < tile_n) {
+                    const u64 k = skeys[p];
+                    const u32 dd = (u32)(k >> shift) & dmask;
+                    const u32 idx = (u32)(k & imask);
+                    kk[b] = k;
+                    gg[b] = S.gofs[dd] + (p - S.bloc[dd]);
+                    if (idx < n) {
+                        ph[b] = phs[idx];
+                        vv[b] = src.value(idx);
+                    } else {
+                        gg[b] = n;  // reported below
+                    }
+                }
+            }
+#pragma unroll
+            for (int b = 0; b < kGather; ++b) {
+                if (gg[b] < n) {
+                    kout[gg[b]] = (kk[b] & ~imask) | (u64)(ph[b] & 1u);
+                    val_out[gg[b]] = (ph[b] & 2u) ? -vv[b] : vv[b];
+                } else if (gg[b] != 0xffffffffu) {
+                    raise_status(status, PL_ERR_INTERNAL);
+                }
+            }
+        }
+        return;
+    }
     for (u32 p = tid; p < tile_n; p += kThreads) {
         const u64 k = skeys[p];
         const u32 dd = (u32)(k >> shift) & dmask;
         const u32 g = S.gofs[dd] + (p - S.bloc[dd]);
-        if (g < n) {
+        if (g >= n) {
+            raise_status(status, PL_ERR_INTERNAL);
+        } else if constexpr (KONLY) {
+            kout[g] = k;
+        } else {
             const u32 pv = svals[p];
             kout[g] = k;
             vout[g] = pv;
             if (LAST) val_out[g] = src.value(pv & kIdxMask);
-        } else {
-            raise_status(status, PL_ERR_INTERNAL);
         }
     }
 }
 
 constexpr size_t radix_smem(int items) { return (sizeof(u64) + sizeof(u32)) * kThreads * items; }
+constexpr size_t radix_smem_konly(int items) { return sizeof(u64) * kThreads * items; }
 
 // ---------------------------------------------------------------------------
 // 4. Segments: equal-key runs of the sorted order.
@@ -577,7 +659,16 @@ struct FoldFilter {
     int on;
     double cutoff;
     u32* tile_kept;
+    double2* seg2;  // kCanonSplit: (phase-0 sum, phase-1 sum) at each head
 };
+
+// canonicalize() on index-packed keys: the sort key is (x, z) only and the
+// phase bit sits in bit 0 of the sorted key; every (x, z) segment keeps two
+// sums, phase 0 and phase 1, each over its members in index order -- the
+// sums a stable sort by (x, z, phase) followed by left-to-right folding
+// gives.  Each can become one output term.  Values arrive with the sign
+// folded in.
+constexpr int kCanonSplit = 3;
 
 // Segment fold.  A warp owns 1024 consecutive sorted terms, staged in shared
 // memory; lane L folds its own 32 terms left to right (32 independent
@@ -619,26 +710,56 @@ __device__ __forceinline__ bool lane_same_key(const SegCtx& C, u32 e, u64 ke, u6
 }
 
 // One term onto a running sum: kCanon folds the sign into the value, kProp
-// keeps the sign-0 and sign-1 sums apart (S0 - S1 at the close).
+// keeps the sign-0 and sign-1 sums apart (S0 - S1 at the close), kCanonSplit
+// the phase-0 and phase-1 sums (bit 31 of p is the phase there).
 template <int MODE>
 __device__ __forceinline__ void fold_add(double& r0, double& r1, double v, u32 p) {
     const bool neg = (p >> 31) != 0;
-    if (MODE == kCanon) r0 = dadd(r0, neg ? -v : v);
+    if (MODE == kCanonSplit) {  // branch-free, as fold_term below
+        r0 = dadd(r0, neg ? 0.0 : v);
+        r1 = dadd(r1, neg ? v : 0.0);
+    } else if (MODE == kCanon) r0 = dadd(r0, neg ? -v : v);
     else if (MODE == kCombine) r0 = dadd(r0, v);
     else if (neg) r1 = dadd(r1, v);
     else r0 = dadd(r0, v);
 }
 
 // The same for a staged term whose kCanon value already carries its sign.
+//
+// kCanonSplit adds every term to both sums, +0.0 to the one it does not
+// belong to: a sum that starts at +0.0 never becomes -0.0, so adding +0.0
+// leaves it unchanged and the result is bit-identical to the branch.
 template <int MODE>
 __device__ __forceinline__ void fold_term(double& r0, double& r1, double v, u32 neg) {
-    if (MODE == kProp && neg) r1 = dadd(r1, v);
-    else r0 = dadd(r0, v);
+    if (MODE == kCanonSplit) {
+        r0 = dadd(r0, neg ? 0.0 : v);
+        r1 = dadd(r1, neg ? v : 0.0);
+    } else if (MODE == kProp && neg) {
+        r1 = dadd(r1, v);
+    } else {
+        r0 = dadd(r0, v);
+    }
+}
+
+// Bit 31 of a term's fold word: the sign (kCanon, kProp) from the payload,
+// or the phase (kCanonSplit) from bit 0 of the sorted key.
+template <int MODE>
+__device__ __forceinline__ u32 fold_word(const SegCtx& C, u32 e, u64 key) {
+    if (MODE == kCanonSplit) return ((u32)key & 1u) << 31;
+    return C.pay[e];
 }
 
 template <int MODE>
 __device__ __forceinline__ u32 fold_close(double* segval, u8* segflag, i64 h, double r0,
                                           double r1, const FoldFilter& F) {
+    if (MODE == kCanonSplit) {
+        // segflag 0x10 | kept phase 0 | kept phase 1 << 1 (the filters are on)
+        const bool k0 = r0 != 0.0 && (F.cutoff <= 0.0 || fabs(r0) >= F.cutoff);
+        const bool k1 = r1 != 0.0 && (F.cutoff <= 0.0 || fabs(r1) >= F.cutoff);
+        F.seg2[h] = make_double2(r0, r1);
+        segflag[h] = (u8)(0x10u | (k0 ? 1u : 0u) | (k1 ? 2u : 0u));
+        return (k0 ? 1u : 0u) + (k1 ? 1u : 0u);
+    }
     const double v = MODE == kProp ? dadd(r0, -r1) : r0;
     segval[h] = v;
     bool keep = true;
@@ -669,7 +790,7 @@ __global__ void __launch_bounds__(32 * kFoldWarps)
     u32 cp = 0;
     if (w0 > 0) {
         ck = C.keys[w0 - 1];
-        cp = C.pay[w0 - 1];
+        cp = fold_word<MODE>(C, w0 - 1, ck);
     }
     u32 first = kNoHead;
     // 8 chunks of loads in flight per lane, then the head flags of those chunks
@@ -683,7 +804,7 @@ __global__ void __launch_bounds__(32 * kFoldWarps)
             const u32 i = (c0 + b) * 32 + lane;
             const bool valid = i < cnt;
             ke[b] = valid ? C.keys[w0 + i] : 0ull;
-            pe[b] = valid ? C.pay[w0 + i] : 0u;
+            pe[b] = valid ? fold_word<MODE>(C, w0 + i, ke[b]) : 0u;
             ve[b] = valid ? C.vals[w0 + i] : 0.0;
         }
 #pragma unroll
@@ -776,7 +897,7 @@ __global__ void __launch_bounds__(32 * kFoldWarps)
         } else {
             // extension: continue past the range, 32 terms at a time
             ck = C.keys[w1 - 1];
-            cp = C.pay[w1 - 1];
+            cp = fold_word<MODE>(C, w1 - 1, ck);
             for (int ext = 0;; ++ext) {
                 const u32 cb = w1 + (u32)ext * 32u;
                 if (cb >= C.n) {
@@ -793,7 +914,7 @@ __global__ void __launch_bounds__(32 * kFoldWarps)
                 const u32 e = cb + lane;
                 const bool valid = e < C.n;
                 const u64 ke = valid ? C.keys[e] : 0ull;
-                const u32 pe = valid ? C.pay[e] : 0u;
+                const u32 pe = valid ? fold_word<MODE>(C, e, ke) : 0u;
                 const double ve = valid ? C.vals[e] : 0.0;
                 u64 kp = __shfl_up_sync(0xffffffffu, ke, 1);
                 u32 pp = __shfl_up_sync(0xffffffffu, pe, 1);
@@ -932,7 +1053,8 @@ __device__ __forceinline__ void tree_sum(double* s0, double* s1, double a0, doub
     for (int st = kThreads / 2; st > 0; st >>= 1) {
         if ((int)threadIdx.x < st) {
             s0[threadIdx.x] = dadd(s0[threadIdx.x], s0[threadIdx.x + st]);
-            if (MODE == kProp) s1[threadIdx.x] = dadd(s1[threadIdx.x], s1[threadIdx.x + st]);
+            if (MODE == kProp || MODE == kCanonSplit)
+                s1[threadIdx.x] = dadd(s1[threadIdx.x], s1[threadIdx.x + st]);
         }
         __syncthreads();
     }
@@ -962,7 +1084,8 @@ __global__ void __launch_bounds__(kThreads)
 #pragma unroll
         for (int j = 0; j < kPer; ++j) {
             const u32 t = s + threadIdx.x + (u32)j * kThreads;
-            q[j] = t < e ? C.pay[t] : 0u;
+            q[j] = t >= e ? 0u
+                          : (MODE == kCanonSplit ? ((u32)C.keys[t] & 1u) << 31 : C.pay[t]);
             v[j] = t < e ? C.vals[t] : 0.0;
         }
         double a0 = 0.0, a1 = 0.0;
@@ -987,7 +1110,7 @@ __global__ void __launch_bounds__(kThreads)
             tree_sum<MODE>(s0, s1, b0, b1);
             if (threadIdx.x == 0) {
                 const u32 keep = fold_close<MODE>(segval, segflag, h, s0[0], s1[0], F);
-                if (F.on && keep) atomicAdd(&F.tile_kept[h / kETile], 1u);
+                if (F.on && keep) atomicAdd(&F.tile_kept[h / kETile], keep);
             }
         }
         __syncthreads();
@@ -1061,6 +1184,64 @@ __device__ __forceinline__ void emit_term(const Src& src, const KeyLayout& L, u6
     }
     out.f[o] = (u8)f;
     out.v[o] = v;
+}
+
+// kCanonSplit emit: a kept head writes its phase-0 term, then its phase-1
+// term (the canonical order: phase is the last key field), at the offsets
+// k_tile_scan gave its tile.
+template <int AS>
+__global__ void __launch_bounds__(kThreads)
+    k_emit_split(KeyLayout L, const u64* keys, const double2* seg2, const u8* segflag, u32 n,
+                 const u32* tile_off, SoAOut out, int* status) {
+    __shared__ u32 swarp[kWarps];
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const u32 tile = blockIdx.x;
+    const u32 wbase = tile * kETile + (u32)warp * (kEItems * 32);
+    u32 kb[kEItems];  // bit 0: phase-0 term kept, bit 1: phase-1 term kept
+#pragma unroll
+    for (int t = 0; t < kEItems; ++t) {
+        const u32 e = wbase + t * 32 + lane;
+        const u32 sf = e < n ? segflag[e] : 0u;
+        kb[t] = (sf & 0x10u) ? (sf & 3u) : 0u;
+    }
+    u32 wcount = 0;
+    u32 myoff[kEItems];
+#pragma unroll
+    for (int t = 0; t < kEItems; ++t) {
+        const u32 b0 = __ballot_sync(0xffffffffu, (kb[t] & 1u) != 0);
+        const u32 b1 = __ballot_sync(0xffffffffu, (kb[t] & 2u) != 0);
+        const u32 lt = lanemask_lt();
+        myoff[t] = wcount + __popc(b0 & lt) + __popc(b1 & lt);
+        wcount += __popc(b0) + __popc(b1);
+    }
+    u32 total;
+    const u32 wexcl = block_excl_scan(lane == 0 ? wcount : 0u, swarp, total);
+    const u32 base_o = tile_off[tile] + __shfl_sync(0xffffffffu, wexcl, 0);
+#pragma unroll
+    for (int t = 0; t < kEItems; ++t) {
+        if (!kb[t]) continue;
+        const u32 e = wbase + t * 32 + lane;
+        u64 xw[AS], zw[AS];
+        u32 fv;
+        unpack_key<AS>(L, keys[e], xw, zw, fv);
+        const double2 sv = seg2[e];
+        i64 o = (i64)base_o + myoff[t];
+        for (u32 ph = 0; ph < 2; ++ph) {
+            if (!((kb[t] >> ph) & 1u)) continue;
+            if (o >= out.capacity) {
+                raise_status(status, PL_ERR_CAPACITY);
+                break;
+            }
+#pragma unroll
+            for (int k = 0; k < AS; ++k) {
+                out.x[(i64)k * out.capacity + o] = xw[k];
+                out.z[(i64)k * out.capacity + o] = zw[k];
+            }
+            out.f[o] = (u8)ph;
+            out.v[o] = ph ? sv.y : sv.x;
+            ++o;
+        }
+    }
 }
 
 // Filters decided by the fold (segflag 1 = kept): each tile writes at the
@@ -1207,6 +1388,7 @@ struct Bufs {
     u64 *orm, *andm;
     i64* d_count;
     int* d_status;
+    size_t planes_bytes;
 };
 
 void carve_all(Carve& c, i64 n, int nch, Bufs& B) {
@@ -1220,6 +1402,7 @@ void carve_all(Carve& c, i64 n, int nch, Bufs& B) {
     B.pb = c.take<u32>(n);
     B.sv = c.take<double>(n);
     B.planes = c.take<u64>(nch > 1 ? (size_t)n * nch : 1);
+    B.planes_bytes = sizeof(u64) * (nch > 1 ? (size_t)n * nch : 1);
     B.hist = c.take<u32>(kMaxPasses * kRadix);
     B.lb = c.take<u32>((size_t)rtiles * kRadix);
     B.segflag = c.take<u8>(n + 16);
@@ -1293,6 +1476,54 @@ void build_layout(int as, int mode, const u64* orm, const u64* andm, KeyLayout& 
     P.npasses = np;
 }
 
+// Index-packed layout (kCanonSplit): the varying x / z bits sit above
+// ibits = ceil(log2 n) index bits, the flags stay out of the key, and the
+// digit passes cover only the x / z bits (8-bit digits at most).  Sorting
+// these words orders terms by (x, z) and, within equal (x, z), by index --
+// a stable sort by (x, z).  False when the word would exceed 64 bits or no
+// x / z bit varies.
+bool build_layout_split(int as, const u64* orm, const u64* andm, u32 n, KeyLayout& L,
+                        PassPlan& P, u64& imask) {
+    const int nf = 2 * as + 1;
+    std::memset(&L, 0, sizeof(L));
+    std::memset(&P, 0, sizeof(P));
+    int ibits = 1;
+    while (ibits < 32 && (1ull << ibits) < (u64)n) ++ibits;
+    int xz = 0;
+    for (int f = 0; f < 2 * as; ++f) {
+        const u64 var = orm[f] ^ andm[f];
+        L.cbits[f] = andm[f];
+        if (var == 0) continue;
+        const int lo = __builtin_ctzll(var), hi = 63 - __builtin_clzll(var);
+        L.lo[f] = lo;
+        L.width[f] = hi - lo + 1;
+        xz += L.width[f];
+    }
+    if (xz == 0 || xz + ibits > 64) return false;
+    int off = ibits;
+    for (int f = nf - 1; f >= 0; --f) {
+        L.off[f] = off;
+        off += L.width[f];
+    }
+    L.total_bits = off;
+    L.nchunks = 1;
+    L.seg_mask0 = ~1ull;  // bit 0 carries the phase once the last pass has run
+    const int passes = (xz + 7) / 8;
+    const int dw = (xz + passes - 1) / passes;
+    int np = 0;
+    for (int p = 0; p < passes; ++p) {
+        P.chunk[np] = 0;
+        P.shift[np] = ibits + p * dw;
+        P.bits[np] = std::min(dw, xz - p * dw);
+        ++np;
+    }
+    P.first[0] = 0;
+    P.first[1] = np;
+    P.npasses = np;
+    imask = (1ull << ibits) - 1ull;
+    return true;
+}
+
 // Segment sums: the warp fold, then the long runs (ends, piece offsets,
 // pieces with the last piece of each run closing it).
 template <int MODE>
@@ -1361,18 +1592,46 @@ int radix_pass(bool last, const u64* kin, const u32* vin, u64* kout, u32* vout, 
     const u32 tiles = (n + kThreads * ITEMS - 1) / (kThreads * ITEMS);
     const SoASrc<1> nosrc{nullptr, nullptr, nullptr, nullptr, 0};
     if (last) {
-        PL_CUDA_TRY(cudaFuncSetAttribute(k_radix_pass<Src, true, ITEMS>,
+        PL_CUDA_TRY(cudaFuncSetAttribute(k_radix_pass<Src, true, ITEMS, false>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)radix_smem(ITEMS)));
-        k_radix_pass<Src, true, ITEMS><<<tiles, kThreads, radix_smem(ITEMS), st>>>(
-            kin, vin, kout, vout, n, shift, bits, bstart, B.lb, ctr, B.d_status, src, B.sv),
+        k_radix_pass<Src, true, ITEMS, false><<<tiles, kThreads, radix_smem(ITEMS), st>>>(
+            kin, vin, kout, vout, n, shift, bits, bstart, B.lb, ctr, B.d_status, src, B.sv,
+            nullptr, 0ull),
             pl::note_launch();
     } else {
-        PL_CUDA_TRY(cudaFuncSetAttribute(k_radix_pass<SoASrc<1>, false, ITEMS>,
+        PL_CUDA_TRY(cudaFuncSetAttribute(k_radix_pass<SoASrc<1>, false, ITEMS, false>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)radix_smem(ITEMS)));
-        k_radix_pass<SoASrc<1>, false, ITEMS><<<tiles, kThreads, radix_smem(ITEMS), st>>>(
-            kin, vin, kout, vout, n, shift, bits, bstart, B.lb, ctr, B.d_status, nosrc, nullptr),
+        k_radix_pass<SoASrc<1>, false, ITEMS, false><<<tiles, kThreads, radix_smem(ITEMS), st>>>(
+            kin, vin, kout, vout, n, shift, bits, bstart, B.lb, ctr, B.d_status, nosrc, nullptr,
+            nullptr, 0ull),
+            pl::note_launch();
+    }
+    return PL_OK;
+}
+
+// Digit pass over index-packed keys (no payload).
+template <class Src, int ITEMS>
+int radix_pass_konly(bool last, const u64* kin, u64* kout, u32 n, int shift, int bits,
+                     const u32* bstart, Bufs& B, u32* ctr, const Src& src, const u8* phs,
+                     u64 imask, cudaStream_t st) {
+    const u32 tiles = (n + kThreads * ITEMS - 1) / (kThreads * ITEMS);
+    const size_t sm = radix_smem_konly(ITEMS);
+    if (last) {
+        PL_CUDA_TRY(cudaFuncSetAttribute(k_radix_pass<Src, true, ITEMS, true>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+        k_radix_pass<Src, true, ITEMS, true><<<tiles, kThreads, sm, st>>>(
+            kin, nullptr, kout, nullptr, n, shift, bits, bstart, B.lb, ctr, B.d_status, src, B.sv,
+            phs, imask),
+            pl::note_launch();
+    } else {
+        const SoASrc<1> nosrc{nullptr, nullptr, nullptr, nullptr, 0};
+        PL_CUDA_TRY(cudaFuncSetAttribute(k_radix_pass<SoASrc<1>, false, ITEMS, true>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+        k_radix_pass<SoASrc<1>, false, ITEMS, true><<<tiles, kThreads, sm, st>>>(
+            kin, nullptr, kout, nullptr, n, shift, bits, bstart, B.lb, ctr, B.d_status, nosrc,
+            nullptr, nullptr, imask),
             pl::note_launch();
     }
     return PL_OK;
@@ -1477,6 +1736,97 @@ int run_collate(const Src& src, u32 n, int mode, const KeyLayout& L, const PassP
     return PL_OK;
 }
 
+// canonicalize() on index-packed keys (layout from build_layout_split;
+// filters: zero and cutoff, no weight filter).
+template <int AS, class Src>
+int run_collate_split(const Src& src, u32 n, const KeyLayout& L, const PassPlan& P, u64 imask,
+                      const CollateArgs& a, const SoAOut& out, i64* out_count, Bufs& B,
+                      cudaStream_t st) {
+    const int items = radix_items();
+    const u32 rtiles = (n + kThreads * items - 1) / (kThreads * items);
+    const int nsm = sm_count();
+    // the chunk-plane buffer is unused with one chunk: phase bytes, then the
+    // (phase-0, phase-1) sums of the segments
+    u8* phs = reinterpret_cast<u8*>(B.planes);
+    double2* seg2 = reinterpret_cast<double2*>(reinterpret_cast<unsigned char*>(B.planes) + al(n));
+    PL_CUDA_TRY(cudaMemsetAsync(B.hist, 0, sizeof(u32) * kMaxPasses * kRadix, st));
+    PL_CUDA_TRY(cudaMemsetAsync(B.counters, 0, sizeof(u32) * (kMaxPasses + 8), st));
+    PL_CUDA_TRY(cudaMemsetAsync(B.d_status, 0, sizeof(int), st));
+    PL_CUDA_TRY(cudaMemsetAsync(B.d_count, 0, sizeof(i64), st));
+    const int gblocks = grid_for(n, 256, nsm * 8);
+    cudaEvent_t e0 = timed_begin(st);
+    const u32 derived = derive_histograms<AS>(src, L, P, B, st);
+    timed_end(e0, st, "k_xor_conv", 0ull);
+    const u32 count_mask = ~derived & ((1u << P.npasses) - 1u);
+    e0 = timed_begin(st);
+    k_pack_split<AS, Src><<<gblocks, 256, 0, st>>>(src, n, L, P, count_mask, B.ka, phs, B.hist),
+        pl::note_launch();
+    timed_end(e0, st, "k_pack", 9ull * n);
+    k_scan_buckets<<<P.npasses, kRadix, 0, st>>>(B.hist, 0), pl::note_launch();
+    u64 *kin = B.ka, *kout = B.kb;
+    for (int p = 0; p < P.npasses; ++p) {
+        PL_CUDA_TRY(cudaMemsetAsync(B.lb, 0, sizeof(u32) * (size_t)rtiles * kRadix, st));
+        cudaEvent_t ev0 = timed_begin(st);
+        const bool last = (p == P.npasses - 1);
+        const u32* bs = B.hist + (size_t)p * kRadix;
+        u32* ctr = B.counters + 8 + p;
+        int rc = PL_OK;
+        if (items == 16)
+            rc = radix_pass_konly<Src, 16>(last, kin, kout, n, P.shift[p], P.bits[p], bs, B, ctr,
+                                           src, phs, imask, st);
+        else if (items == 12)
+            rc = radix_pass_konly<Src, 12>(last, kin, kout, n, P.shift[p], P.bits[p], bs, B, ctr,
+                                           src, phs, imask, st);
+        else
+            rc = radix_pass_konly<Src, 8>(last, kin, kout, n, P.shift[p], P.bits[p], bs, B, ctr,
+                                          src, phs, imask, st);
+        if (rc) return rc;
+        // algorithmic bytes: read and write one u64 key per term (+ the phase
+        // byte read and the u64 coefficient written by the last pass)
+        timed_end(ev0, st, "k_radix_pass", 16ull * n + (last ? 9ull * n : 0ull));
+        std::swap(kin, kout);
+    }
+    SegCtx C{kin, nullptr, B.sv, B.planes, n, 1, L.seg_mask0, kCanon};
+    const u32 etiles = (n + kETile - 1) / kETile;
+    const FoldFilter F{1, a.cutoff, B.tile_kept, seg2};
+    PL_CUDA_TRY(cudaMemsetAsync(B.tile_kept, 0, sizeof(u32) * etiles, st));
+    e0 = timed_begin(st);
+    int rc = fold_segments<kCanonSplit>(C, B, F, nsm, st);
+    if (rc != PL_OK) return rc;
+    timed_end(e0, st, "k_fold", 16ull * n);
+    e0 = timed_begin(st);
+    k_tile_scan<<<1, 1024, 0, st>>>(B.tile_kept, etiles, B.tile_off, B.d_count),
+        pl::note_launch();
+    k_emit_split<AS><<<etiles, kThreads, 0, st>>>(L, kin, seg2, B.segflag, n, B.tile_off, out,
+                                                  B.d_status),
+        pl::note_launch();
+    timed_end(e0, st, "k_emit", 0ull);
+    PL_CUDA_TRY(cudaGetLastError());
+    i64 cnt = 0;
+    int dstat = 0;
+    PL_CUDA_TRY(cudaMemcpyAsync(&cnt, B.d_count, sizeof(i64), cudaMemcpyDeviceToHost, st));
+    PL_CUDA_TRY(cudaMemcpyAsync(&dstat, B.d_status, sizeof(int), cudaMemcpyDeviceToHost, st));
+    PL_CUDA_TRY(cudaStreamSynchronize(st));
+    *out_count = cnt;
+    if (dstat != 0) return record_status(dstat, "collate: device-side check");
+    return PL_OK;
+}
+
+// The index-packed path applies to canonicalize() without a weight filter
+// whenever the varying (x, z) bits and the index fit one word.
+template <int AS, class Src>
+bool try_split(const Src& src, u32 n, const u64* orm, const u64* andm, const CollateArgs& a,
+               const SoAOut& out, i64* out_count, Bufs& B, cudaStream_t st, int* rc) {
+    if (a.mode != kCanon || a.max_weight != ~0ull || tuning(PL_TUNE_INDEX_KEYS) < 0) return false;
+    if (B.planes_bytes < al(n) + sizeof(double2) * (size_t)n) return false;
+    KeyLayout L;
+    PassPlan P;
+    u64 imask = 0;
+    if (!build_layout_split(AS, orm, andm, n, L, P, imask)) return false;
+    *rc = run_collate_split<AS>(src, n, L, P, imask, a, out, out_count, B, st);
+    return true;
+}
+
 }  // namespace
 
 // ---------------------------------------------------------------------------
@@ -1526,10 +1876,12 @@ int collate_soa(int as, const SoAView& in, const SoAOut& out, const CollateArgs&
         PL_CUDA_TRY(cudaMemcpyAsync(hor, B.orm, 8 * kMaxFields, cudaMemcpyDeviceToHost, st));
         PL_CUDA_TRY(cudaMemcpyAsync(hand, B.andm, 8 * kMaxFields, cudaMemcpyDeviceToHost, st));
         PL_CUDA_TRY(cudaStreamSynchronize(st));
-        KeyLayout L;
-        PassPlan P;
-        build_layout(AS, a.mode, hor, hand, L, P);
-        rc = run_collate<AS>(src, n, a.mode, L, P, a, out, out_count, B, st);
+        if (!try_split<AS>(src, n, hor, hand, a, out, out_count, B, st, &rc)) {
+            KeyLayout L;
+            PassPlan P;
+            build_layout(AS, a.mode, hor, hand, L, P);
+            rc = run_collate<AS>(src, n, a.mode, L, P, a, out, out_count, B, st);
+        }
     });
     return rc;
 }
@@ -1582,13 +1934,15 @@ int multiply_collate(int as, const SoAView& lhs, const SoAView& rhs, const SoAOu
         }
         por[2 * AS] = a.mode == kCanon ? 1ull : 3ull;  // the phase (and sign) may vary
         pand[2 * AS] = 0;
-        KeyLayout L;
-        PassPlan P;
-        build_layout(AS, a.mode, por, pand, L, P);
         ProdSrc<AS> src{lhs.x, lhs.z, rhs.x,      rhs.z,      lhs.f,      rhs.f,
                         lhs.v, rhs.v, (u32)lhs.n, (u32)rhs.n, lhs.stride, rhs.stride,
                         FastDiv::make((u32)lhs.n)};
-        rc = run_collate<AS>(src, n, a.mode, L, P, a, out, out_count, B, st);
+        if (!try_split<AS>(src, n, por, pand, a, out, out_count, B, st, &rc)) {
+            KeyLayout L;
+            PassPlan P;
+            build_layout(AS, a.mode, por, pand, L, P);
+            rc = run_collate<AS>(src, n, a.mode, L, P, a, out, out_count, B, st);
+        }
     });
     return rc;
 }
