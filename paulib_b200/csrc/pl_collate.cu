@@ -441,28 +441,30 @@ __device__ __forceinline__ u32 block_excl_scan(u32 v, u32* s_warp, u32& total) {
     return wpre + inc - v;
 }
 
-// Decoupled look-back over per-tile counters (status | count words).
-// Publishes this tile's aggregate, walks predecessors four at a time (one
-// round trip per window), publishes the inclusive prefix and returns the
-// exclusive prefix.  Bounded.
-__device__ __forceinline__ u32 lookback(u32* lb, u32 tile, u32 stride, u32 cnt, int* status) {
-    if (tile == 0) {
-        st_volatile(lb, kFlagPre | cnt);
-        return 0;
-    }
+// Decoupled look-back over per-tile counters (status | count words), in two
+// halves so a tile can do other work between them: lb_publish posts this
+// tile's aggregate (tile 0: its inclusive prefix); lb_walk reads the
+// predecessors W at a time (one round trip per window), posts the inclusive
+// prefix and returns the exclusive prefix.  Bounded.
+__device__ __forceinline__ void lb_publish(u32* lb, u32 tile, u32 stride, u32 cnt) {
+    st_volatile(lb + (size_t)tile * stride, (tile == 0 ? kFlagPre : kFlagAgg) | cnt);
+}
+
+template <int W = 4>
+__device__ __forceinline__ u32 lb_walk(u32* lb, u32 tile, u32 stride, u32 cnt, int* status) {
+    if (tile == 0) return 0;
     u32* mine = lb + (size_t)tile * stride;
-    st_volatile(mine, kFlagAgg | cnt);
     u32 excl = 0;
     i64 t = (i64)tile - 1;
     u32 spins = 0;
     while (t >= 0) {
-        u32 w[4];
+        u32 w[W];
 #pragma unroll
-        for (int k = 0; k < 4; ++k)
+        for (int k = 0; k < W; ++k)
             w[k] = t - k >= 0 ? ld_volatile(lb + (size_t)(t - k) * stride) : kFlagPre;
         int k = 0;
         bool done = false;
-        for (; k < 4; ++k) {
+        for (; k < W; ++k) {
             const u32 fl = w[k] >> 30;
             if (fl == 0) break;
             excl += w[k] & kCountMask;
@@ -485,13 +487,21 @@ __device__ __forceinline__ u32 lookback(u32* lb, u32 tile, u32 stride, u32 cnt, 
     return excl;
 }
 
+__device__ __forceinline__ u32 lookback(u32* lb, u32 tile, u32 stride, u32 cnt, int* status) {
+    lb_publish(lb, tile, stride, cnt);
+    return lb_walk<4>(lb, tile, stride, cnt, status);
+}
+
 // ---------------------------------------------------------------------------
 // 3. One onesweep digit pass: stable scatter of (key, payload) by digit
 //    bits [shift, shift+bits).
 // ---------------------------------------------------------------------------
+// whist[w][d]: per warp w, its digit-d count while ranking, then the tile
+// position of its first digit-d key (block offset of d + earlier warps'
+// counts).  gofs[d]: global position of the tile's first digit-d key minus
+// its tile position, so a key at tile position p goes to gofs[d] + p.
 struct RadixSmem {
     u32 whist[kWarps * kRadix];
-    u32 bloc[kRadix];
     u32 gofs[kRadix];
     u32 swarp[kWarps];
     u32 tile;
@@ -524,7 +534,7 @@ __global__ void __launch_bounds__(kThreads, KONLY ? (ITEMS <= 12 ? 4 : 3)
 
     u64 keys[ITEMS];
     u32 vals[KONLY ? 1 : ITEMS];
-    u32 rank[ITEMS];
+    u32 rank[(ITEMS + 1) / 2];  // two 16-bit in-warp ranks per word (a warp ranks < 2^16 keys)
     const u32 wbase = base + (u32)warp * (ITEMS * 32);
 #pragma unroll
     for (int t = 0; t < ITEMS; ++t) {
@@ -545,7 +555,8 @@ __global__ void __launch_bounds__(kThreads, KONLY ? (ITEMS <= 12 ? 4 : 3)
             wh[d] = before + __popc(peers);
         }
         before = __shfl_sync(0xffffffffu, before, leader);
-        rank[t] = before + __popc(peers & lanemask_lt());
+        const u32 r = before + __popc(peers & lanemask_lt());
+        rank[t / 2] = (t & 1) ? (rank[t / 2] | (r << 16)) : r;
         __syncwarp();
     }
     __syncthreads();
@@ -560,19 +571,23 @@ __global__ void __launch_bounds__(kThreads, KONLY ? (ITEMS <= 12 ? 4 : 3)
     }
     u32 total;
     const u32 bl = block_excl_scan(run, S.swarp, total);
-    S.bloc[d] = bl;
-    const u32 excl = lookback(lb + d, tile, kRadix, run, status);
-    S.gofs[d] = bstart[d] + excl;
+#pragma unroll
+    for (int w = 0; w < kWarps; ++w) S.whist[w * kRadix + d] += bl;
+    // the aggregate goes out first; the scatter into shared memory needs only
+    // tile positions and runs while the predecessors' prefixes arrive
+    lb_publish(lb + d, tile, kRadix, run);
     __syncthreads();
 #pragma unroll
     for (int t = 0; t < ITEMS; ++t) {
         if (wbase + t * 32 + lane < n) {
             const u32 dd = (u32)(keys[t] >> shift) & dmask;
-            const u32 pos = S.bloc[dd] + S.whist[warp * kRadix + dd] + rank[t];
+            const u32 pos = S.whist[warp * kRadix + dd] + ((rank[t / 2] >> ((t & 1) * 16)) & 0xffffu);
             skeys[pos] = keys[t];
             if constexpr (!KONLY) svals[pos] = vals[t];
         }
     }
+    const u32 excl = lb_walk<4>(lb + d, tile, kRadix, run, status);
+    S.gofs[d] = bstart[d] + excl - bl;  // modulo 2^32; gofs[d] + p >= 0 for p >= bl
     __syncthreads();
     const u32 tile_n = min((u32)(kThreads * ITEMS), n - base);
     if constexpr (KONLY && LAST) {
@@ -595,7 +610,7 @@ __global__ void __launch_bounds__(kThreads, KONLY ? (ITEMS <= 12 ? 4 : 3)
                     const u32 dd = (u32)(k >> shift) & dmask;
                     const u32 idx = (u32)(k & imask);
                     kk[b] = k;
-                    gg[b] = S.gofs[dd] + (p - S.bloc[dd]);
+                    gg[b] = S.gofs[dd] + p;
                     if (idx < n) {
                         ph[b] = phs[idx];
                         vv[b] = src.value(idx);
@@ -616,10 +631,35 @@ __global__ void __launch_bounds__(kThreads, KONLY ? (ITEMS <= 12 ? 4 : 3)
         }
         return;
     }
+    if (tile_n == (u32)(kThreads * ITEMS) && (KONLY || !LAST)) {
+        // full tile: half of a thread's keys and offsets at a time are loaded
+        // before their stores
+        constexpr int kH = ITEMS / 2;
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            u64 kk[kH];
+            u32 gg[kH];
+#pragma unroll
+            for (int t = 0; t < kH; ++t) kk[t] = skeys[tid + (h * kH + t) * kThreads];
+#pragma unroll
+            for (int t = 0; t < kH; ++t)
+                gg[t] = S.gofs[(u32)(kk[t] >> shift) & dmask] + (u32)(tid + (h * kH + t) * kThreads);
+#pragma unroll
+            for (int t = 0; t < kH; ++t) {
+                if (gg[t] >= n) {
+                    raise_status(status, PL_ERR_INTERNAL);
+                    continue;
+                }
+                kout[gg[t]] = kk[t];
+                if constexpr (!KONLY) vout[gg[t]] = svals[tid + (h * kH + t) * kThreads];
+            }
+        }
+        return;
+    }
     for (u32 p = tid; p < tile_n; p += kThreads) {
         const u64 k = skeys[p];
         const u32 dd = (u32)(k >> shift) & dmask;
-        const u32 g = S.gofs[dd] + (p - S.bloc[dd]);
+        const u32 g = S.gofs[dd] + p;
         if (g >= n) {
             raise_status(status, PL_ERR_INTERNAL);
         } else if constexpr (KONLY) {
@@ -1586,23 +1626,27 @@ int radix_items() {
     return v == 12 || v == 16 ? (int)v : 8;
 }
 
+// Dynamic shared memory of a digit pass.  (The default carveout is kept:
+// the largest one admits more CTAs per SM but leaves the L1 too small for
+// the last pass's gathers, and measured slower.)
+template <class K>
+cudaError_t radix_attrs(K* kernel, int smem) {
+    return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+}
+
 template <class Src, int ITEMS>
 int radix_pass(bool last, const u64* kin, const u32* vin, u64* kout, u32* vout, u32 n, int shift,
                int bits, const u32* bstart, Bufs& B, u32* ctr, const Src& src, cudaStream_t st) {
     const u32 tiles = (n + kThreads * ITEMS - 1) / (kThreads * ITEMS);
     const SoASrc<1> nosrc{nullptr, nullptr, nullptr, nullptr, 0};
     if (last) {
-        PL_CUDA_TRY(cudaFuncSetAttribute(k_radix_pass<Src, true, ITEMS, false>,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)radix_smem(ITEMS)));
+        PL_CUDA_TRY(radix_attrs(k_radix_pass<Src, true, ITEMS, false>, (int)radix_smem(ITEMS)));
         k_radix_pass<Src, true, ITEMS, false><<<tiles, kThreads, radix_smem(ITEMS), st>>>(
             kin, vin, kout, vout, n, shift, bits, bstart, B.lb, ctr, B.d_status, src, B.sv,
             nullptr, 0ull),
             pl::note_launch();
     } else {
-        PL_CUDA_TRY(cudaFuncSetAttribute(k_radix_pass<SoASrc<1>, false, ITEMS, false>,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)radix_smem(ITEMS)));
+        PL_CUDA_TRY(radix_attrs(k_radix_pass<SoASrc<1>, false, ITEMS, false>, (int)radix_smem(ITEMS)));
         k_radix_pass<SoASrc<1>, false, ITEMS, false><<<tiles, kThreads, radix_smem(ITEMS), st>>>(
             kin, vin, kout, vout, n, shift, bits, bstart, B.lb, ctr, B.d_status, nosrc, nullptr,
             nullptr, 0ull),
@@ -1619,16 +1663,14 @@ int radix_pass_konly(bool last, const u64* kin, u64* kout, u32 n, int shift, int
     const u32 tiles = (n + kThreads * ITEMS - 1) / (kThreads * ITEMS);
     const size_t sm = radix_smem_konly(ITEMS);
     if (last) {
-        PL_CUDA_TRY(cudaFuncSetAttribute(k_radix_pass<Src, true, ITEMS, true>,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+        PL_CUDA_TRY(radix_attrs(k_radix_pass<Src, true, ITEMS, true>, (int)sm));
         k_radix_pass<Src, true, ITEMS, true><<<tiles, kThreads, sm, st>>>(
             kin, nullptr, kout, nullptr, n, shift, bits, bstart, B.lb, ctr, B.d_status, src, B.sv,
             phs, imask),
             pl::note_launch();
     } else {
         const SoASrc<1> nosrc{nullptr, nullptr, nullptr, nullptr, 0};
-        PL_CUDA_TRY(cudaFuncSetAttribute(k_radix_pass<SoASrc<1>, false, ITEMS, true>,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+        PL_CUDA_TRY(radix_attrs(k_radix_pass<SoASrc<1>, false, ITEMS, true>, (int)sm));
         k_radix_pass<SoASrc<1>, false, ITEMS, true><<<tiles, kThreads, sm, st>>>(
             kin, nullptr, kout, nullptr, n, shift, bits, bstart, B.lb, ctr, B.d_status, nosrc,
             nullptr, nullptr, imask),
