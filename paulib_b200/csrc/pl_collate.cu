@@ -1458,8 +1458,8 @@ void carve_all(Carve& c, i64 n, int nch, Bufs& B) {
     B.tile_off = c.take<u32>(etiles);
     B.lb_emit = c.take<u32>(etiles);
     B.counters = c.take<u32>(128 + 16 * kRadix);
-    B.orm = c.take<u64>(kMaxFields);
-    B.andm = c.take<u64>(kMaxFields);
+    B.orm = c.take<u64>(2 * kMaxFields);   // one set per operand of a product
+    B.andm = c.take<u64>(2 * kMaxFields);
     B.d_count = c.take<i64>(1);
     B.d_status = c.take<int>(1);
 }
@@ -1907,11 +1907,8 @@ int collate_soa(int as, const SoAView& in, const SoAOut& out, const CollateArgs&
     int rc = PL_OK;
     PL_DISPATCH_AS(as, {
         SoASrc<AS> src{in.x, in.z, in.f, in.v, in.stride};
-        std::vector<u64> init_or(kMaxFields, 0ull), init_and(kMaxFields, ~0ull);
-        PL_CUDA_TRY(cudaMemcpyAsync(B.orm, init_or.data(), 8 * kMaxFields,
-                                    cudaMemcpyHostToDevice, st));
-        PL_CUDA_TRY(cudaMemcpyAsync(B.andm, init_and.data(), 8 * kMaxFields,
-                                    cudaMemcpyHostToDevice, st));
+        PL_CUDA_TRY(cudaMemsetAsync(B.orm, 0, 8 * kMaxFields, st));
+        PL_CUDA_TRY(cudaMemsetAsync(B.andm, 0xff, 8 * kMaxFields, st));
         k_masks<AS><<<grid_for(n, 256, sm_count() * 4), 256, 0, st>>>(src, n, a.mode, B.orm,
                                                                      B.andm), pl::note_launch();
         u64 hor[kMaxFields], hand[kMaxFields];
@@ -1953,22 +1950,19 @@ int multiply_collate(int as, const SoAView& lhs, const SoAView& rhs, const SoAOu
         // Varying bits of a product lie inside OR(lhs) | OR(rhs) word by word;
         // the operand masks give a conservative layout without touching the
         // n*m products.
-        std::vector<u64> init_or(kMaxFields, 0ull), init_and(kMaxFields, ~0ull);
-        u64 hor[2][kMaxFields], hand[2][kMaxFields];
+        // both operands' masks, one read-back
+        u64 hor[2][kMaxFields];
         const SoAView* ops[2] = {&lhs, &rhs};
+        PL_CUDA_TRY(cudaMemsetAsync(B.orm, 0, 8 * 2 * kMaxFields, st));
+        PL_CUDA_TRY(cudaMemsetAsync(B.andm, 0xff, 8 * 2 * kMaxFields, st));
         for (int w = 0; w < 2; ++w) {
             SoASrc<AS> s{ops[w]->x, ops[w]->z, ops[w]->f, ops[w]->v, ops[w]->stride};
-            PL_CUDA_TRY(cudaMemcpyAsync(B.orm, init_or.data(), 8 * kMaxFields,
-                                        cudaMemcpyHostToDevice, st));
-            PL_CUDA_TRY(cudaMemcpyAsync(B.andm, init_and.data(), 8 * kMaxFields,
-                                        cudaMemcpyHostToDevice, st));
             k_masks<AS><<<grid_for(ops[w]->n, 256, sm_count() * 4), 256, 0, st>>>(
-                s, (u32)ops[w]->n, a.mode, B.orm, B.andm), pl::note_launch();
-            PL_CUDA_TRY(cudaMemcpyAsync(hor[w], B.orm, 8 * kMaxFields, cudaMemcpyDeviceToHost, st));
-            PL_CUDA_TRY(
-                cudaMemcpyAsync(hand[w], B.andm, 8 * kMaxFields, cudaMemcpyDeviceToHost, st));
-            PL_CUDA_TRY(cudaStreamSynchronize(st));
+                s, (u32)ops[w]->n, a.mode, B.orm + w * kMaxFields, B.andm + w * kMaxFields),
+                pl::note_launch();
         }
+        PL_CUDA_TRY(cudaMemcpyAsync(hor, B.orm, 8 * 2 * kMaxFields, cudaMemcpyDeviceToHost, st));
+        PL_CUDA_TRY(cudaStreamSynchronize(st));
         u64 por[kMaxFields], pand[kMaxFields];
         for (int f = 0; f < 2 * AS; ++f) {
             por[f] = hor[0][f] | hor[1][f];
