@@ -131,6 +131,15 @@ __device__ __forceinline__ u32 out_flags(u32 fv, int mode) {
 // ---------------------------------------------------------------------------
 // Term sources: where keys and values of the (virtual) input come from.
 // ---------------------------------------------------------------------------
+
+// Phase / sign bit planes of index-packed keys: word w holds, for terms
+// 32w .. 32w+31, the imaginary bits (x) and the sign bits (y); n/4 bytes in
+// all, small enough to stay in L2 for the gathers of the last digit pass.
+__device__ __forceinline__ u32 phase_bits(const uint2* phs, u32 i) {
+    const uint2 w = phs[i >> 5];
+    const u32 b = i & 31u;
+    return ((w.x >> b) & 1u) | (((w.y >> b) & 1u) << 1);
+}
 template <int AS>
 struct SoASrc {
     const u64* x;
@@ -147,6 +156,13 @@ struct SoASrc {
         fl = __ldg(f + i);
     }
     __device__ __forceinline__ double value(u32 i) const { return __ldg(v + i); }
+    // Index-packed keys: the phase / sign bits (flags & 3) of term i come from
+    // the bit planes k_pack_split stored, the coefficient from the source.
+    __device__ __forceinline__ void flags_value(u32 i, const uint2* phs, u32& fl,
+                                                double& val) const {
+        fl = phase_bits(phs, i);
+        val = __ldg(v + i);
+    }
 };
 
 // Division by a loop-invariant u32 d via a 32-bit magic multiplier
@@ -202,6 +218,13 @@ struct ProdSrc {
         u32 i, j;
         split(p, i, j);
         return dmul(__ldg(av + j), __ldg(bv + i));
+    }
+    // Index-packed keys: the product's phase / sign bits from the bit planes
+    // k_pack_split stored, its coefficient from the operands.
+    __device__ __forceinline__ void flags_value(u32 p, const uint2* phs, u32& fl,
+                                                double& val) const {
+        fl = phase_bits(phs, p);
+        val = value(p);
     }
 };
 
@@ -291,7 +314,7 @@ __global__ void __launch_bounds__(256) k_pack(Src src, u32 n, int mode, KeyLayou
 // the digit histograms of the passes not derived from operand histograms.
 template <int AS, class Src>
 __global__ void __launch_bounds__(256) k_pack_split(Src src, u32 n, KeyLayout L, PassPlan P,
-                                                    u32 count_mask, u64* keys, u8* phs,
+                                                    u32 count_mask, u64* keys, uint2* phs,
                                                     u32* hist) {
     __shared__ u32 sh[8 * kRadix];
     const int np = P.npasses;
@@ -303,13 +326,17 @@ __global__ void __launch_bounds__(256) k_pack_split(Src src, u32 n, KeyLayout L,
         const u32 i = w0 + lane;
         const bool valid = i < n;
         u64 k0 = 0;
+        u32 fl = 0;
         if (valid) {
             u64 xw[AS], zw[AS];
-            u32 fl;
             src.key(i, xw, zw, fl);
             k0 = pack_chunk<AS>(L, xw, zw, 0u, 0) | (u64)i;
             keys[i] = k0;
-            phs[i] = (u8)(fl & 3u);
+        }
+        {
+            const u32 im = __ballot_sync(0xffffffffu, valid && (fl & 1u));
+            const u32 sg = __ballot_sync(0xffffffffu, valid && (fl & 2u));
+            if (lane == 0) phs[w0 >> 5] = make_uint2(im, sg);
         }
         if (!count_mask) continue;
         for (int p = 0; p < np; ++p) {
@@ -519,7 +546,7 @@ __global__ void __launch_bounds__(kThreads, KONLY ? (ITEMS <= 12 ? 4 : 3)
     k_radix_pass(const u64* __restrict__ kin, const u32* __restrict__ vin, u64* __restrict__ kout,
                  u32* __restrict__ vout, u32 n, int shift, int bits,
                  const u32* __restrict__ bstart, u32* lb, u32* tile_ctr, int* status, Src src,
-                 double* __restrict__ val_out, const u8* __restrict__ phs, u64 imask) {
+                 double* __restrict__ val_out, const uint2* __restrict__ phs, u64 imask) {
     extern __shared__ __align__(16) unsigned char dsm[];
     u64* skeys = reinterpret_cast<u64*>(dsm);
     u32* svals = reinterpret_cast<u32*>(dsm + sizeof(u64) * (kThreads * ITEMS));
@@ -612,8 +639,7 @@ __global__ void __launch_bounds__(kThreads, KONLY ? (ITEMS <= 12 ? 4 : 3)
                     kk[b] = k;
                     gg[b] = S.gofs[dd] + p;
                     if (idx < n) {
-                        ph[b] = phs[idx];
-                        vv[b] = src.value(idx);
+                        src.flags_value(idx, phs, ph[b], vv[b]);
                     } else {
                         gg[b] = n;  // reported below
                     }
@@ -1658,7 +1684,7 @@ int radix_pass(bool last, const u64* kin, const u32* vin, u64* kout, u32* vout, 
 // Digit pass over index-packed keys (no payload).
 template <class Src, int ITEMS>
 int radix_pass_konly(bool last, const u64* kin, u64* kout, u32 n, int shift, int bits,
-                     const u32* bstart, Bufs& B, u32* ctr, const Src& src, const u8* phs,
+                     const u32* bstart, Bufs& B, u32* ctr, const Src& src, const uint2* phs,
                      u64 imask, cudaStream_t st) {
     const u32 tiles = (n + kThreads * ITEMS - 1) / (kThreads * ITEMS);
     const size_t sm = radix_smem_konly(ITEMS);
@@ -1787,9 +1813,9 @@ int run_collate_split(const Src& src, u32 n, const KeyLayout& L, const PassPlan&
     const int items = radix_items();
     const u32 rtiles = (n + kThreads * items - 1) / (kThreads * items);
     const int nsm = sm_count();
-    // the chunk-plane buffer is unused with one chunk: phase bytes, then the
-    // (phase-0, phase-1) sums of the segments
-    u8* phs = reinterpret_cast<u8*>(B.planes);
+    // the chunk-plane buffer is unused with one chunk: phase / sign bit planes,
+    // then the (phase-0, phase-1) sums of the segments
+    uint2* phs = reinterpret_cast<uint2*>(B.planes);
     double2* seg2 = reinterpret_cast<double2*>(reinterpret_cast<unsigned char*>(B.planes) + al(n));
     PL_CUDA_TRY(cudaMemsetAsync(B.hist, 0, sizeof(u32) * kMaxPasses * kRadix, st));
     PL_CUDA_TRY(cudaMemsetAsync(B.counters, 0, sizeof(u32) * (kMaxPasses + 8), st));
@@ -1803,7 +1829,7 @@ int run_collate_split(const Src& src, u32 n, const KeyLayout& L, const PassPlan&
     e0 = timed_begin(st);
     k_pack_split<AS, Src><<<gblocks, 256, 0, st>>>(src, n, L, P, count_mask, B.ka, phs, B.hist),
         pl::note_launch();
-    timed_end(e0, st, "k_pack", 9ull * n);
+    timed_end(e0, st, "k_pack", 8ull * n + n / 4);
     k_scan_buckets<<<P.npasses, kRadix, 0, st>>>(B.hist, 0), pl::note_launch();
     u64 *kin = B.ka, *kout = B.kb;
     for (int p = 0; p < P.npasses; ++p) {
@@ -1823,9 +1849,9 @@ int run_collate_split(const Src& src, u32 n, const KeyLayout& L, const PassPlan&
             rc = radix_pass_konly<Src, 8>(last, kin, kout, n, P.shift[p], P.bits[p], bs, B, ctr,
                                           src, phs, imask, st);
         if (rc) return rc;
-        // algorithmic bytes: read and write one u64 key per term (+ the phase
-        // byte read and the u64 coefficient written by the last pass)
-        timed_end(ev0, st, "k_radix_pass", 16ull * n + (last ? 9ull * n : 0ull));
+        // algorithmic bytes: read and write one u64 key per term (+ the two
+        // phase / sign bits read and the u64 coefficient written by the last pass)
+        timed_end(ev0, st, "k_radix_pass", 16ull * n + (last ? 8ull * n + n / 4 : 0ull));
         std::swap(kin, kout);
     }
     SegCtx C{kin, nullptr, B.sv, B.planes, n, 1, L.seg_mask0, kCanon};
