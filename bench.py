@@ -324,10 +324,13 @@ def run_product_collate(args, rank, local, ws):
     per_launch_ms = timed_ms / max(timed_n, 1)
     per_launch_bytes = timed_bytes / max(timed_n, 1)
     achieved = per_launch_bytes / (per_launch_ms / 1e3) / 1e9
+    # DRAM bytes per launch from the committed ncu capture of this workload,
+    # scaled by this run's algorithmic bytes per launch over the captured one
     prof = profile_traffic("radix_pass_product_collate")
     traffic = None
-    if prof and prof.get("bytes_per_term"):
-        traffic = prof["bytes_per_term"] * (per_launch_bytes / 24.0)
+    if prof and prof.get("dram_bytes_per_launch") and prof.get("algorithmic_bytes_per_launch"):
+        traffic = prof["dram_bytes_per_launch"] * (per_launch_bytes /
+                                                   prof["algorithmic_bytes_per_launch"])
     bits = 41
     pipe_bytes = b_canon(total, n_out, bits)
     pipe_gbs = pipe_bytes / (ms_per_step / 1e3) / 1e9

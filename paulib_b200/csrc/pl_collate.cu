@@ -351,6 +351,61 @@ __global__ void __launch_bounds__(256) k_pack_split(Src src, u32 n, KeyLayout L,
         if (sh[i]) atomicAdd(&hist[i], sh[i]);
 }
 
+// Pack of a product's index-packed keys when every digit histogram comes
+// from the operands (no counting): one block row per rhs term i (its words
+// held in registers), lhs terms j across the threads.  Packing is linear
+// over XOR (x = ax ^ bx, z = az ^ bz), so the packed key is the XOR of the
+// operands' packed keys.  Needs n % 32 == 0 so each warp's 32 products are
+// one bit-plane word.
+constexpr int kPackPerThread = 8;
+template <int AS>
+__global__ void __launch_bounds__(256) k_pack_split_prod(ProdSrc<AS> src, KeyLayout L, u64* keys,
+                                                         uint2* phs) {
+    const u32 i = blockIdx.y;
+    const u32 j = blockIdx.x * blockDim.x * kPackPerThread + threadIdx.x;
+    u64 bxw[AS], bzw[AS];
+#pragma unroll
+    for (int k = 0; k < AS; ++k) {
+        bxw[k] = __ldg(src.bx + (i64)k * src.sb + i);
+        bzw[k] = __ldg(src.bz + (i64)k * src.sb + i);
+    }
+    const u64 kb = pack_chunk<AS>(L, bxw, bzw, 0u, 0);
+    const u32 bfl = __ldg(src.bf + i);
+#pragma unroll
+    for (int r = 0; r < kPackPerThread; ++r) {
+        const u32 jj = j + (u32)r * blockDim.x;
+        if (jj >= src.n) break;  // whole warps: n % 32 == 0
+        u64 axw[AS], azw[AS];
+        PhaseAcc acc;
+#pragma unroll
+        for (int k = 0; k < AS; ++k) {
+            axw[k] = __ldg(src.ax + (i64)k * src.sa + jj);
+            azw[k] = __ldg(src.az + (i64)k * src.sa + jj);
+            acc.step(axw[k], azw[k], bxw[k], bzw[k]);
+        }
+        const u32 fl = acc.phase(__ldg(src.af + jj), bfl);
+        const u32 p = i * src.n + jj;
+        keys[p] = (pack_chunk<AS>(L, axw, azw, 0u, 0) ^ kb) | (u64)p;
+        const u32 im = __ballot_sync(0xffffffffu, (fl & 1u) != 0);
+        const u32 sg = __ballot_sync(0xffffffffu, (fl & 2u) != 0);
+        if ((threadIdx.x & 31) == 0) phs[p >> 5] = make_uint2(im, sg);
+    }
+}
+
+// Generic pack unless the product fast path applies.
+template <int AS>
+bool pack_split_fast(const SoASrc<AS>&, u32, const KeyLayout&, u32, u64*, uint2*, cudaStream_t) {
+    return false;
+}
+template <int AS>
+bool pack_split_fast(const ProdSrc<AS>& src, u32, const KeyLayout& L, u32 count_mask, u64* keys,
+                     uint2* phs, cudaStream_t st) {
+    if (count_mask != 0 || src.n % 32 != 0 || src.m > 65535u) return false;
+    const dim3 grid((src.n + 256 * kPackPerThread - 1) / (256 * kPackPerThread), src.m);
+    k_pack_split_prod<AS><<<grid, 256, 0, st>>>(src, L, keys, phs), pl::note_launch();
+    return true;
+}
+
 // Digit histograms of the operands of a product.  For a digit made only of
 // x / z bits, the product's digit is the XOR of the operands' digits
 // (x = ax ^ bx, z = az ^ bz), so the histogram over all n*m products is the
@@ -1827,8 +1882,9 @@ int run_collate_split(const Src& src, u32 n, const KeyLayout& L, const PassPlan&
     timed_end(e0, st, "k_xor_conv", 0ull);
     const u32 count_mask = ~derived & ((1u << P.npasses) - 1u);
     e0 = timed_begin(st);
-    k_pack_split<AS, Src><<<gblocks, 256, 0, st>>>(src, n, L, P, count_mask, B.ka, phs, B.hist),
-        pl::note_launch();
+    if (!pack_split_fast<AS>(src, n, L, count_mask, B.ka, phs, st))
+        k_pack_split<AS, Src><<<gblocks, 256, 0, st>>>(src, n, L, P, count_mask, B.ka, phs,
+                                                       B.hist), pl::note_launch();
     timed_end(e0, st, "k_pack", 8ull * n + n / 4);
     k_scan_buckets<<<P.npasses, kRadix, 0, st>>>(B.hist, 0), pl::note_launch();
     u64 *kin = B.ka, *kout = B.kb;
