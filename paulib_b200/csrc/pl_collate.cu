@@ -807,9 +807,14 @@ constexpr int kCanonSplit = 3;
 constexpr int kFoldWarps = 4;
 constexpr int kLaneSpan = 32;
 constexpr u32 kFoldSpan = 32u * kLaneSpan;  // 1024 terms per warp
-constexpr u32 kFoldSlots = 33u * 32u;       // lane spans padded to 33 slots (no bank conflicts)
+constexpr u32 kLook = 64;                   // terms after the range staged as well
+constexpr u32 kLookSlot = 33u * 32u;        // lane spans padded to 33 slots (no bank conflicts)
+constexpr u32 kFoldSlots = kLookSlot + kLook;
 constexpr int kExtChunks = 32;              // at most 1024 more
-constexpr size_t kFoldWarpSmem = kFoldSlots * (8 + 1);  // value, head | sign << 1
+constexpr u32 kFoldChunks = 32u + kLook / 32u;
+// per warp: the staged values, then per 32-term chunk a word of head bits and
+// a word of sign bits (chunk c < 32 is lane c's span)
+constexpr size_t kFoldWarpSmem = kFoldSlots * 8 + kFoldChunks * 8;
 constexpr size_t kFoldSmem = ((kFoldWarpSmem + 15) & ~size_t(15)) * kFoldWarps;
 constexpr u32 kNoHead = 0xffffffffu;
 constexpr u32 kPiece = 4096;  // terms per partial sum of a long run
@@ -893,7 +898,7 @@ __device__ __forceinline__ u32 fold_close(double* segval, u8* segflag, i64 h, do
 }
 
 template <int MODE>
-__global__ void __launch_bounds__(32 * kFoldWarps)
+__global__ void __launch_bounds__(32 * kFoldWarps, 5)
     k_fold(SegCtx C, double* segval, u8* segflag, u32* wfirst, u32* long_list, u32* counters,
            FoldFilter F) {
     extern __shared__ __align__(16) unsigned char fsm[];
@@ -905,7 +910,8 @@ __global__ void __launch_bounds__(32 * kFoldWarps)
     const u32 cnt = w1 - w0;
     unsigned char* base = fsm + ((kFoldWarpSmem + 15) & ~size_t(15)) * warp;
     double* sv = reinterpret_cast<double*>(base);
-    u8* sh = base + 8 * kFoldSlots;
+    u32* hbw = reinterpret_cast<u32*>(base + 8 * kFoldSlots);
+    u32* nbw = hbw + kFoldChunks;
     // ---- staging: coalesced loads, head flags, non-head segflag = 0
     u64 ck = 0;
     u32 cp = 0;
@@ -914,7 +920,8 @@ __global__ void __launch_bounds__(32 * kFoldWarps)
         cp = fold_word<MODE>(C, w0 - 1, ck);
     }
     u32 first = kNoHead;
-    // 8 chunks of loads in flight per lane, then the head flags of those chunks
+    // kBatch chunks of loads in flight per lane, then the head flags of those
+    // chunks; per chunk, a word of head bits and a word of sign bits
     constexpr int kBatch = 8;
     for (u32 c0 = 0; c0 * 32 < cnt; c0 += kBatch) {
         u64 ke[kBatch];
@@ -939,17 +946,61 @@ __global__ void __launch_bounds__(32 * kFoldWarps)
                 kp = ck;
                 pp = cp;
             }
-            bool head = false;
+            bool head = false, neg = false;
             if (i < cnt) {
                 head = (e == 0) || !lane_same_key(C, e, ke[b], kp, pe[b], pp);
-                const u32 neg = pe[b] >> 31;
-                const u32 slot = c * 33 + lane;
-                sh[slot] = (u8)((head ? 1u : 0u) | (neg << 1));
-                sv[slot] = (MODE == kCanon && neg) ? -ve[b] : ve[b];
+                neg = (pe[b] >> 31) != 0;
+                sv[c * 33 + lane] = (MODE == kCanon && neg) ? -ve[b] : ve[b];
                 if (!head) segflag[e] = 0;
             }
             const u32 hb = __ballot_sync(0xffffffffu, head);
+            const u32 nb = __ballot_sync(0xffffffffu, neg);
+            if (lane == 0 && c < 32) {
+                hbw[c] = hb;
+                nbw[c] = nb;
+            }
             if (first == kNoHead && hb) first = c * 32 + (u32)(__ffs(hb) - 1);
+            ck = __shfl_sync(0xffffffffu, ke[b], 31);
+            cp = __shfl_sync(0xffffffffu, pe[b], 31);
+        }
+    }
+    // Up to kLook terms after the range, for the continuation of a segment
+    // still open at its end (their segflag belongs to the next range); lanes
+    // past the lookahead count as heads, which stops the continuation there.
+    const u32 look = w1 < C.n ? min(kLook, C.n - w1) : 0u;
+    if (look) {
+        u64 ke[kLook / 32];
+        u32 pe[kLook / 32];
+        double ve[kLook / 32];
+#pragma unroll
+        for (int b = 0; b < (int)(kLook / 32); ++b) {
+            const u32 q = (u32)b * 32 + lane;
+            const bool valid = q < look;
+            ke[b] = valid ? C.keys[w1 + q] : 0ull;
+            pe[b] = valid ? fold_word<MODE>(C, w1 + q, ke[b]) : 0u;
+            ve[b] = valid ? C.vals[w1 + q] : 0.0;
+        }
+#pragma unroll
+        for (int b = 0; b < (int)(kLook / 32); ++b) {
+            const u32 q = (u32)b * 32 + lane;
+            u64 kp = __shfl_up_sync(0xffffffffu, ke[b], 1);
+            u32 pp = __shfl_up_sync(0xffffffffu, pe[b], 1);
+            if (lane == 0) {
+                kp = ck;
+                pp = cp;
+            }
+            bool head = true, neg = false;
+            if (q < look) {
+                head = !lane_same_key(C, w1 + q, ke[b], kp, pe[b], pp);
+                neg = (pe[b] >> 31) != 0;
+                sv[kLookSlot + q] = (MODE == kCanon && neg) ? -ve[b] : ve[b];
+            }
+            const u32 hb = __ballot_sync(0xffffffffu, head);
+            const u32 nb = __ballot_sync(0xffffffffu, neg);
+            if (lane == 0) {
+                hbw[32 + b] = hb;
+                nbw[32 + b] = nb;
+            }
             ck = __shfl_sync(0xffffffffu, ke[b], 31);
             cp = __shfl_sync(0xffffffffu, pe[b], 31);
         }
@@ -960,21 +1011,22 @@ __global__ void __launch_bounds__(32 * kFoldWarps)
     const u32 a = (u32)lane * kLaneSpan;
     const u32 sa = (u32)lane * 33u;
     const u32 lcnt = cnt > a ? min(cnt - a, (u32)kLaneSpan) : 0u;
+    const u32 HB = lcnt ? hbw[lane] : 0u;  // head / sign bits of the lane's span
+    const u32 NB = lcnt ? nbw[lane] : 0u;
     u32 fh = lcnt;  // prefix length (terms before the lane's first head)
     i64 h = -1;
     double r0 = 0.0, r1 = 0.0;
     u32 kept = 0;
     for (u32 i = 0; i < lcnt; ++i) {
-        const u32 s = sh[sa + i];
         const double v = sv[sa + i];
-        if (s & 1u) {
+        if ((HB >> i) & 1u) {
             if (h >= 0) kept += fold_close<MODE>(segval, segflag, h, r0, r1, F);
             else fh = i;
             h = (i64)(w0 + a + i);
             r0 = 0.0;
             r1 = 0.0;
         }
-        if (h >= 0) fold_term<MODE>(r0, r1, v, s >> 1);
+        if (h >= 0) fold_term<MODE>(r0, r1, v, (NB >> i) & 1u);
     }
     // ---- phase 2: carries across lane borders.  (oh, o0, o1) is the segment
     // open at the end of the lane's span; oh = -1 when it belongs to an
@@ -994,7 +1046,7 @@ __global__ void __launch_bounds__(32 * kFoldWarps)
             o0 = p0;
             o1 = p1;
             if (ph >= 0)
-                for (u32 i = 0; i < lcnt; ++i) fold_term<MODE>(o0, o1, sv[sa + i], sh[sa + i] >> 1);
+                for (u32 i = 0; i < lcnt; ++i) fold_term<MODE>(o0, o1, sv[sa + i], (NB >> i) & 1u);
             ready = true;
         }
     }
@@ -1004,7 +1056,7 @@ __global__ void __launch_bounds__(32 * kFoldWarps)
         double q1 = __shfl_up_sync(0xffffffffu, o1, 1);
         if (lane == 0) cin = -1;
         if (hh && cin >= 0) {
-            for (u32 i = 0; i < fh; ++i) fold_term<MODE>(q0, q1, sv[sa + i], sh[sa + i] >> 1);
+            for (u32 i = 0; i < fh; ++i) fold_term<MODE>(q0, q1, sv[sa + i], (NB >> i) & 1u);
             kept += fold_close<MODE>(segval, segflag, cin, q0, q1, F);
         }
     }
@@ -1016,16 +1068,41 @@ __global__ void __launch_bounds__(32 * kFoldWarps)
         if (w1 == C.n) {
             if (lane == 0) kept += fold_close<MODE>(segval, segflag, ch, c0, c1, F);
         } else {
-            // extension: continue past the range, 32 terms at a time
-            ck = C.keys[w1 - 1];
-            cp = fold_word<MODE>(C, w1 - 1, ck);
-            for (int ext = 0;; ++ext) {
-                const u32 cb = w1 + (u32)ext * 32u;
+            // continuation: first the staged lookahead terms, in order, on
+            // lane 0; a segment still open after them continues from global
+            // memory, 32 terms at a time, up to kExtChunks * 32 terms past the
+            // range in all (longer ones go to the long-run kernels)
+            int closed = 0;
+            if (lane == 0) {
+                for (u32 q = 0; q < look; ++q) {
+                    const u32 wq = 32u + (q >> 5), bq = q & 31u;
+                    if ((hbw[wq] >> bq) & 1u) {
+                        kept += fold_close<MODE>(segval, segflag, ch, c0, c1, F);
+                        closed = 1;
+                        break;
+                    }
+                    fold_term<MODE>(c0, c1, sv[kLookSlot + q], (nbw[wq] >> bq) & 1u);
+                }
+                if (!closed && w1 + look == C.n) {
+                    kept += fold_close<MODE>(segval, segflag, ch, c0, c1, F);
+                    closed = 1;
+                }
+            }
+            closed = __shfl_sync(0xffffffffu, closed, 0);
+            c0 = __shfl_sync(0xffffffffu, c0, 0);
+            c1 = __shfl_sync(0xffffffffu, c1, 0);
+            const u32 gs = w1 + look;  // look == kLook here (a shorter one reaches the end)
+            if (!closed) {
+                ck = C.keys[gs - 1];
+                cp = fold_word<MODE>(C, gs - 1, ck);
+            }
+            for (int ext = 0; !closed; ++ext) {
+                const u32 cb = gs + (u32)ext * 32u;
                 if (cb >= C.n) {
                     if (lane == 0) kept += fold_close<MODE>(segval, segflag, ch, c0, c1, F);
                     break;
                 }
-                if (ext >= kExtChunks) {
+                if (ext >= kExtChunks - (int)(kLook / 32)) {
                     if (lane == 0) {
                         segflag[ch] = 2;
                         long_list[atomicAdd(&counters[2], 1u)] = (u32)ch;
