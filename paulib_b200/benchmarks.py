@@ -58,6 +58,22 @@ def _propagation(args, rank, ws):
         return st.zero_state_expectation()
 
     steps = max(1, min(args.steps, 5))
+    # autotune: graph replay of the rotation chunks on or off (after one
+    # untimed run each, which for graphs includes their capture)
+    trial = {}
+    for g in (False, True):
+        st.use_graphs(g)
+        once()
+        _sync()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        once()
+        e1.record()
+        _sync()
+        trial[g] = e0.elapsed_time(e1)
+    graphs = min(trial, key=trial.get)
+    st.use_graphs(graphs)
     for _ in range(max(1, min(args.warmup, 2))):
         e = once()
     _abi.profile_reset(False)
@@ -80,7 +96,9 @@ def _propagation(args, rank, ws):
             "dtype": "u64 keys / f64 coefficients", "data": "synthetic, seeded",
             "config": {"workload": "propagation: sum_i Z_i, 64 qubits, 20 brickwork layers "
                                    "CNOT+RX+RZ, cutoff 1e-4, max_weight 8",
-                       "rotations": int(r.n), "final_terms": final, "expectation": e},
+                       "rotations": int(r.n), "final_terms": final, "expectation": e,
+                       "tuned": {"graphs": graphs,
+                                 "trials_ms": {"off": trial[False], "on": trial[True]}}},
             "gpu_launches": int(launches // steps)}
 
 
