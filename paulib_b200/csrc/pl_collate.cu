@@ -1767,7 +1767,7 @@ u32 derive_histograms(const ProdSrc<AS>& src, const KeyLayout& L, const PassPlan
     if (!mask) return 0u;
     u32* hA = B.counters + 128;                   // scratch after the counters
     u32* hB = hA + 8 * kRadix;
-    if (cudaMemsetAsync(hA, 0, sizeof(u32) * 16 * kRadix, st) != cudaSuccess) return 0u;
+    if (fill32_async(hA, 0u, sizeof(u32) * 16 * kRadix, st) != cudaSuccess) return 0u;
     const SoASrc<AS> a{src.ax, src.az, src.af, src.av, src.sa};
     const SoASrc<AS> b{src.bx, src.bz, src.bf, src.bv, src.sb};
     k_operand_hist<AS><<<grid_for(src.n, 256, 64), 256, 0, st>>>(a, src.n, L, P, mask, hA),
@@ -1844,10 +1844,10 @@ int run_collate(const Src& src, u32 n, int mode, const KeyLayout& L, const PassP
     const int items = radix_items();
     const u32 rtiles = (n + kThreads * items - 1) / (kThreads * items);
     const int nsm = sm_count();
-    PL_CUDA_TRY(cudaMemsetAsync(B.hist, 0, sizeof(u32) * kMaxPasses * kRadix, st));
-    PL_CUDA_TRY(cudaMemsetAsync(B.counters, 0, sizeof(u32) * (kMaxPasses + 8), st));
-    PL_CUDA_TRY(cudaMemsetAsync(B.d_status, 0, sizeof(int), st));
-    PL_CUDA_TRY(cudaMemsetAsync(B.d_count, 0, sizeof(i64), st));
+    PL_CUDA_TRY(fill32_async(B.hist, 0u, sizeof(u32) * kMaxPasses * kRadix, st));
+    PL_CUDA_TRY(fill32_async(B.counters, 0u, sizeof(u32) * (kMaxPasses + 8), st));
+    PL_CUDA_TRY(fill32_async(B.d_status, 0u, sizeof(int), st));
+    PL_CUDA_TRY(fill32_async(B.d_count, 0u, sizeof(i64), st));
     const int gblocks = grid_for(n, 256, nsm * 8);
     cudaEvent_t e0 = timed_begin(st);
     const u32 derived = derive_histograms<AS>(src, L, P, B, st);
@@ -1871,7 +1871,7 @@ int run_collate(const Src& src, u32 n, int mode, const KeyLayout& L, const PassP
         }
         k_scan_buckets<<<np, kRadix, 0, st>>>(B.hist, p0), pl::note_launch();
         for (int p = p0; p < p0 + np; ++p) {
-            PL_CUDA_TRY(cudaMemsetAsync(B.lb, 0, sizeof(u32) * (size_t)rtiles * kRadix, st));
+            PL_CUDA_TRY(fill32_async(B.lb, 0u, sizeof(u32) * (size_t)rtiles * kRadix, st));
             cudaEvent_t ev0 = timed_begin(st);
             const bool last = (p == P.npasses - 1);
             const u32* bs = B.hist + (size_t)p * kRadix;
@@ -1902,7 +1902,7 @@ int run_collate(const Src& src, u32 n, int mode, const KeyLayout& L, const PassP
     // counts survivors per emit tile, so the emit needs no look-back.
     const bool counted = a.max_weight == ~0ull;
     const FoldFilter F{counted ? 1 : 0, a.cutoff, B.tile_kept};
-    if (counted) PL_CUDA_TRY(cudaMemsetAsync(B.tile_kept, 0, sizeof(u32) * etiles, st));
+    if (counted) PL_CUDA_TRY(fill32_async(B.tile_kept, 0u, sizeof(u32) * etiles, st));
     e0 = timed_begin(st);
     int rc = PL_OK;
     if (mode == kCanon) rc = fold_segments<kCanon>(C, B, F, nsm, st);
@@ -1918,7 +1918,7 @@ int run_collate(const Src& src, u32 n, int mode, const KeyLayout& L, const PassP
                                                              B.segflag, n, B.tile_off, mode, out,
                                                              B.d_status), pl::note_launch();
     } else {
-        PL_CUDA_TRY(cudaMemsetAsync(B.lb_emit, 0, sizeof(u32) * etiles, st));
+        PL_CUDA_TRY(fill32_async(B.lb_emit, 0u, sizeof(u32) * etiles, st));
         k_emit<AS, Src><<<etiles, kThreads, 0, st>>>(src, L, kin, vin, B.seg_sum, B.segflag, n,
                                                      B.counters, B.lb_emit, mode, a.cutoff,
                                                      a.max_weight, out, B.d_count, B.d_status),
@@ -1928,9 +1928,8 @@ int run_collate(const Src& src, u32 n, int mode, const KeyLayout& L, const PassP
     PL_CUDA_TRY(cudaGetLastError());
     i64 cnt = 0;
     int dstat = 0;
-    PL_CUDA_TRY(cudaMemcpyAsync(&cnt, B.d_count, sizeof(i64), cudaMemcpyDeviceToHost, st));
-    PL_CUDA_TRY(cudaMemcpyAsync(&dstat, B.d_status, sizeof(int), cudaMemcpyDeviceToHost, st));
-    PL_CUDA_TRY(cudaStreamSynchronize(st));
+    const ReadReq rr[2] = {{&cnt, B.d_count, sizeof(i64)}, {&dstat, B.d_status, sizeof(int)}};
+    PL_CUDA_TRY(readback_sync(rr, 2, st));
     *out_count = cnt;
     if (dstat != 0) return record_status(dstat, "collate: device-side check");
     return PL_OK;
@@ -1949,10 +1948,10 @@ int run_collate_split(const Src& src, u32 n, const KeyLayout& L, const PassPlan&
     // then the (phase-0, phase-1) sums of the segments
     uint2* phs = reinterpret_cast<uint2*>(B.planes);
     double2* seg2 = reinterpret_cast<double2*>(reinterpret_cast<unsigned char*>(B.planes) + al(n));
-    PL_CUDA_TRY(cudaMemsetAsync(B.hist, 0, sizeof(u32) * kMaxPasses * kRadix, st));
-    PL_CUDA_TRY(cudaMemsetAsync(B.counters, 0, sizeof(u32) * (kMaxPasses + 8), st));
-    PL_CUDA_TRY(cudaMemsetAsync(B.d_status, 0, sizeof(int), st));
-    PL_CUDA_TRY(cudaMemsetAsync(B.d_count, 0, sizeof(i64), st));
+    PL_CUDA_TRY(fill32_async(B.hist, 0u, sizeof(u32) * kMaxPasses * kRadix, st));
+    PL_CUDA_TRY(fill32_async(B.counters, 0u, sizeof(u32) * (kMaxPasses + 8), st));
+    PL_CUDA_TRY(fill32_async(B.d_status, 0u, sizeof(int), st));
+    PL_CUDA_TRY(fill32_async(B.d_count, 0u, sizeof(i64), st));
     const int gblocks = grid_for(n, 256, nsm * 8);
     cudaEvent_t e0 = timed_begin(st);
     const u32 derived = derive_histograms<AS>(src, L, P, B, st);
@@ -1966,7 +1965,7 @@ int run_collate_split(const Src& src, u32 n, const KeyLayout& L, const PassPlan&
     k_scan_buckets<<<P.npasses, kRadix, 0, st>>>(B.hist, 0), pl::note_launch();
     u64 *kin = B.ka, *kout = B.kb;
     for (int p = 0; p < P.npasses; ++p) {
-        PL_CUDA_TRY(cudaMemsetAsync(B.lb, 0, sizeof(u32) * (size_t)rtiles * kRadix, st));
+        PL_CUDA_TRY(fill32_async(B.lb, 0u, sizeof(u32) * (size_t)rtiles * kRadix, st));
         cudaEvent_t ev0 = timed_begin(st);
         const bool last = (p == P.npasses - 1);
         const u32* bs = B.hist + (size_t)p * kRadix;
@@ -1990,7 +1989,7 @@ int run_collate_split(const Src& src, u32 n, const KeyLayout& L, const PassPlan&
     SegCtx C{kin, nullptr, B.sv, B.planes, n, 1, L.seg_mask0, kCanon};
     const u32 etiles = (n + kETile - 1) / kETile;
     const FoldFilter F{1, a.cutoff, B.tile_kept, seg2};
-    PL_CUDA_TRY(cudaMemsetAsync(B.tile_kept, 0, sizeof(u32) * etiles, st));
+    PL_CUDA_TRY(fill32_async(B.tile_kept, 0u, sizeof(u32) * etiles, st));
     e0 = timed_begin(st);
     int rc = fold_segments<kCanonSplit>(C, B, F, nsm, st);
     if (rc != PL_OK) return rc;
@@ -2005,9 +2004,8 @@ int run_collate_split(const Src& src, u32 n, const KeyLayout& L, const PassPlan&
     PL_CUDA_TRY(cudaGetLastError());
     i64 cnt = 0;
     int dstat = 0;
-    PL_CUDA_TRY(cudaMemcpyAsync(&cnt, B.d_count, sizeof(i64), cudaMemcpyDeviceToHost, st));
-    PL_CUDA_TRY(cudaMemcpyAsync(&dstat, B.d_status, sizeof(int), cudaMemcpyDeviceToHost, st));
-    PL_CUDA_TRY(cudaStreamSynchronize(st));
+    const ReadReq rr[2] = {{&cnt, B.d_count, sizeof(i64)}, {&dstat, B.d_status, sizeof(int)}};
+    PL_CUDA_TRY(readback_sync(rr, 2, st));
     *out_count = cnt;
     if (dstat != 0) return record_status(dstat, "collate: device-side check");
     return PL_OK;
@@ -2066,14 +2064,13 @@ int collate_soa(int as, const SoAView& in, const SoAOut& out, const CollateArgs&
     int rc = PL_OK;
     PL_DISPATCH_AS(as, {
         SoASrc<AS> src{in.x, in.z, in.f, in.v, in.stride};
-        PL_CUDA_TRY(cudaMemsetAsync(B.orm, 0, 8 * kMaxFields, st));
-        PL_CUDA_TRY(cudaMemsetAsync(B.andm, 0xff, 8 * kMaxFields, st));
+        PL_CUDA_TRY(fill32_async(B.orm, 0u, 8 * kMaxFields, st));
+        PL_CUDA_TRY(fill32_async(B.andm, 0xffffffffu, 8 * kMaxFields, st));
         k_masks<AS><<<grid_for(n, 256, sm_count() * 4), 256, 0, st>>>(src, n, a.mode, B.orm,
                                                                      B.andm), pl::note_launch();
         u64 hor[kMaxFields], hand[kMaxFields];
-        PL_CUDA_TRY(cudaMemcpyAsync(hor, B.orm, 8 * kMaxFields, cudaMemcpyDeviceToHost, st));
-        PL_CUDA_TRY(cudaMemcpyAsync(hand, B.andm, 8 * kMaxFields, cudaMemcpyDeviceToHost, st));
-        PL_CUDA_TRY(cudaStreamSynchronize(st));
+        const ReadReq rr[2] = {{hor, B.orm, 8 * kMaxFields}, {hand, B.andm, 8 * kMaxFields}};
+        PL_CUDA_TRY(readback_sync(rr, 2, st));
         if (!try_split<AS>(src, n, hor, hand, a, out, out_count, B, st, &rc)) {
             KeyLayout L;
             PassPlan P;
@@ -2112,16 +2109,16 @@ int multiply_collate(int as, const SoAView& lhs, const SoAView& rhs, const SoAOu
         // both operands' masks, one read-back
         u64 hor[2][kMaxFields];
         const SoAView* ops[2] = {&lhs, &rhs};
-        PL_CUDA_TRY(cudaMemsetAsync(B.orm, 0, 8 * 2 * kMaxFields, st));
-        PL_CUDA_TRY(cudaMemsetAsync(B.andm, 0xff, 8 * 2 * kMaxFields, st));
+        PL_CUDA_TRY(fill32_async(B.orm, 0u, 8 * 2 * kMaxFields, st));
+        PL_CUDA_TRY(fill32_async(B.andm, 0xffffffffu, 8 * 2 * kMaxFields, st));
         for (int w = 0; w < 2; ++w) {
             SoASrc<AS> s{ops[w]->x, ops[w]->z, ops[w]->f, ops[w]->v, ops[w]->stride};
             k_masks<AS><<<grid_for(ops[w]->n, 256, sm_count() * 4), 256, 0, st>>>(
                 s, (u32)ops[w]->n, a.mode, B.orm + w * kMaxFields, B.andm + w * kMaxFields),
                 pl::note_launch();
         }
-        PL_CUDA_TRY(cudaMemcpyAsync(hor, B.orm, 8 * 2 * kMaxFields, cudaMemcpyDeviceToHost, st));
-        PL_CUDA_TRY(cudaStreamSynchronize(st));
+        const ReadReq rr[1] = {{hor, B.orm, 8 * 2 * kMaxFields}};
+        PL_CUDA_TRY(readback_sync(rr, 1, st));
         u64 por[kMaxFields], pand[kMaxFields];
         for (int f = 0; f < 2 * AS; ++f) {
             por[f] = hor[0][f] | hor[1][f];

@@ -134,6 +134,22 @@ void capture_unlock();
 void note_launches(unsigned long long n);
 bool timing_enabled();
 void timed_push(cudaEvent_t start, cudaEvent_t stop, unsigned long long bytes, const char* name);
+// Small device-to-host reads (output counts, status words, key masks) that
+// must not wait behind large copies the caller has queued on other streams:
+// a one-warp kernel copies the words into a per-thread pinned, mapped host
+// buffer and only this stream is synchronised -- no copy engine is used.
+// Each request: `bytes` (a multiple of 4) from a 4-byte aligned device
+// address.
+struct ReadReq {
+    void* host;
+    const void* dev;
+    size_t bytes;
+};
+cudaError_t readback_sync(const ReadReq* reqs, int n, cudaStream_t st);
+// Fill `bytes` (a multiple of 4, 4-byte aligned) with a 32-bit pattern by a
+// kernel: a cudaMemsetAsync may run on a copy engine and then waits behind
+// copies the caller has queued on other streams.
+cudaError_t fill32_async(void* p, unsigned int value, size_t bytes, cudaStream_t st);
 // Event pair around one launch when timing is enabled (no-op otherwise).
 cudaEvent_t timed_begin(cudaStream_t st);
 void timed_end(cudaEvent_t start, cudaStream_t st, const char* name, unsigned long long bytes);

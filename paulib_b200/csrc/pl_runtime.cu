@@ -7,6 +7,8 @@
 // the void drop-ins can be checked with pl_get_last_error().
 
 #include <atomic>
+#include <cstdint>
+#include <cstring>
 #include <cstdio>
 #include <mutex>
 #include <string>
@@ -48,6 +50,92 @@ int record_cuda(cudaError_t e) {
     g_last_status = e == cudaErrorMemoryAllocation ? PL_ERR_OOM : PL_ERR_CUDA;
     g_last_msg = std::string("CUDA: ") + (s ? s : "unknown error");
     return g_last_status;
+}
+
+namespace {
+constexpr int kMaxReads = 4;
+struct ReadArgs {
+    const unsigned int* src[kMaxReads];
+    unsigned int dst_off[kMaxReads];
+    unsigned int words[kMaxReads];
+    int n;
+};
+__global__ void __launch_bounds__(32) k_readback(ReadArgs a, unsigned int* dst) {
+    for (int r = 0; r < a.n; ++r)
+        for (unsigned int i = threadIdx.x; i < a.words[r]; i += 32) dst[a.dst_off[r] + i] = a.src[r][i];
+}
+struct PinnedBuf {
+    void* host = nullptr;
+    unsigned int* dev = nullptr;
+    size_t bytes = 0;
+    ~PinnedBuf() {
+        if (host) cudaFreeHost(host);
+    }
+};
+thread_local PinnedBuf g_readback;
+
+__global__ void __launch_bounds__(256) k_fill32(unsigned int* p, size_t words, unsigned int v) {
+    const size_t stride = (size_t)gridDim.x * blockDim.x;
+    const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if ((reinterpret_cast<uintptr_t>(p) & 15u) == 0) {
+        uint4* q = reinterpret_cast<uint4*>(p);
+        const size_t n4 = words / 4;
+        for (size_t k = i; k < n4; k += stride) q[k] = make_uint4(v, v, v, v);
+        for (size_t k = n4 * 4 + i; k < words; k += stride) p[k] = v;
+    } else {
+        for (size_t k = i; k < words; k += stride) p[k] = v;
+    }
+}
+}  // namespace
+
+cudaError_t readback_sync(const ReadReq* reqs, int n, cudaStream_t st) {
+    if (n < 1 || n > kMaxReads) return cudaErrorInvalidValue;
+    ReadArgs a{};
+    size_t total = 0;
+    for (int r = 0; r < n; ++r) {
+        if (reqs[r].bytes % 4 != 0 || (reinterpret_cast<uintptr_t>(reqs[r].dev) & 3u) != 0)
+            return cudaErrorInvalidValue;
+        a.src[r] = static_cast<const unsigned int*>(reqs[r].dev);
+        a.dst_off[r] = (unsigned int)(total / 4);
+        a.words[r] = (unsigned int)(reqs[r].bytes / 4);
+        total += reqs[r].bytes;
+    }
+    a.n = n;
+    PinnedBuf& b = g_readback;
+    // one buffer per host thread: every use ends in a stream synchronisation,
+    // so no kernel of this thread still writes to it when it is replaced
+    if (b.bytes < total) {
+        if (b.host) cudaFreeHost(b.host);
+        b.host = nullptr;
+        b.bytes = 0;
+        const size_t want = total < 4096 ? 4096 : total;
+        cudaError_t e = cudaHostAlloc(&b.host, want, cudaHostAllocMapped | cudaHostAllocPortable);
+        if (e != cudaSuccess) return e;
+        void* d = nullptr;
+        e = cudaHostGetDevicePointer(&d, b.host, 0);
+        if (e != cudaSuccess) return e;
+        b.dev = static_cast<unsigned int*>(d);
+        b.bytes = want;
+    }
+    k_readback<<<1, 32, 0, st>>>(a, b.dev);
+    note_launch();
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) return e;
+    const unsigned char* h = static_cast<const unsigned char*>(b.host);
+    for (int r = 0; r < n; ++r) std::memcpy(reqs[r].host, h + (size_t)a.dst_off[r] * 4, reqs[r].bytes);
+    return cudaSuccess;
+}
+
+cudaError_t fill32_async(void* p, unsigned int value, size_t bytes, cudaStream_t st) {
+    if (bytes == 0) return cudaSuccess;
+    if (bytes % 4 != 0 || (reinterpret_cast<uintptr_t>(p) & 3u) != 0) return cudaErrorInvalidValue;
+    const size_t words = bytes / 4;
+    const int blocks = grid_for((i64)((words + 3) / 4), 256, sm_count() * 4);
+    k_fill32<<<blocks, 256, 0, st>>>(static_cast<unsigned int*>(p), words, value);
+    note_launch();
+    return cudaGetLastError();
 }
 
 static std::mutex g_alloc_mu;
