@@ -1844,10 +1844,11 @@ int run_collate(const Src& src, u32 n, int mode, const KeyLayout& L, const PassP
     const int items = radix_items();
     const u32 rtiles = (n + kThreads * items - 1) / (kThreads * items);
     const int nsm = sm_count();
-    PL_CUDA_TRY(fill32_async(B.hist, 0u, sizeof(u32) * kMaxPasses * kRadix, st));
-    PL_CUDA_TRY(fill32_async(B.counters, 0u, sizeof(u32) * (kMaxPasses + 8), st));
-    PL_CUDA_TRY(fill32_async(B.d_status, 0u, sizeof(int), st));
-    PL_CUDA_TRY(fill32_async(B.d_count, 0u, sizeof(i64), st));
+    const FillReq fr[4] = {{B.hist, 0u, sizeof(u32) * kMaxPasses * kRadix},
+                           {B.counters, 0u, sizeof(u32) * (kMaxPasses + 8)},
+                           {B.d_status, 0u, sizeof(int)},
+                           {B.d_count, 0u, sizeof(i64)}};
+    PL_CUDA_TRY(fill32_multi(fr, 4, st));
     const int gblocks = grid_for(n, 256, nsm * 8);
     cudaEvent_t e0 = timed_begin(st);
     const u32 derived = derive_histograms<AS>(src, L, P, B, st);
@@ -1948,10 +1949,13 @@ int run_collate_split(const Src& src, u32 n, const KeyLayout& L, const PassPlan&
     // then the (phase-0, phase-1) sums of the segments
     uint2* phs = reinterpret_cast<uint2*>(B.planes);
     double2* seg2 = reinterpret_cast<double2*>(reinterpret_cast<unsigned char*>(B.planes) + al(n));
-    PL_CUDA_TRY(fill32_async(B.hist, 0u, sizeof(u32) * kMaxPasses * kRadix, st));
-    PL_CUDA_TRY(fill32_async(B.counters, 0u, sizeof(u32) * (kMaxPasses + 8), st));
-    PL_CUDA_TRY(fill32_async(B.d_status, 0u, sizeof(int), st));
-    PL_CUDA_TRY(fill32_async(B.d_count, 0u, sizeof(i64), st));
+    const u32 etiles0 = (n + kETile - 1) / kETile;
+    const FillReq fr[5] = {{B.hist, 0u, sizeof(u32) * kMaxPasses * kRadix},
+                           {B.counters, 0u, sizeof(u32) * (kMaxPasses + 8)},
+                           {B.d_status, 0u, sizeof(int)},
+                           {B.d_count, 0u, sizeof(i64)},
+                           {B.tile_kept, 0u, sizeof(u32) * etiles0}};
+    PL_CUDA_TRY(fill32_multi(fr, 5, st));
     const int gblocks = grid_for(n, 256, nsm * 8);
     cudaEvent_t e0 = timed_begin(st);
     const u32 derived = derive_histograms<AS>(src, L, P, B, st);
@@ -1989,7 +1993,6 @@ int run_collate_split(const Src& src, u32 n, const KeyLayout& L, const PassPlan&
     SegCtx C{kin, nullptr, B.sv, B.planes, n, 1, L.seg_mask0, kCanon};
     const u32 etiles = (n + kETile - 1) / kETile;
     const FoldFilter F{1, a.cutoff, B.tile_kept, seg2};
-    PL_CUDA_TRY(fill32_async(B.tile_kept, 0u, sizeof(u32) * etiles, st));
     e0 = timed_begin(st);
     int rc = fold_segments<kCanonSplit>(C, B, F, nsm, st);
     if (rc != PL_OK) return rc;
@@ -2064,8 +2067,8 @@ int collate_soa(int as, const SoAView& in, const SoAOut& out, const CollateArgs&
     int rc = PL_OK;
     PL_DISPATCH_AS(as, {
         SoASrc<AS> src{in.x, in.z, in.f, in.v, in.stride};
-        PL_CUDA_TRY(fill32_async(B.orm, 0u, 8 * kMaxFields, st));
-        PL_CUDA_TRY(fill32_async(B.andm, 0xffffffffu, 8 * kMaxFields, st));
+        const FillReq fm[2] = {{B.orm, 0u, 8 * kMaxFields}, {B.andm, 0xffffffffu, 8 * kMaxFields}};
+        PL_CUDA_TRY(fill32_multi(fm, 2, st));
         k_masks<AS><<<grid_for(n, 256, sm_count() * 4), 256, 0, st>>>(src, n, a.mode, B.orm,
                                                                      B.andm), pl::note_launch();
         u64 hor[kMaxFields], hand[kMaxFields];
@@ -2109,8 +2112,9 @@ int multiply_collate(int as, const SoAView& lhs, const SoAView& rhs, const SoAOu
         // both operands' masks, one read-back
         u64 hor[2][kMaxFields];
         const SoAView* ops[2] = {&lhs, &rhs};
-        PL_CUDA_TRY(fill32_async(B.orm, 0u, 8 * 2 * kMaxFields, st));
-        PL_CUDA_TRY(fill32_async(B.andm, 0xffffffffu, 8 * 2 * kMaxFields, st));
+        const FillReq fm[2] = {{B.orm, 0u, 8 * 2 * kMaxFields},
+                               {B.andm, 0xffffffffu, 8 * 2 * kMaxFields}};
+        PL_CUDA_TRY(fill32_multi(fm, 2, st));
         for (int w = 0; w < 2; ++w) {
             SoASrc<AS> s{ops[w]->x, ops[w]->z, ops[w]->f, ops[w]->v, ops[w]->stride};
             k_masks<AS><<<grid_for(ops[w]->n, 256, sm_count() * 4), 256, 0, st>>>(

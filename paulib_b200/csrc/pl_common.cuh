@@ -150,6 +150,14 @@ cudaError_t readback_sync(const ReadReq* reqs, int n, cudaStream_t st);
 // kernel: a cudaMemsetAsync may run on a copy engine and then waits behind
 // copies the caller has queued on other streams.
 cudaError_t fill32_async(void* p, unsigned int value, size_t bytes, cudaStream_t st);
+// Several such fills in one launch (at most kMaxFills regions).
+struct FillReq {
+    void* p;
+    unsigned int value;
+    size_t bytes;
+};
+constexpr int kMaxFills = 8;
+cudaError_t fill32_multi(const FillReq* reqs, int n, cudaStream_t st);
 // Event pair around one launch when timing is enabled (no-op otherwise).
 cudaEvent_t timed_begin(cudaStream_t st);
 void timed_end(cudaEvent_t start, cudaStream_t st, const char* name, unsigned long long bytes);

@@ -86,7 +86,39 @@ __global__ void __launch_bounds__(256) k_fill32(unsigned int* p, size_t words, u
         for (size_t k = i; k < words; k += stride) p[k] = v;
     }
 }
+struct FillArgs {
+    unsigned int* p[kMaxFills];
+    size_t words[kMaxFills];
+    unsigned int v[kMaxFills];
+};
+// Region blockIdx.y of a multi-region fill.
+__global__ void __launch_bounds__(256) k_fill32_multi(FillArgs a) {
+    const int r = blockIdx.y;
+    unsigned int* p = a.p[r];
+    const size_t words = a.words[r];
+    const unsigned int v = a.v[r];
+    const size_t stride = (size_t)gridDim.x * blockDim.x;
+    for (size_t k = (size_t)blockIdx.x * blockDim.x + threadIdx.x; k < words; k += stride) p[k] = v;
+}
 }  // namespace
+
+cudaError_t fill32_multi(const FillReq* reqs, int n, cudaStream_t st) {
+    if (n < 1 || n > kMaxFills) return cudaErrorInvalidValue;
+    FillArgs a{};
+    size_t most = 0;
+    for (int r = 0; r < n; ++r) {
+        if (reqs[r].bytes % 4 != 0 || (reinterpret_cast<uintptr_t>(reqs[r].p) & 3u) != 0)
+            return cudaErrorInvalidValue;
+        a.p[r] = static_cast<unsigned int*>(reqs[r].p);
+        a.words[r] = reqs[r].bytes / 4;
+        a.v[r] = reqs[r].value;
+        if (a.words[r] > most) most = a.words[r];
+    }
+    const int bx = grid_for((i64)(most ? most : 1), 256, sm_count() * 2);
+    k_fill32_multi<<<dim3(bx, n), 256, 0, st>>>(a);
+    note_launch();
+    return cudaGetLastError();
+}
 
 cudaError_t readback_sync(const ReadReq* reqs, int n, cudaStream_t st) {
     if (n < 1 || n > kMaxReads) return cudaErrorInvalidValue;
