@@ -75,8 +75,12 @@ PL_API void launch_gpu_mul_soa(int array_size, const uint64_t* lhs_x, const uint
  * the reference); *d_count ends at the number of emitted terms.  Unlike the
  * reference's atomic slot claim, the emission order is deterministic:
  * lhs-major, rhs-minor, the order of the reference's single-threaded CPU
- * commutator_impl (PauliSumOperations.h:316-346).  Terms beyond `capacity`
- * are not written and record PL_ERR_CAPACITY. */
+ * commutator_impl (PauliSumOperations.h:316-346).  Asynchronous on `stream`,
+ * like the reference's launcher: the host never waits, and the look-back
+ * scratch is allocated and released in stream order.  Terms beyond
+ * `capacity` are not written (the reference writes past the end); *d_count
+ * still ends at the full count, so *d_count > capacity after the stream
+ * completes means the output did not fit. */
 PL_API void launch_gpu_commutator_soa(int array_size, int multiply_by_i, const uint64_t* lhs_x,
                                const uint64_t* lhs_z, const uint8_t* lhs_flags,
                                const double* lhs_val, const uint64_t* rhs_x,
@@ -113,7 +117,9 @@ PL_API int pl_commutator(int array_size, int multiply_by_i, const uint64_t* lhs_
  * address up (cudaGetSymbolAddress); make that first call before any stream
  * capture.  All calls share the array: calls that overlap on the GPU (other
  * streams, other threads) race and must be serialised by the caller.
- * Synchronous, like pl_commutator.  Calls no cudaMalloc / cudaFree. */
+ * Synchronous, like pl_commutator: before it returns it waits for the
+ * stream, because it copies the 4-byte device status back to the host.
+ * Calls no cudaMalloc / cudaFree / cudaHostAlloc. */
 PL_API int pl_commutator_noalloc(int array_size, int multiply_by_i, const uint64_t* lhs_x,
                                  const uint64_t* lhs_z, const uint8_t* lhs_flags,
                                  const double* lhs_val, int64_t n, const uint64_t* rhs_x,
@@ -313,7 +319,16 @@ PL_API int pl_propagate(pl_state* state, const uint64_t* rot_x, const uint64_t* 
 #define PL_OPT_GRAPHS 1  /* value != 0: runs of single-qubit rotations replay a captured
                             CUDA graph of their kernel chain (gate records live in device
                             memory, so one graph serves every run of that length) */
+#define PL_OPT_GATE_LOG 2  /* value != 0: every fast-path rotation of pl_propagate records
+                              its sizes (terms in, anticommuting terms, terms out) in a
+                              device log, one i64 triple per op in processing order (the
+                              circuit reversed); other ops record zeros.  For byte models;
+                              no counterpart in the reference. */
 PL_API int pl_state_set_option(pl_state* state, int option, int64_t value);
+/* Copy the gate log of the state's last pl_propagate (PL_OPT_GATE_LOG):
+ * min(max_ops, *n_ops) triples into sizes[3*q .. 3*q+2]; synchronous. */
+PL_API int pl_state_gate_log(pl_state* state, int64_t* sizes, int64_t max_ops,
+                             int64_t* n_ops);
 /* Device bytes the state's buffers and workspace hold. */
 PL_API int pl_state_memory(pl_state* state, uint64_t* bytes);
 

@@ -19,9 +19,10 @@ from __future__ import annotations
 import ctypes as C
 import os
 import platform
-from dataclasses import dataclass
 
 import numpy as np
+
+from paulib_b200.planes import Planes  # noqa: F401  (re-exported for the tests)
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 U64P = C.POINTER(C.c_uint64)
@@ -29,36 +30,6 @@ U8P = C.POINTER(C.c_uint8)
 F64P = C.POINTER(C.c_double)
 I32P = C.POINTER(C.c_int32)
 UINT64_MAX = (1 << 64) - 1
-
-
-@dataclass
-class Planes:
-    """Host SoA planes of a Pauli sum (the wire format of the C ABIs)."""
-
-    x: np.ndarray  # (AS, n) uint64
-    z: np.ndarray  # (AS, n) uint64
-    flags: np.ndarray  # (n,) uint8
-    val: np.ndarray  # (n,) float64
-
-    @property
-    def n(self) -> int:
-        return int(self.val.shape[0])
-
-    @property
-    def array_size(self) -> int:
-        return int(self.x.shape[0])
-
-    def copy(self) -> "Planes":
-        return Planes(self.x.copy(), self.z.copy(), self.flags.copy(), self.val.copy())
-
-    @staticmethod
-    def empty(array_size: int, n: int) -> "Planes":
-        return Planes(
-            np.zeros((array_size, n), np.uint64),
-            np.zeros((array_size, n), np.uint64),
-            np.zeros(n, np.uint8),
-            np.zeros(n, np.float64),
-        )
 
 
 def _c(a: np.ndarray, t):

@@ -47,7 +47,7 @@ EXPORTS = (
     "pl_set_tuning", "pl_get_tuning", "pl_state_apply_clifford", "pl_state_apply_rotation_gate",
     "pl_state_basis_state_expectation", "pl_state_trace", "pl_state_frobenius_norm2",
     "pl_state_lookup", "pl_state_trace_product", "pl_state_shard_pack", "pl_state_shard_unpack",
-    "pl_state_count_above", "pl_state_max_abs",
+    "pl_state_count_above", "pl_state_max_abs", "pl_state_gate_log",
 )
 PL_OP_CLIFFORD = 100
 GATES = {"H": 1, "S": 2, "H_YZ": 3, "H_XY": 4, "SQRT_X": 5, "SQRT_Y": 6, "X": 7, "Y": 8,
@@ -56,6 +56,7 @@ GATES = {"H": 1, "S": 2, "H_YZ": 3, "H_XY": 4, "SQRT_X": 5, "SQRT_Y": 6, "X": 7,
 PL_TUNE_RADIX_ITEMS = 1
 PL_TUNE_INDEX_KEYS = 2
 PL_OPT_GRAPHS = 1
+PL_OPT_GATE_LOG = 2
 PL_ORDER_GIVEN = 0
 PL_ORDER_LONGEST_FIRST = 1
 
@@ -165,6 +166,7 @@ def lib():
         "pl_state_shard_unpack": (I32, [VP, VP, I64]),
         "pl_state_count_above": (I32, [VP, C.c_double, C.POINTER(I64)]),
         "pl_state_max_abs": (I32, [VP, C.POINTER(C.c_double)]),
+        "pl_state_gate_log": (I32, [VP, VP, I64, C.POINTER(I64)]),
         "pl_state_apply_rotation_gate": (I32, [VP, I32, I32, C.c_double]),
         "pl_set_tuning": (I32, [I32, I64]),
         "pl_get_tuning": (I32, [I32, C.POINTER(I64)]),

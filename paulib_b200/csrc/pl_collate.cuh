@@ -67,6 +67,6 @@ int multiply_impl(int as, const u64* ax, const u64* az, const u8* af, const doub
 int commutator_impl(int as, int mul_i, const u64* ax, const u64* az, const u8* af,
                     const double* av, i64 n, i64 sa, const u64* bx, const u64* bz, const u8* bf,
                     const double* bv, i64 m, i64 sb, u64* ox, u64* oz, u8* of, double* ov,
-                    i64 capacity, unsigned long long* d_count, cudaStream_t st);
+                    i64 capacity, unsigned long long* d_count, bool wait, cudaStream_t st);
 
 }  // namespace pl

@@ -1371,6 +1371,17 @@ __global__ void __launch_bounds__(256) k_rot_begin(uint4* zero, size_t n16, int*
 
 __global__ void k_set_int(int* p, int v) { *p = v; }
 
+// The sizes of the rotation the cursor names: terms in, anticommuting terms
+// (children), terms out after the merge and truncation.
+__global__ void k_log_gate(i64* log, i64 nlog, const int* cursor, const i64* n_in,
+                           const i64* k, const i64* n_out) {
+    const int q = *cursor;
+    if (q < 0 || q >= nlog) return;
+    log[3 * q] = *n_in;
+    log[3 * q + 1] = k[0] + k[1];
+    log[3 * q + 2] = *n_out;
+}
+
 // A layer of CNOTs (PauliSumClifford.h:213-239) applied in op order to each
 // term in one pass: pairs[2k] = control, pairs[2k+1] = target.
 template <int AS>
@@ -1947,6 +1958,12 @@ struct pl_state {
     void* trim_mem = nullptr;       // trim control block and per-tile counts
     size_t trim_bytes = 0;
     double* red = nullptr;          // block sums and the result of a reduction
+    // Per-op sizes of the fast-path rotations (PL_OPT_GATE_LOG): terms in,
+    // anticommuting terms, terms out, three i64 per op in processing order.
+    bool gate_log = false;
+    i64* d_log = nullptr;
+    i64 log_ops = 0;       // ops the log holds
+    i64 log_used = 0;      // ops of the last propagation
 };
 
 namespace pl {
@@ -2233,6 +2250,11 @@ int rotation_chain(pl_state* s, int in, int op, const pl_truncation& tr, bool ti
         s->S[outb], s->d_size + outb, mw, cut, s->lbC, s->ctr + 2, s->d_status, s->d_fail);
     if (timed) timed_end(e0, s->st, "k_merge_reduce", 0ull);
     pl::note_launches(6);
+    if (s->gate_log && s->d_log) {
+        k_log_gate<<<1, 1, 0, s->st>>>(s->d_log, s->log_ops, s->d_cursor, s->d_size + in,
+                                        s->d_k, s->d_size + outb);
+        pl::note_launch();
+    }
     return PL_OK;
 }
 constexpr int kChainKernels = 6;
@@ -2291,7 +2313,8 @@ int rotation_graph(pl_state* s, int first, int len, const pl_truncation& tr) {
         k_set_int<<<1, 1, 0, s->st>>>(s->d_cursor, first - 1);
         pl::note_launch();
         for (int c = 0; c < chunks; ++c) PL_CUDA_TRY(cudaGraphLaunch(ex, s->st));
-        pl::note_launches((unsigned long long)kChainKernels * kGraphChunk * chunks);
+        pl::note_launches((unsigned long long)(kChainKernels + (s->gate_log ? 1 : 0)) *
+                          kGraphChunk * chunks);
     }
     for (int r = chunks * kGraphChunk; r < len; ++r) {
         const int rc = rotation_chain<AS>(s, s->cur, first + r, tr, true);
@@ -2304,7 +2327,8 @@ int rotation_graph(pl_state* s, int first, int len, const pl_truncation& tr) {
 // General-path rotation (any state, any generator) with or without the
 // following apply_truncation.
 template <int AS>
-int general_rotation(pl_state* s, const Rot& r, bool truncate, const pl_truncation& tr) {
+int general_rotation(pl_state* s, const Rot& r, bool truncate, const pl_truncation& tr,
+                     i64* k_anti = nullptr) {
     bool single = false;
     const GateP<AS> g = make_gate<AS>(r, &single);
     double c, sn;
@@ -2338,6 +2362,7 @@ int general_rotation(pl_state* s, const Rot& r, bool truncate, const pl_truncati
         PL_CUDA_TRY(cudaStreamSynchronize(s->st));
         if (n == 0) total = 0;
         if (st[0]) return record_status(st[0], "evolve: materialise");
+        if (k_anti) *k_anti = total - n;
         s->cur = other;
         CollateArgs a;
         if (truncate) {
@@ -2481,6 +2506,24 @@ int run_ops(pl_state* s, const std::vector<Rot>& rots, const std::vector<Op>& op
         modes[r] = classify(rots[r].theta, &cs[r], &sns[r]);
     }
     if (ops.empty()) return PL_OK;
+    if (s->gate_log) {
+        if (s->log_ops < (i64)ops.size()) {
+            // captured chains hold the log's address
+            drop_graphs(s);
+            if (s->d_log) dev_free(s->d_log, s->st);
+            s->d_log = nullptr;
+            s->log_ops = 0;
+            void* p = nullptr;
+            if (dev_alloc(&p, 24 * ops.size(), s->st) != cudaSuccess) {
+                cudaGetLastError();
+                return record_status(PL_ERR_OOM, "propagate: gate log");
+            }
+            s->d_log = static_cast<i64*>(p);
+            s->log_ops = (i64)ops.size();
+        }
+        PL_CUDA_TRY(fill32_async(s->d_log, 0u, 24 * ops.size(), s->st));
+        s->log_used = (i64)ops.size();
+    }
     {
         std::vector<GateRec<AS>> recs(ops.size());
         std::vector<int> pairs(2 * ops.size(), 0);
@@ -2615,8 +2658,17 @@ int run_ops(pl_state* s, const std::vector<Rot>& rots, const std::vector<Op>& op
                 rc = checkpoint(&rewound);
                 if (rc) return rc;
                 if (rewound) continue;
-                rc = general_rotation<AS>(s, rots[r], true, tr);
+                i64 m_in = 0, k_anti = 0;
+                if (s->gate_log && s->d_log && (rc = read_size(s, &m_in))) return rc;
+                rc = general_rotation<AS>(s, rots[r], true, tr, &k_anti);
                 if (rc) return rc;
+                if (s->gate_log && s->d_log) {
+                    i64 trip[3] = {m_in, k_anti, 0};
+                    if ((rc = read_size(s, &trip[2]))) return rc;
+                    PL_CUDA_TRY(cudaMemcpyAsync(s->d_log + 3 * i, trip, sizeof(trip),
+                                                cudaMemcpyHostToDevice, s->st));
+                    PL_CUDA_TRY(cudaStreamSynchronize(s->st));
+                }
                 if (trimming) {
                     rc = trim_state<AS>(s, tr.max_terms, no_protect);
                     if (rc) return rc;
@@ -2690,6 +2742,7 @@ extern "C" int pl_state_destroy(pl_state* s) {
     s->ws.ptr = nullptr;
     if (s->trim_mem) dev_free(s->trim_mem, s->st);
     if (s->red) dev_free(s->red, s->st);
+    if (s->d_log) dev_free(s->d_log, s->st);
     cudaStreamSynchronize(s->st);
     delete s;
     return record_status(PL_OK, nullptr);
@@ -2703,7 +2756,27 @@ extern "C" int pl_state_set_option(pl_state* s, int option, int64_t value) {
         if (!s->use_graphs) drop_graphs(s);
         return record_status(PL_OK, nullptr);
     }
+    if (option == PL_OPT_GATE_LOG) {
+        if ((value != 0) != s->gate_log) drop_graphs(s);  // chains with / without the log
+        s->gate_log = value != 0;
+        return record_status(PL_OK, nullptr);
+    }
     return record_status(PL_ERR_INVALID_ARG, "pl_state_set_option: unknown option");
+}
+
+extern "C" int pl_state_gate_log(pl_state* s, int64_t* sizes, int64_t max_ops, int64_t* n_ops) {
+    int rc = check_state(s);
+    if (rc) return rc;
+    if (!n_ops || max_ops < 0 || (max_ops > 0 && !sizes))
+        return record_status(PL_ERR_INVALID_ARG, "pl_state_gate_log");
+    *n_ops = s->d_log ? s->log_used : 0;
+    const i64 n = std::min<i64>(*n_ops, max_ops);
+    if (n > 0) {
+        PL_CUDA_TRY(cudaMemcpyAsync(sizes, s->d_log, 24 * (size_t)n, cudaMemcpyDeviceToHost,
+                                    s->st));
+        PL_CUDA_TRY(cudaStreamSynchronize(s->st));
+    }
+    return record_status(PL_OK, nullptr);
 }
 
 extern "C" int pl_state_memory(pl_state* s, uint64_t* bytes) {
@@ -3369,7 +3442,7 @@ extern "C" int pl_state_commutator(pl_state* out, pl_state* a, pl_state* b, int 
         PL_CUDA_TRY(cudaMemsetAsync(out->d_tmp, 0, sizeof(i64), out->st));
         rc = commutator_impl(out->as, multiply_by_i ? 1 : 0, A.x, A.z, A.f, A.v, n, A.cap, B.x,
                              B.z, B.f, B.v, m, B.cap, O.x, O.z, O.f, O.v, O.cap,
-                             (unsigned long long*)out->d_tmp, out->st);
+                             (unsigned long long*)out->d_tmp, true, out->st);
         i64 cnt = 0;
         PL_CUDA_TRY(cudaMemcpyAsync(&cnt, out->d_tmp, sizeof(i64), cudaMemcpyDeviceToHost,
                                     out->st));

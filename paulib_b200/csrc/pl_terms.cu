@@ -263,7 +263,9 @@ int commutator_launch(int as, int mul_i, const u64* ax, const u64* az, const u8*
     unsigned char* s = (unsigned char*)scratch;
     u64* lb = (u64*)(s + 256);
     u32* tile_ctr = (u32*)s;
-    PL_CUDA_TRY(cudaMemsetAsync(scratch, 0, commutator_scratch_bytes(npairs), st));
+    // a fill kernel, not a copy-engine memset: it never queues behind a
+    // caller's large copies on other streams
+    PL_CUDA_TRY(fill32_async(scratch, 0u, commutator_scratch_bytes(npairs), st));
     PL_DISPATCH_AS(as, k_commutator<AS><<<(unsigned)tiles, kCThreads, 0, st>>>(
                            ax, az, af, av, (u64)n, (u64)sa, bx, bz, bf, bv, (u64)m, (u64)sb,
                            mul_i, ox, oz, of, ov, capacity, d_count, npairs, lb, tile_ctr,
@@ -272,10 +274,16 @@ int commutator_launch(int as, int mul_i, const u64* ax, const u64* az, const u8*
     return PL_OK;
 }
 
+// The commutator with stream-ordered scratch.  With `wait` the call reads the
+// device status back (a stream synchronisation) and reports a capacity or
+// look-back failure; without it the call is asynchronous like the
+// reference's launcher (paulib_gpu_api.h:35-42): nothing waits on the host,
+// the scratch is released in stream order, and an output that did not fit
+// shows as *d_count > capacity.
 int commutator_impl(int as, int mul_i, const u64* ax, const u64* az, const u8* af,
                     const double* av, i64 n, i64 sa, const u64* bx, const u64* bz, const u8* bf,
                     const double* bv, i64 m, i64 sb, u64* ox, u64* oz, u8* of, double* ov,
-                    i64 capacity, unsigned long long* d_count, cudaStream_t st) {
+                    i64 capacity, unsigned long long* d_count, bool wait, cudaStream_t st) {
     if (as < 1 || as > kMaxAS || n < 0 || m < 0 || capacity < 0 || !d_count ||
         (n > 0 && m > (1ll << 40) / n))
         return record_status(PL_ERR_INVALID_ARG, "commutator: bad array_size or size");
@@ -287,15 +295,17 @@ int commutator_impl(int as, int mul_i, const u64* ax, const u64* az, const u8* a
     void* scratch = nullptr;
     PL_CUDA_TRY(cudaMallocAsync(&scratch, bytes, st));
     int* d_status = (int*)((unsigned char*)scratch + bytes - 256);
-    PL_CUDA_TRY(cudaMemsetAsync(d_status, 0, sizeof(int), st));
-    int rc = commutator_launch(as, mul_i, ax, az, af, av, n, sa, bx, bz, bf, bv, m, sb, ox, oz,
+    int rc = PL_OK;
+    cudaError_t e = fill32_async(d_status, 0u, sizeof(int), st);
+    if (e != cudaSuccess) rc = record_cuda(e);
+    if (rc == PL_OK)
+        rc = commutator_launch(as, mul_i, ax, az, af, av, n, sa, bx, bz, bf, bv, m, sb, ox, oz,
                                of, ov, capacity, d_count, scratch, d_status, st);
     int dstat = 0;
-    if (rc == PL_OK) {
-        // The capacity/timeout check needs the device status: read it back
-        // stream-ordered, then release the scratch.
-        cudaError_t e = cudaMemcpyAsync(&dstat, d_status, sizeof(int), cudaMemcpyDeviceToHost, st);
-        if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (rc == PL_OK && wait) {
+        // the capacity / timeout check needs the device status
+        const ReadReq rr[1] = {{&dstat, d_status, sizeof(int)}};
+        e = readback_sync(rr, 1, st);
         if (e != cudaSuccess) rc = record_cuda(e);
     }
     cudaFreeAsync(scratch, st);
@@ -344,7 +354,7 @@ extern "C" void launch_gpu_commutator_soa(int array_size, int multiply_by_i,
     commutator_impl(array_size, multiply_by_i ? 1 : 0, (const u64*)lhs_x, (const u64*)lhs_z,
                     lhs_flags, lhs_val, n, n, (const u64*)rhs_x, (const u64*)rhs_z, rhs_flags,
                     rhs_val, m, m, (u64*)out_x, (u64*)out_z, out_flags, out_val, capacity,
-                    d_count, stream);
+                    d_count, false, stream);
 }
 
 extern "C" int pl_commutator(int array_size, int multiply_by_i, const uint64_t* lhs_x,
@@ -357,7 +367,7 @@ extern "C" int pl_commutator(int array_size, int multiply_by_i, const uint64_t* 
     return commutator_impl(array_size, multiply_by_i ? 1 : 0, (const u64*)lhs_x,
                            (const u64*)lhs_z, lhs_flags, lhs_val, n, n, (const u64*)rhs_x,
                            (const u64*)rhs_z, rhs_flags, rhs_val, m, m, (u64*)out_x,
-                           (u64*)out_z, out_flags, out_val, capacity, d_count, stream);
+                           (u64*)out_z, out_flags, out_val, capacity, d_count, true, stream);
 }
 
 extern "C" int pl_apply_cnot(int array_size, uint64_t* x, uint64_t* z, uint8_t* flags, int64_t n,
@@ -452,7 +462,8 @@ extern "C" int pl_commutator_noalloc(int array_size, int multiply_by_i, const ui
     if (rc) return rc;
     int* d_status = (int*)((unsigned char*)scratch + kNoAllocBytes - 256);
     // the array keeps the previous call's contents: clear what must start at 0
-    PL_CUDA_TRY(cudaMemsetAsync(d_status, 0, sizeof(int), stream));
+    // (a fill kernel; the look-back words are cleared by commutator_launch)
+    PL_CUDA_TRY(fill32_async(d_status, 0u, sizeof(int), stream));
     rc = commutator_launch(array_size, multiply_by_i ? 1 : 0, (const u64*)lhs_x,
                            (const u64*)lhs_z, lhs_flags, lhs_val, n, n, (const u64*)rhs_x,
                            (const u64*)rhs_z, rhs_flags, rhs_val, m, m, (u64*)out_x,
@@ -460,6 +471,9 @@ extern "C" int pl_commutator_noalloc(int array_size, int multiply_by_i, const ui
                            stream);
     if (rc) return rc;
     (void)npairs;
+    // The 4-byte status comes back by a plain copy into this stack variable:
+    // the mapped pinned buffer the other entry points read through is
+    // allocated on a thread's first use, which this entry point must not do.
     int dstat = 0;
     PL_CUDA_TRY(cudaMemcpyAsync(&dstat, d_status, sizeof(int), cudaMemcpyDeviceToHost, stream));
     PL_CUDA_TRY(cudaStreamSynchronize(stream));

@@ -60,6 +60,25 @@ class State:
                    "pl_state_set_option")
         return self
 
+    def log_gates(self, enable: bool = True):
+        """Record (terms in, anticommuting terms, terms out) of every
+        fast-path rotation of the next propagate() (PL_OPT_GATE_LOG)."""
+        _abi.check(self._lib.pl_state_set_option(self._h, _abi.PL_OPT_GATE_LOG,
+                                                 int(bool(enable))), "pl_state_set_option")
+        return self
+
+    def gate_log(self) -> np.ndarray:
+        """(ops, 3) int64 sizes of the last propagate(), in processing order
+        (the circuit reversed); rows of ops that are not fast-path rotations
+        are zero."""
+        n = C.c_int64()
+        _abi.check(self._lib.pl_state_gate_log(self._h, None, 0, C.byref(n)), "pl_state_gate_log")
+        out = np.zeros((n.value, 3), np.int64)
+        if n.value:
+            _abi.check(self._lib.pl_state_gate_log(self._h, out.ctypes.data_as(C.c_void_p),
+                                                   n.value, C.byref(n)), "pl_state_gate_log")
+        return out
+
     def memory(self) -> int:
         b = C.c_uint64()
         _abi.check(self._lib.pl_state_memory(self._h, C.byref(b)), "pl_state_memory")

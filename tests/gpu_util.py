@@ -5,7 +5,7 @@ import ctypes as C
 
 import numpy as np
 
-from oracle.oracle import Planes
+from paulib_b200.planes import Planes
 from paulib_b200 import _abi
 
 

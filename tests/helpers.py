@@ -3,7 +3,7 @@ from __future__ import annotations
 
 import numpy as np
 
-from oracle.oracle import Planes
+from paulib_b200.planes import Planes
 from paulib_b200 import strings
 
 
@@ -82,3 +82,33 @@ def assert_values_close(a: Planes, b: Planes, scale=None, rtol=1e-12):
 def bit_identical(a: Planes, b: Planes) -> bool:
     return a.val.shape == b.val.shape and np.array_equal(a.val.view(np.uint64),
                                                          b.val.view(np.uint64))
+
+
+def key_records(p: Planes, phase_only=True) -> np.ndarray:
+    """One fixed-width byte record per term whose byte order is the sort
+    order of the canonical key (x[0..AS), z[0..AS), flags): each u64 word
+    big-endian, then the flags byte (its phase bit with phase_only)."""
+    aw, n = p.array_size, p.n
+    rec = np.empty((n, 16 * aw + 1), np.uint8)
+    for k in range(aw):
+        rec[:, 8 * k: 8 * k + 8] = np.ascontiguousarray(p.x[k]).astype(">u8").view(
+            np.uint8).reshape(n, 8)
+        rec[:, 8 * (aw + k): 8 * (aw + k) + 8] = np.ascontiguousarray(p.z[k]).astype(
+            ">u8").view(np.uint8).reshape(n, 8)
+    rec[:, 16 * aw] = p.flags & np.uint8(1 if phase_only else 3)
+    return rec.view(f"V{16 * aw + 1}").ravel()
+
+
+def assert_values_close_sorted(a: Planes, b: Planes, scale: Planes, rtol=1e-12):
+    """Vectorised assert_values_close for canonical sums: `scale` is the
+    sort_and_combine of the input with |values| and the sign folded (keys a
+    sorted superset of b's keys); |a - b| <= rtol * max(|b|, scale[key])."""
+    kb, ks = key_records(b), key_records(scale)
+    pos = np.searchsorted(ks, kb)
+    assert (pos < ks.shape[0]).all() and (ks[np.minimum(pos, ks.shape[0] - 1)] == kb).all(), \
+        "scale keys do not cover the result"
+    ref = np.maximum(np.abs(b.val), scale.val[pos])
+    err = np.abs(a.val - b.val)
+    bad = err > rtol * ref
+    assert not bad.any(), (f"{int(bad.sum())} coefficients differ beyond {rtol} relative; "
+                           f"worst {float((err / np.maximum(ref, 1e-300)).max()):.3e}")

@@ -9,7 +9,7 @@ one-instance-at-a-time path (no graphs, one lane).
 import numpy as np
 import pytest
 
-from oracle.oracle import Planes
+from paulib_b200.planes import Planes
 from paulib_b200 import batch as B
 from paulib_b200 import propagation as PR
 from paulib_b200 import workloads as W

@@ -13,7 +13,7 @@ import pytest
 from gpu_util import as_planes, gpu_collate, gpu_multiply_collate
 from helpers import (abs_scale, assert_keys_equal, assert_values_close, bit_identical, planes,
                      random_sum, to_str)
-from oracle.oracle import Planes
+from paulib_b200.planes import Planes
 from paulib_b200 import _abi
 from paulib_b200 import workloads as W
 

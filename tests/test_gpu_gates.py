@@ -12,7 +12,7 @@ import pytest
 
 from gates_golden import GATE, ONE_QUBIT, ROTATIONS, TWO_QUBIT
 from helpers import assert_keys_equal, bit_identical, planes, random_sum, to_str
-from oracle.oracle import Planes
+from paulib_b200.planes import Planes
 from paulib_b200 import propagation as PR
 from paulib_b200 import workloads as W
 

@@ -14,7 +14,7 @@ import pytest
 from gpu_util import as_planes
 from helpers import (abs_scale, assert_keys_equal, assert_values_close, bit_identical, planes,
                      random_sum, to_str)
-from oracle.oracle import Planes
+from paulib_b200.planes import Planes
 from paulib_b200 import propagation as PR
 from paulib_b200 import workloads as W
 
@@ -218,3 +218,29 @@ def test_state_commutator(cuda, oracle, mul_i):
     o = oracle.commutator(a, b, bool(mul_i))
     assert_keys_equal(g, o)
     assert bit_identical(g, o)
+
+
+def test_gate_log_sizes(cuda, oracle):
+    # PL_OPT_GATE_LOG: per fast-path rotation (terms in, anticommuting,
+    # terms out), in processing order; logging changes no result.
+    obs, circ, tr = W.heisenberg_workload(seed=2, num_qubits=20, layers=3)
+    kw = dict(max_weight=tr["max_weight"], cutoff=tr["cutoff"])
+    r = circ.rotations
+    with state_of(as_planes(obs)) as st:
+        st.use_graphs(True).log_gates(True)
+        st.propagate(r.x, r.z, r.flags, r.val, circ.ops, **kw)
+        g = planes_of(st)
+        log = st.gate_log()
+    o = oracle.propagate(as_planes(obs), as_planes(r), circ.ops, **kw)
+    assert bit_identical(g, o)
+    assert log.shape == (circ.ops.shape[0], 3)
+    rot_rows = circ.ops[::-1, 0] == W.OP_ROT
+    assert (log[~rot_rows] == 0).all()
+    rows = log[rot_rows]
+    # every rotation of this circuit takes the fast path
+    assert (rows[:, 0] > 0).all()
+    assert rows[0, 0] == obs.n and rows[-1, 2] == g.n
+    # CNOT layers keep the size: each rotation starts from the last one's output
+    assert np.array_equal(rows[1:, 0], rows[:-1, 2])
+    assert (rows[:, 1] <= rows[:, 0]).all()
+    assert (rows[:, 2] <= rows[:, 0] + rows[:, 1]).all()

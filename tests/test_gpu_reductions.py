@@ -10,7 +10,7 @@ from helpers import planes, random_sum
 from paulib_b200 import paulib as PL
 from paulib_b200 import propagation as PR
 from paulib_b200 import strings
-from oracle.oracle import Planes
+from paulib_b200.planes import Planes
 
 pytestmark = pytest.mark.gpu
 

@@ -12,7 +12,7 @@ import pytest
 
 import shard_ref
 from helpers import assert_keys_equal, bit_identical, random_sum
-from oracle.oracle import Planes
+from paulib_b200.planes import Planes
 from paulib_b200 import _abi
 from paulib_b200 import propagation as PR
 

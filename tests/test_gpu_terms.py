@@ -16,7 +16,7 @@ import pytest
 
 from gpu_util import (as_planes, gpu_cnot, gpu_commutator, gpu_multiply, gpu_zero_state)
 from helpers import assert_keys_equal, bit_identical, planes, random_sum
-from oracle.oracle import Planes
+from paulib_b200.planes import Planes
 from paulib_b200 import workloads as W
 
 pytestmark = pytest.mark.gpu
@@ -86,6 +86,33 @@ def test_commutator_capacity_reported(cuda, oracle):
     with pytest.raises(_abi.PLError) as e:
         gpu_commutator(a, b, capacity=max(full.n // 2, 1))
     assert e.value.status == _abi.PL_ERR_CAPACITY
+
+
+def test_dropin_commutator_is_async_and_counts_overflow(cuda, oracle):
+    # The drop-in launcher is asynchronous like the reference's
+    # (paulib_gpu_api.h:35-42): no status read-back; an output that does not
+    # fit shows as a final count above the capacity, and the slots that fit
+    # hold the first terms in order.
+    import torch
+    from gpu_util import dev, host
+    from paulib_b200 import _abi
+    a, b = random_sum(64, 1, 5, 20), random_sum(64, 1, 6, 20)
+    full = oracle.commutator(a, b)
+    cap = max(full.n // 2, 1)
+    da, db = dev(a), dev(b)
+    out = _abi.DeviceSum(1, cap)
+    cnt = torch.zeros(1, dtype=torch.int64, device="cuda")
+    L = _abi.lib()
+    L.launch_gpu_commutator_soa(1, 0, *da.ptrs(), *db.ptrs(), *out.ptrs(), cnt.data_ptr(),
+                                a.n, b.n, cap, _abi.stream_ptr())
+    torch.cuda.synchronize()
+    assert _abi.last_error() == _abi.PL_OK
+    assert int(cnt.item()) == full.n > cap
+    out.n = cap
+    g = host(out)
+    head = Planes(full.x[:, :cap], full.z[:, :cap], full.flags[:cap], full.val[:cap])
+    assert_keys_equal(g, head)
+    assert bit_identical(g, head)
 
 
 @pytest.mark.parametrize("words,c,t", [(1, 0, 1), (1, 3, 9), (2, 0, 70), (2, 100, 5),

@@ -9,7 +9,7 @@ import numpy as np
 import pytest
 
 from helpers import assert_keys_equal, bit_identical, planes, random_sum, to_str
-from oracle.oracle import Planes
+from paulib_b200.planes import Planes
 from paulib_b200 import propagation as PR
 from paulib_b200 import workloads as W
 

@@ -14,7 +14,7 @@ import numpy as np
 import pytest
 
 from helpers import planes, random_sum, to_str
-from oracle.oracle import Planes
+from paulib_b200.planes import Planes
 
 IMPLS = ["oracle", "reference"]
 

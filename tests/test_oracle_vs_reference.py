@@ -12,7 +12,7 @@ import pytest
 
 from helpers import abs_scale, assert_keys_equal, assert_values_close, bit_identical, random_sum
 from paulib_b200 import workloads as W
-from oracle.oracle import Planes
+from paulib_b200.planes import Planes
 
 
 def P(s):

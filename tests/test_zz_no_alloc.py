@@ -57,3 +57,35 @@ def test_noalloc_rejects_oversized_requests(cuda):
     rc = L.pl_commutator_noalloc(1, 0, *args, 1 << 15, *args, 1 << 15, *args, 1, dummy, None)
     assert rc == _abi.PL_ERR_INVALID_ARG
     assert b"2^29" in L.pl_last_error_message()
+
+
+def test_noalloc_accepts_exactly_the_limit(cuda):
+    # 2^15 x 2^14 = 2^29 pairs fill the static array's 2^16 look-back tiles
+    # exactly.  All-Z strings commute pairwise, so nothing is emitted and no
+    # output memory is needed.  One more rhs term is over the limit.
+    import torch
+    from paulib_b200 import _abi
+    from paulib_b200.planes import Planes
+    L = _abi.lib()
+    rng = np.random.default_rng(3)
+
+    def all_z(n):
+        z = rng.integers(1, 1 << 20, size=(1, n), dtype=np.uint64)
+        return Planes(np.zeros((1, n), np.uint64), z, np.zeros(n, np.uint8),
+                      rng.standard_normal(n))
+
+    a, b = all_z(1 << 15), all_z((1 << 14) + 1)
+    da = _abi.DeviceSum.from_host(a.x, a.z, a.flags, a.val)
+    db = _abi.DeviceSum.from_host(b.x, b.z, b.flags, b.val)
+    out = _abi.DeviceSum(1, 1)
+    cnt = torch.zeros(1, dtype=torch.int64, device="cuda")
+    for _ in range(2):
+        cnt.zero_()
+        rc = L.pl_commutator_noalloc(1, 0, *da.ptrs(), a.n, *db.ptrs(), 1 << 14, *out.ptrs(),
+                                     0, cnt.data_ptr(), _abi.stream_ptr())
+        assert rc == _abi.PL_OK
+        torch.cuda.synchronize()
+        assert int(cnt.item()) == 0
+    rc = L.pl_commutator_noalloc(1, 0, *da.ptrs(), a.n, *db.ptrs(), (1 << 14) + 1, *out.ptrs(),
+                                 0, cnt.data_ptr(), _abi.stream_ptr())
+    assert rc == _abi.PL_ERR_INVALID_ARG
