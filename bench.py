@@ -8,7 +8,13 @@ Default workload (the headline metric, "Pauli products collated/s"):
   pl_multiply_collate C-ABI call.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                  [--workload product_collate|propagation|commutator]
+                  [--workload product_collate|propagation|commutator|batch|serve]
+
+At N = 1 the product_collate line also carries: parity of the timed output
+against the reference build, the reference's own CUDA kernels timed beside
+ours (gpu_comparator), the 64-qubit propagation with its byte-model roofline
+and a reference CPU baseline on a circuit prefix (propagation), and the
+served stream against plain FIFO service (served); --no-extras skips them.
 
 Under torchrun (N > 1) every rank runs an independent instance of the
 workload (weak scaling, no data-path collective); times are the max over
@@ -168,10 +174,43 @@ def b_canon(n_in, n_out, bits, s_in=25, s_out=25):
 # product + collate (our arm)
 # ---------------------------------------------------------------------------
 def product_workload(seed):
-    from oracle.oracle import Planes  # plain numpy container, no oracle code runs
     from paulib_b200 import workloads as W
+    from paulib_b200.planes import Planes
     a, b = W.product_operands(seed=seed)
     return Planes(a.x, a.z, a.flags, a.val), Planes(b.x, b.z, b.flags, b.val)
+
+
+def product_config(ws, n=4096, m=4096):
+    """The workload description both arms print (identical by construction)."""
+    return {"workload": "product_collate: PauliSum<64,double> 4096 x 4096 product + "
+                        "canonicalize, 20 active qubits, weight U{1..4}",
+            "terms_lhs": n, "terms_rhs": m, "products_per_step": n * m, "array_size": 1,
+            "parallelism": f"replicas x{ws}",
+            "l2": "flushed between steps (256 MB write outside the step events); "
+                  "step working set 0.6 GB > 126 MB L2"}
+
+
+def host_cpu():
+    """Model name and thread count of this host (lscpu, else /proc/cpuinfo)."""
+    name = None
+    try:
+        out = subprocess.run(["lscpu"], capture_output=True, text=True, timeout=10).stdout
+        for ln in out.splitlines():
+            if ln.startswith("Model name:"):
+                name = ln.split(":", 1)[1].strip()
+                break
+    except (OSError, subprocess.SubprocessError):
+        pass
+    if name is None:
+        try:
+            with open("/proc/cpuinfo") as fh:
+                for ln in fh:
+                    if ln.startswith("model name"):
+                        name = ln.split(":", 1)[1].strip()
+                        break
+        except OSError:
+            pass
+    return {"model": name, "nproc": os.cpu_count()}
 
 
 def run_product_collate(args, rank, local, ws):
@@ -351,14 +390,10 @@ def run_product_collate(args, rank, local, ws):
         "scaling": "weak", "vs_baseline": None, "dtype": "u64 keys / f64 coefficients",
         "data": "synthetic, seeded (numpy PCG64); shapes and distributions of the "
                 "product+collate benchmark",
-        "config": {"workload": "product_collate: PauliSum<64,double> 4096 x 4096 product + "
-                               "canonicalize, 20 active qubits, weight U{1..4}",
-                   "terms_lhs": n, "terms_rhs": m, "products_per_step": total,
-                   "terms_out": n_out, "array_size": 1, "parallelism": f"replicas x{ws}",
-                   "l2": "flushed between steps (256 MB write outside the step events); "
-                         "step working set 0.6 GB > 126 MB L2",
-                   "tuned": {"radix_items": best_items,
-                             "trials_ms_per_step": dict(zip(("8", "12", "16"), tune_ms))}},
+        "config": product_config(ws, n, m),
+        "result": {"terms_out": n_out},
+        "tuned": {"radix_items": best_items,
+                  "trials_ms_per_step": dict(zip(("8", "12", "16"), tune_ms))},
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d,
                 "d2h_bytes_per_step": int(statistics.mean(d2h)),
                 "path": "pinned host planes -> H2D -> pl_multiply_collate (C ABI) -> D2H of "
@@ -378,60 +413,257 @@ def run_product_collate(args, rank, local, ws):
         "clocks": clk.summary(),
     }
     if ws == 1 and rank == 0 and not args.no_cpu_baseline:
-        line["cpu_baseline"] = cpu_baseline_product()
+        line["cpu_baseline"], ref = cpu_baseline_product()
+        line["parity"] = product_parity(out, n_out, ref)
+    if ws == 1 and not args.no_extras:
+        line["gpu_comparator"] = gpu_comparator(da, db, n, m, stream)
+        del out, dev_out, ea, eb, host_out
+        torch.cuda.empty_cache()
+        line["propagation"] = propagation_extra(args, peak)
+        line["served"] = served_extra(args)
     return line
 
 
 def cpu_baseline_product(reps=3):
     """The reference build (oracle/_ref, OpenMP, all host threads) on the
-    full product + canonicalize, `reps` times."""
+    full product + canonicalize, `reps` times; also returns its result (the
+    parity check of the timed output)."""
     from oracle.oracle import Reference
     R = Reference()
     a, b = product_workload(seed=1)
     R.multiply_canonicalize(a, b)  # warm
     t0 = time.perf_counter()
     for _ in range(reps):
-        R.multiply_canonicalize(a, b)
+        ref = R.multiply_canonicalize(a, b)
     dt = time.perf_counter() - t0
-    return {"value": reps * a.n * b.n / dt, "unit": UNIT, "cores": R.threads,
-            "kind": "reference",
-            "sample": f"{reps} x full 4096x4096 multiply + canonicalize "
-                      f"({dt:.1f} s, {os.path.basename(R.path)})"}
+    return ({"value": reps * a.n * b.n / dt, "unit": UNIT, "cores": R.threads,
+             "kind": "reference", "cpu": host_cpu(),
+             "sample": f"{reps} x full 4096x4096 multiply + canonicalize "
+                       f"({dt:.1f} s, {os.path.basename(R.path)})"}, ref)
+
+
+def product_parity(out, n_out, ref):
+    """The device-timed step's output against the reference build's result
+    on the same operands: strings, phases and order exact; coefficients
+    within 1e-12 relative of max(|c|, 1) (the reference's -ffast-math build
+    reassociates its segment sums)."""
+    import numpy as np
+    got = out.to_host(n_out)
+    keys = (n_out == ref.n and np.array_equal(got[0], ref.x) and np.array_equal(got[1], ref.z)
+            and np.array_equal(got[2], ref.flags))
+    rel = float((np.abs(got[3] - ref.val) / np.maximum(np.abs(ref.val), 1.0)).max()) \
+        if keys and n_out else None
+    ok = bool(keys and rel is not None and rel <= 1e-12)
+    return {"vs": "reference build (oracle/_ref) on the rank-0 operands", "ok": ok,
+            "terms": int(n_out), "reference_terms": int(ref.n), "strings_exact": bool(keys),
+            "max_rel_err": rel, "tolerance": "1e-12 of max(|c|, 1)"}
+
+
+def gpu_comparator(da, db, n, m, stream, reps=10):
+    """The reference's own CUDA kernels (baseline/_ref/libpaulib_refgpu.so:
+    src/gpu/gpu_mul.cu and gpu_commutator.cu built unchanged for sm_100a by
+    baseline/Makefile) against this library's drop-ins with the same C
+    signatures, on the same device operands, CUDA-event timed (median of
+    `reps` launches after 3 untimed)."""
+    import torch
+    from paulib_b200 import _abi
+    from paulib_b200 import workloads as W
+    path = os.path.join(ROOT, "baseline", "_ref", "libpaulib_refgpu.so")
+    if not os.path.exists(path):
+        return {"unavailable": "baseline/_ref/libpaulib_refgpu.so not built (make -C baseline)"}
+    R = C.CDLL(path)  # RTLD_LOCAL: its launch_gpu_* stay apart from ours
+    L = _abi.lib()
+    sp = int(stream.cuda_stream)
+    VP = C.c_void_p
+    for lib in (R, L):
+        lib.launch_gpu_mul_soa.restype = None
+        lib.launch_gpu_mul_soa.argtypes = [C.c_int] + [VP] * 12 + [C.c_int, C.c_int, VP]
+        lib.launch_gpu_commutator_soa.restype = None
+        lib.launch_gpu_commutator_soa.argtypes = ([C.c_int, C.c_int] + [VP] * 13 +
+                                                  [C.c_int, C.c_int, C.c_longlong, VP])
+
+    def timeit(fn, pre=None):
+        for _ in range(3):
+            if pre:
+                pre()
+            fn()
+        ts = []
+        for _ in range(reps):
+            if pre:
+                pre()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            fn()
+            e1.record(stream)
+            torch.cuda.synchronize()
+            ts.append(e0.elapsed_time(e1))
+        return statistics.median(ts)
+
+    res = {"reference_build": "src/gpu/gpu_mul.cu + gpu_commutator.cu, nvcc "
+                              "-gencode arch=compute_100a,code=sm_100a --use_fast_math -O3"}
+    # outer product, 4096 x 4096 at AS = 1 (the reference's launcher needs
+    # only n*m output slots; its kernel writes one term per pair)
+    prod = _abi.DeviceSum(1, n * m)
+    same = True
+    outs = {}
+    for name, lib in (("reference", R), ("ours", L)):
+        t = timeit(lambda lib=lib: lib.launch_gpu_mul_soa(1, *da.ptrs(), *db.ptrs(),
+                                                          *prod.ptrs(), n, m, sp))
+        outs[name] = t
+        h = prod.val[: n * m].clone()
+        if name == "reference":
+            ref_val = h
+        else:
+            same = bool(torch.equal(ref_val, h))
+    res["multiply"] = {"shape": f"{n} x {m}, array_size 1", "reference_ms": outs["reference"],
+                       "ours_ms": outs["ours"], "speedup": outs["reference"] / outs["ours"],
+                       "products_per_s_ours": n * m / (outs["ours"] / 1e3),
+                       "write_gbs_ours": n * m * 25 / (outs["ours"] / 1e3) / 1e9,
+                       "values_identical": same}
+    del prod, ref_val, h
+    # commutator, 16384 x 16384 at 256 qubits (AS = 4): the reference's
+    # kernel claims output slots with an unchecked atomic counter, so its
+    # output planes get the only capacity that is safe by construction, n*m
+    a, b = W.window_sums(seed=3)
+    ca = _abi.DeviceSum.from_host(a.x, a.z, a.flags, a.val)
+    cb = _abi.DeviceSum.from_host(b.x, b.z, b.flags, b.val)
+    cap = a.n * b.n
+    try:
+        big = _abi.DeviceSum(4, cap)
+    except RuntimeError as e:  # allocation
+        res["commutator"] = {"unavailable": f"n*m output planes: {e}"}
+        return res
+    cnt = torch.zeros(1, dtype=torch.int64, device="cuda")
+    counts = {}
+    for name, lib in (("reference", R), ("ours", L)):
+        t = timeit(lambda lib=lib: lib.launch_gpu_commutator_soa(
+            4, 0, *ca.ptrs(), *cb.ptrs(), *big.ptrs(), cnt.data_ptr(), a.n, b.n, cap, sp),
+            pre=cnt.zero_)
+        outs[name] = t
+        counts[name] = int(cnt.item())
+    res["commutator"] = {"shape": f"{a.n} x {b.n}, array_size 4 (256 qubits, windowed)",
+                         "reference_ms": outs["reference"], "ours_ms": outs["ours"],
+                         "speedup": outs["reference"] / outs["ours"],
+                         "pairs_per_s_ours": a.n * b.n / (outs["ours"] / 1e3),
+                         "emitted": counts["ours"],
+                         "emitted_equal": counts["ours"] == counts["reference"],
+                         "note": "ours includes its stream-ordered look-back scratch "
+                                 "(allocate, clear, free) and emits in deterministic order"}
+    del big
+    torch.cuda.empty_cache()
+    return res
+
+
+def propagation_extra(args, peak):
+    """Propagation (sum_i Z_i, 64 qubits, 20 layers): GPU timing with the
+    gate-log rooflines, plus the reference build timed on a prefix of the
+    circuit beside the GPU on the same prefix."""
+    from paulib_b200 import benchmarks
+    from paulib_b200 import propagation as PR
+    from paulib_b200 import workloads as W
+    out = benchmarks.propagation_summary(steps=3, warmup=2, peak_gbs=peak)
+    if args.no_cpu_baseline:
+        return out
+    from oracle.oracle import Reference
+    from paulib_b200.planes import Planes
+    layers = int(args.prop_cpu_layers)
+    obs, circ, tr = W.heisenberg_workload(seed=2, num_qubits=64, layers=20)
+    sub = benchmarks.sub_circuit(circ, layers)
+    R = Reference()
+    r = sub.rotations
+    t0 = time.perf_counter()
+    ref = R.propagate(Planes(obs.x, obs.z, obs.flags, obs.val), Planes(r.x, r.z, r.flags, r.val),
+                      sub.ops, max_weight=tr["max_weight"], cutoff=tr["cutoff"])
+    cpu_s = time.perf_counter() - t0
+    import torch
+    with PR.State(1, 1 << 20) as st:
+        st.upload(obs.x, obs.z, obs.flags, obs.val)
+        st.propagate(r.x, r.z, r.flags, r.val, sub.ops, tr["max_weight"], tr["cutoff"])
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        st.upload(obs.x, obs.z, obs.flags, obs.val)
+        st.propagate(r.x, r.z, r.flags, r.val, sub.ops, tr["max_weight"], tr["cutoff"])
+        e1.record()
+        torch.cuda.synchronize()
+        gpu_ms = e0.elapsed_time(e1)
+        same = st.size() == ref.n
+    out["cpu_baseline"] = {"value": 1.0 / cpu_s, "unit": "propagations/s of the prefix",
+                           "cores": R.threads, "kind": "reference", "cpu": host_cpu(),
+                           "sample": f"the first {layers} of the 20 layers "
+                                     f"({r.n} rotations): {cpu_s:.2f} s; the GPU on the same "
+                                     f"prefix {gpu_ms:.2f} ms",
+                           "gpu_ms_same_prefix": gpu_ms,
+                           "speedup_same_prefix": cpu_s * 1e3 / gpu_ms,
+                           "terms_equal": bool(same)}
+    return out
+
+
+def served_extra(args):
+    """Served stream (Poisson arrivals of mixed-batch jobs + one heavy job)
+    against plain FIFO service at the same arrivals."""
+    from paulib_b200 import benchmarks
+    ns = argparse.Namespace(serve_jobs=args.serve_jobs, serve_lanes=args.serve_lanes,
+                            serve_load=args.serve_load)
+    line = benchmarks.run("serve", ns, 0, torch_local_rank(), 1)
+    c = line["config"]
+    return {"workload": c["workload"], "jobs": c["jobs"], "value": line["value"],
+            "unit": line["unit"], "arrival_rate_per_s": c["arrival_rate_per_s"],
+            "offered_load_vs_plain": c["offered_load_vs_plain"], "lanes": c["lanes"],
+            "latency": c["latency"], "plain_fifo": {"value": c["plain_fifo_value"],
+                                                    "latency": c["plain_fifo_latency"]},
+            "speedup_vs_plain_fifo": line["value"] / c["plain_fifo_value"],
+            "results_identical": c["results_identical"],
+            "peak_device_gb": c["peak_device_gb"]}
+
+
+def torch_local_rank():
+    return int(os.environ.get("LOCAL_RANK", "0"))
 
 
 def run_reference(args, rank, ws):
-    """Reference arm: the reference's CPU implementation, all host threads."""
+    """Reference arm: the reference's CPU implementation (oracle/_ref, its
+    own header-only code with its flags), all host threads, on the same
+    workload and config as our arm.  Each step is the full 4096 x 4096
+    product + canonicalize unless the whole run would exceed a few minutes;
+    then each step takes the same row subset of the rhs (stated in
+    cpu_baseline.sample), and products/s is counted over the rows done."""
     if rank != 0:
         return None
-    from oracle.oracle import Planes, Reference
+    from oracle.oracle import Reference
+    from paulib_b200.planes import Planes
     R = Reference()
     a, b = product_workload(seed=1)
-    total_budget = 90.0  # seconds for warm-up + timed steps
-    rows = 256
-    sub = lambda r: Planes(b.x[:, :r], b.z[:, :r], b.flags[:r], b.val[:r])  # noqa: E731
+    budget_s = 240.0
     t0 = time.perf_counter()
-    R.multiply_canonicalize(a, sub(rows))
-    t1 = time.perf_counter() - t0
-    per_step = total_budget / max(1, args.steps + args.warmup)
-    rows = int(max(16, min(b.n, rows * per_step / max(t1, 1e-3))))
-    for _ in range(args.warmup):
-        R.multiply_canonicalize(a, sub(rows))
+    R.multiply_canonicalize(a, b)  # first warm-up step doubles as the size probe
+    t_full = time.perf_counter() - t0
+    rows = b.n
+    if t_full * (args.steps + args.warmup) > budget_s:
+        rows = int(max(64, b.n * budget_s / (t_full * (args.steps + args.warmup))))
+    sub = Planes(b.x[:, :rows], b.z[:, :rows], b.flags[:rows], b.val[:rows])
+    for _ in range(args.warmup - 1):
+        R.multiply_canonicalize(a, sub)
     t0 = time.perf_counter()
     for _ in range(args.steps):
-        R.multiply_canonicalize(a, sub(rows))
+        R.multiply_canonicalize(a, sub)
     dt = time.perf_counter() - t0
     value = args.steps * a.n * rows / dt
+    sample = ("per step: the full 4096 x 4096 product + canonicalize" if rows == b.n else
+              f"per step: 4096 x {rows} product + canonicalize (the first {rows} rhs rows; "
+              f"the full step takes {t_full:.2f} s here)")
     return {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": 1e3 * dt / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "u64 keys / f64 coefficients",
-        "data": "synthetic, seeded (numpy PCG64)", "impl": "reference",
-        "config": {"workload": "product_collate: PauliSum<64,double> 4096 x 4096 product + "
-                               "canonicalize, 20 active qubits, weight U{1..4}",
-                   "parallelism": "host OpenMP"},
+        "data": "synthetic, seeded (numpy PCG64); shapes and distributions of the "
+                "product+collate benchmark",
+        "impl": "reference", "config": product_config(ws),
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": R.threads, "kind": "reference",
-                         "sample": f"per step: 4096 x {rows} product + canonicalize "
-                                   f"(a row subset of the 4096 x 4096 workload)"},
+                         "cpu": host_cpu(), "sample": sample,
+                         "build": os.path.basename(R.path)},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
 
@@ -452,6 +684,12 @@ def main(argv=None):
     ap.add_argument("--serve-load", type=float, default=1.2,
                     help="serve workload: arrival rate as a multiple of the plain path's capacity")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="product_collate: skip the GPU comparator, propagation and served "
+                         "sub-objects")
+    ap.add_argument("--prop-cpu-layers", type=int, default=6,
+                    help="propagation sub-object: layers of the circuit prefix the reference "
+                         "build is timed on")
     args = ap.parse_args(argv)
     if args.warmup < 3:
         ap.error("--warmup must be >= 3")

@@ -45,6 +45,7 @@ extern "C" {
 #define PL_ERR_CAPACITY 5      /* output would exceed the stated capacity   */
 #define PL_ERR_UNSUPPORTED 6   /* valid request outside what is built       */
 #define PL_ERR_INTERNAL 7      /* device-side consistency check failed      */
+#define PL_ERR_CANCELLED 8     /* the caller's cancel flag stopped the work */
 
 #define PL_MAX_ARRAY_SIZE 16
 
@@ -325,6 +326,11 @@ PL_API int pl_propagate(pl_state* state, const uint64_t* rot_x, const uint64_t* 
                               circuit reversed); other ops record zeros.  For byte models;
                               no counterpart in the reference. */
 PL_API int pl_state_set_option(pl_state* state, int option, int64_t value);
+/* Cancellation: while `flag` (host memory, or NULL to clear) is non-zero,
+ * pl_propagate stops between gates -- it drains the work already queued
+ * and returns PL_ERR_CANCELLED, leaving the state holding the sum after
+ * the last gate that ran. */
+PL_API int pl_state_set_cancel_flag(pl_state* state, const int32_t* flag);
 /* Copy the gate log of the state's last pl_propagate (PL_OPT_GATE_LOG):
  * min(max_ops, *n_ops) triples into sizes[3*q .. 3*q+2]; synchronous. */
 PL_API int pl_state_gate_log(pl_state* state, int64_t* sizes, int64_t max_ops,
@@ -377,6 +383,8 @@ typedef struct {
     int64_t n_ops;
     pl_truncation trunc;
     double arrival_s;            /* pl_serve: seconds after its start the job arrives */
+    const int32_t* cancel;       /* host flag or NULL: once non-zero, the job stops between
+                                    gates (or does not start) with PL_ERR_CANCELLED */
 } pl_job;
 
 typedef struct {
@@ -403,9 +411,29 @@ typedef struct {
 typedef struct {
     double wall_s;
     uint64_t peak_bytes;         /* peak of the budgeted bytes */
-    uint64_t budget_waits;       /* times a lane waited for memory */
-    uint64_t jobs_failed;
+    uint64_t budget_waits;       /* times a lane waited for memory (admission or growth) */
+    uint64_t jobs_failed;        /* jobs that ended with a status other than PL_OK */
+    uint64_t jobs_rejected;      /* jobs refused at admission (PL_ERR_OOM, never started) */
+    uint64_t admission_waits;    /* jobs deferred at admission until memory freed up */
 } pl_batch_stats;
+
+/* Admission estimate of one job (host-only arithmetic, no device work):
+ * *terms bounds the terms its canonical sum can hold after any truncation
+ * step, the least of
+ *   (a) the Frobenius bound 2 * (sum |c|)^2 / cutoff^2: conjugation by the
+ *       circuit keeps ||O||_F, truncation only removes terms, and every kept
+ *       term has |c| >= cutoff (x2 for the two phases of one string);
+ *   (b) the weight bound 2 * sum_{k <= min(w, s)} C(s, k) 3^k over the s
+ *       qubits of the observable's light cone (its support grown through the
+ *       circuit's two-qubit gates, walked in Heisenberg order);
+ * and *bytes = 20 * S * terms + 64 MiB: the five term buffers of a state
+ * (S = 16*AS + 9 bytes per term) at up to twice the live terms before a
+ * truncation and twice again after a capacity doubling, plus workspace.
+ * Saturates at UINT64_MAX.  pl_serve and pl_batch_propagate reserve
+ * min(bytes, budget / lanes) (at least a fresh state's size) when they
+ * admit the job, and refuse a job whose fresh state alone exceeds the
+ * budget. */
+PL_API int pl_job_estimate(const pl_job* job, uint64_t* terms, uint64_t* bytes);
 
 /* All jobs available at once. */
 PL_API int pl_batch_propagate(const pl_job* jobs, int64_t count, const pl_batch_opts* opts,
@@ -426,8 +454,25 @@ PL_API int pl_serve(const pl_job* jobs, int64_t count, const pl_batch_opts* opts
  * segment sums.  0 (default) or 1: used where it fits; -1: never (the
  * general key + payload sort).  Results are identical either way. */
 #define PL_TUNE_INDEX_KEYS 2
+/* Polls a cross-CTA wait (decoupled look-back) makes before it records
+ * PL_ERR_TIMEOUT and returns: 1 .. 2^30, 0 = the default 2^20 (with a 64 ns
+ * back-off past 64 polls: well under a second).  Written into the device
+ * code of the current device; set it again after switching devices. */
+#define PL_TUNE_SPIN_LIMIT 3
+/* Host-side fault injection: value k > 0 makes the k-th following device
+ * allocation of the library fail as if the device were out of memory (the
+ * call then reports PL_ERR_OOM); the injection is then spent.  0 = off. */
+#define PL_TUNE_FAIL_ALLOC 4
 PL_API int pl_set_tuning(int key, int64_t value);
 PL_API int pl_get_tuning(int key, int64_t* value);
+
+/* Runs one decoupled look-back wait on a predecessor tile that never
+ * publishes (a flag that nothing sets) and stores the status the kernel
+ * recorded in *device_status: PL_ERR_TIMEOUT once PL_TUNE_SPIN_LIMIT polls
+ * have run out.  Shows on a live device that the library's cross-CTA waits
+ * end and leave the context usable.  Synchronous.  No counterpart in the
+ * reference (whose kernels do not wait across CTAs). */
+PL_API int pl_check_bounded_wait(int* device_status);
 
 /* ---- measurement hooks ------------------------------------------------ */
 

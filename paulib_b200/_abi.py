@@ -26,6 +26,7 @@ PL_ERR_CUDA = 4
 PL_ERR_CAPACITY = 5
 PL_ERR_UNSUPPORTED = 6
 PL_ERR_INTERNAL = 7
+PL_ERR_CANCELLED = 8
 PL_COLLATE_CANONICALIZE = 0
 PL_COLLATE_SORT_AND_COMBINE = 1
 UINT64_MAX = (1 << 64) - 1
@@ -47,7 +48,8 @@ EXPORTS = (
     "pl_set_tuning", "pl_get_tuning", "pl_state_apply_clifford", "pl_state_apply_rotation_gate",
     "pl_state_basis_state_expectation", "pl_state_trace", "pl_state_frobenius_norm2",
     "pl_state_lookup", "pl_state_trace_product", "pl_state_shard_pack", "pl_state_shard_unpack",
-    "pl_state_count_above", "pl_state_max_abs", "pl_state_gate_log",
+    "pl_state_count_above", "pl_state_max_abs", "pl_state_gate_log", "pl_job_estimate",
+    "pl_state_set_cancel_flag", "pl_check_bounded_wait",
 )
 PL_OP_CLIFFORD = 100
 GATES = {"H": 1, "S": 2, "H_YZ": 3, "H_XY": 4, "SQRT_X": 5, "SQRT_Y": 6, "X": 7, "Y": 8,
@@ -55,6 +57,8 @@ GATES = {"H": 1, "S": 2, "H_YZ": 3, "H_XY": 4, "SQRT_X": 5, "SQRT_Y": 6, "X": 7,
          "YC_X": 17, "YC_Y": 18, "YC_Z": 19, "SWAP": 20, "ISWAP": 21}
 PL_TUNE_RADIX_ITEMS = 1
 PL_TUNE_INDEX_KEYS = 2
+PL_TUNE_SPIN_LIMIT = 3
+PL_TUNE_FAIL_ALLOC = 4
 PL_OPT_GRAPHS = 1
 PL_OPT_GATE_LOG = 2
 PL_ORDER_GIVEN = 0
@@ -75,7 +79,8 @@ class Job(C.Structure):
     _fields_ = [("array_size", C.c_int32), ("obs_x", VP), ("obs_z", VP), ("obs_flags", VP),
                 ("obs_val", VP), ("obs_n", I64), ("rot_x", VP), ("rot_z", VP),
                 ("rot_flags", VP), ("rot_theta", VP), ("n_rot", I64), ("ops", VP),
-                ("n_ops", I64), ("trunc", Truncation), ("arrival_s", C.c_double)]
+                ("n_ops", I64), ("trunc", Truncation), ("arrival_s", C.c_double),
+                ("cancel", VP)]
 
 
 class JobResult(C.Structure):
@@ -90,7 +95,8 @@ class BatchOpts(C.Structure):
 
 class BatchStats(C.Structure):
     _fields_ = [("wall_s", C.c_double), ("peak_bytes", C.c_uint64),
-                ("budget_waits", C.c_uint64), ("jobs_failed", C.c_uint64)]
+                ("budget_waits", C.c_uint64), ("jobs_failed", C.c_uint64),
+                ("jobs_rejected", C.c_uint64), ("admission_waits", C.c_uint64)]
 
 
 class PLError(RuntimeError):
@@ -167,6 +173,10 @@ def lib():
         "pl_state_count_above": (I32, [VP, C.c_double, C.POINTER(I64)]),
         "pl_state_max_abs": (I32, [VP, C.POINTER(C.c_double)]),
         "pl_state_gate_log": (I32, [VP, VP, I64, C.POINTER(I64)]),
+        "pl_job_estimate": (I32, [C.POINTER(Job), C.POINTER(C.c_uint64),
+                                  C.POINTER(C.c_uint64)]),
+        "pl_state_set_cancel_flag": (I32, [VP, VP]),
+        "pl_check_bounded_wait": (I32, [C.POINTER(C.c_int)]),
         "pl_state_apply_rotation_gate": (I32, [VP, I32, I32, C.c_double]),
         "pl_set_tuning": (I32, [I32, I64]),
         "pl_get_tuning": (I32, [I32, C.POINTER(I64)]),

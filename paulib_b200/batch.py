@@ -25,11 +25,16 @@ def _p(a):
 
 
 class JobSet:
-    """ctypes job array over workloads.Instance objects (arrays kept alive)."""
+    """ctypes job array over workloads.Instance objects (arrays kept alive).
+
+    ``cancel`` is an int32 array, one flag per job: setting flag i to a
+    non-zero value (from any host thread, at any time) makes job i stop
+    between gates -- or not start -- with PL_ERR_CANCELLED."""
 
     def __init__(self, instances, arrivals=None):
         self.instances = list(instances)
         self._keep = []
+        self.cancel = np.zeros(max(len(self.instances), 1), np.int32)
         self.jobs = (_abi.Job * max(len(self.instances), 1))()
         for i, inst in enumerate(self.instances):
             obs, circ = inst.observable, inst.circuit
@@ -56,6 +61,14 @@ class JobSet:
             j.trunc.coefficient_cutoff = float(inst.cutoff or 0.0)
             j.trunc.max_terms = U64_MAX
             j.arrival_s = 0.0 if arrivals is None else float(arrivals[i])
+            j.cancel = self.cancel[i:].ctypes.data_as(C.c_void_p)
+
+    def estimate(self, i: int):
+        """(terms, bytes) admission estimate of job i (pl_job_estimate)."""
+        t, b = C.c_uint64(), C.c_uint64()
+        _abi.check(_abi.lib().pl_job_estimate(C.byref(self.jobs[i]), C.byref(t), C.byref(b)),
+                   "pl_job_estimate")
+        return t.value, b.value
 
     def __len__(self):
         return len(self.instances)
@@ -72,6 +85,8 @@ class BatchResult:
     wall_s: float
     peak_bytes: int
     budget_waits: int
+    rejected: int = 0
+    admission_waits: int = 0
 
 
 def _opts(lanes, graphs, order, hbm_budget, keep_bytes):
@@ -89,7 +104,8 @@ def _collect(res, n, st) -> BatchResult:
     g = lambda f, dt: np.array([getattr(res[i], f) for i in range(n)], dt)
     return BatchResult(g("expectation", np.float64), g("final_terms", np.int64),
                        g("status", np.int32), g("lane", np.int32), g("start_s", np.float64),
-                       g("end_s", np.float64), st.wall_s, st.peak_bytes, st.budget_waits)
+                       g("end_s", np.float64), st.wall_s, st.peak_bytes, st.budget_waits,
+                       st.jobs_rejected, st.admission_waits)
 
 
 def _run(fn, js: JobSet, opts, check: bool) -> BatchResult:

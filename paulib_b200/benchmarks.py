@@ -102,6 +102,135 @@ def _propagation(args, rank, ws):
             "gpu_launches": int(launches // steps)}
 
 
+def sub_circuit(circ: W.Circuit, layers: int) -> W.Circuit:
+    """The first `layers` brickwork layers of a circuit (its ops and the
+    rotations they use)."""
+    n = circ.num_qubits
+    per_layer = 2 * n  # rotations per layer (RX and RZ on every qubit)
+    keep = [row for row in circ.ops
+            if row[0] != W.OP_ROT or int(row[1]) < layers * per_layer]
+    # CNOT rows of later layers come after the last kept rotation
+    last = max(i for i, row in enumerate(keep) if row[0] == W.OP_ROT)
+    ops = np.asarray(keep[: last + 1], np.int32).reshape(-1, 3)
+    r = circ.rotations
+    m = layers * per_layer
+    rot = W.SoA(r.x[:, :m].copy(), r.z[:, :m].copy(), r.flags[:m].copy(), r.val[:m].copy(), n)
+    return W.Circuit(rot, ops, n, {"layers": layers})
+
+
+def propagation_bytes(log: np.ndarray, ops_reversed: np.ndarray, array_size: int,
+                      n_obs: int) -> dict:
+    """Byte models of one propagation from its gate log (terms in m,
+    anticommuting k, terms out per rotation, processing order).
+
+    design: the merge path's own traffic -- k_expand reads m terms and
+    writes k children, the run merge reads and writes k, k_merge_reduce
+    reads m + k and writes the out survivors: S*(2m + 4k + out) per
+    rotation; a CNOT layer reads and writes the x, z and flags planes of
+    its m terms.  survey: the reference algorithm's per-gate model,
+    m*S + (m+k)*S + B_canon(m+k, out, b) with b = 2*64*AS + 1 key bits."""
+    S = 16 * array_size + 9
+    design = 0
+    survey = 0
+    b = 2 * 64 * array_size + 1
+    kb = 8 * ((b + 63) // 64)
+    passes = (b + 7) // 8
+    size = n_obs
+    prev_cnot = False
+    for q, row in enumerate(ops_reversed):
+        if row[0] == W.OP_ROT:
+            m, k, out = (int(v) for v in log[q])
+            if m == 0 and k == 0 and out == 0:
+                continue
+            design += S * (2 * m + 4 * k + out)
+            survey += m * S + (m + k) * S + (m + k) * S + passes * (m + k) * 2 * (kb + 4) \
+                + out * S
+            size = out
+            prev_cnot = False
+        else:
+            if not prev_cnot:
+                design += 2 * (16 * array_size + 1) * size
+            prev_cnot = True
+    rows = log[log[:, 0] > 0]
+    return {"design_bytes": int(design), "survey_bytes": int(survey),
+            "rotations_logged": int(rows.shape[0]),
+            "sum_m": int(rows[:, 0].sum()), "sum_k": int(rows[:, 1].sum()),
+            "sum_out": int(rows[:, 2].sum()), "peak_terms": int(rows[:, 0].max(initial=0))}
+
+
+def propagation_summary(seed=2, num_qubits=64, layers=20, steps=3, warmup=2, peak_gbs=None):
+    """One propagation of sum_i Z_i through the brickwork circuit (cutoff 1e-4,
+    max weight 8), CUDA-event timed per propagation (upload through
+    zero_state_expectation), with graph replay autotuned, the gate log of an
+    untimed run and the byte-model rooflines."""
+    import torch
+    obs, circ, tr = W.heisenberg_workload(seed=seed, num_qubits=num_qubits, layers=layers)
+    r = circ.rotations
+    st = PR.State(obs.array_size, 1 << 24)
+
+    def once():
+        st.upload(obs.x, obs.z, obs.flags, obs.val)
+        st.propagate(r.x, r.z, r.flags, r.val, circ.ops, tr["max_weight"], tr["cutoff"])
+        return st.zero_state_expectation()
+
+    def timed():
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        e = once()
+        e1.record()
+        _sync()
+        return e0.elapsed_time(e1), e
+
+    trial = {}
+    for g in (False, True):
+        st.use_graphs(g)
+        once()
+        _sync()
+        trial[g] = timed()[0]
+    graphs = min(trial, key=trial.get)
+    st.use_graphs(graphs)
+    for _ in range(max(1, warmup)):
+        once()
+    _sync()
+    times, e = [], None
+    for _ in range(max(1, steps)):
+        t, e = timed()
+        times.append(t)
+    final = st.size()
+    # sizes per gate from an untimed run with the log on
+    st.log_gates(True)
+    once()
+    log = st.gate_log()
+    st.log_gates(False)
+    st.close()
+    ms = float(np.median(times))
+    bm = propagation_bytes(log, circ.ops[::-1], obs.array_size, obs.n)
+    out = {"workload": f"sum_i Z_i, {num_qubits} qubits, {layers} brickwork layers CNOT+RX+RZ, "
+                       f"cutoff {tr['cutoff']:g}, max_weight {tr['max_weight']}",
+           "ms_per_propagation": ms, "value": 1e3 / ms, "unit": "propagations/s",
+           "steps": len(times), "final_terms": final, "expectation": e,
+           "graphs": graphs, "trials_ms": {"graphs_off": trial[False], "graphs_on": trial[True]},
+           "gate_counts": {k: bm[k] for k in ("rotations_logged", "sum_m", "sum_k", "sum_out",
+                                              "peak_terms")}}
+    if peak_gbs:
+        gbs = bm["design_bytes"] / (ms / 1e3) / 1e9
+        out["roofline"] = {
+            "bound": "hbm", "unit": "GB/s", "peak": peak_gbs,
+            "bytes_model": "per rotation S*(2m + 4k + out) (expand, run merge, merge-reduce), "
+                           "per CNOT layer 2*(16*AS+1)*m; S = 16*AS + 9; sums over the logged "
+                           "(m, k, out); re-sorts after CNOT layers not counted",
+            "bytes_per_propagation": bm["design_bytes"], "achieved": gbs,
+            "frac": gbs / peak_gbs}
+        sgbs = bm["survey_bytes"] / (ms / 1e3) / 1e9
+        out["survey_byte_model"] = {
+            "bytes_model": "per rotation m*S + (m+k)*S + B_canon(m+k, out, b=129): the "
+                           "reference algorithm's append + full sort per gate",
+            "bytes_per_propagation": bm["survey_bytes"], "equivalent_gbs": sgbs,
+            "equivalent_frac": sgbs / peak_gbs}
+    return out
+
+
 def _commutator(args, rank, ws):
     import torch
     a, b = W.window_sums(seed=3 + rank)

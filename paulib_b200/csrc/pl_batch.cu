@@ -19,6 +19,7 @@
 
 #include <algorithm>
 #include <atomic>
+#include <cmath>
 #include <chrono>
 #include <condition_variable>
 #include <mutex>
@@ -37,6 +38,89 @@ namespace {
 
 using Clock = std::chrono::steady_clock;
 
+// Terms a lane's state is created with (and the floor of every admission
+// reserve: a fresh state's five buffers).
+constexpr int64_t kFreshTerms = 1 << 16;
+
+size_t term_bytes(int as) { return (size_t)(16 * as + 9); }
+size_t fresh_bytes(const pl_job& j) {
+    const int64_t n = std::max<int64_t>(j.obs_n, kFreshTerms);
+    return 5 * term_bytes(j.array_size) * (size_t)n;
+}
+
+// Qubits of the observable's light cone: its support, grown through every
+// multi-qubit generator and two-qubit gate it meets, walking the circuit in
+// Heisenberg order (last op first).  Single-qubit rotations cannot add a
+// qubit: a term only branches when it anticommutes with the generator, i.e.
+// already acts on the generator's qubit.
+int light_cone(const pl_job& j) {
+    const int nq = 64 * j.array_size;
+    std::vector<char> in(nq, 0);
+    auto add_words = [&](const uint64_t* x, const uint64_t* z, int64_t stride, int64_t t) {
+        for (int k = 0; k < j.array_size; ++k) {
+            const uint64_t w = x[(size_t)k * stride + t] | z[(size_t)k * stride + t];
+            for (int b = 0; b < 64; ++b)
+                if ((w >> b) & 1ull) in[64 * k + b] = 1;
+        }
+    };
+    auto touches = [&](const uint64_t* x, const uint64_t* z, int64_t stride, int64_t t) {
+        for (int k = 0; k < j.array_size; ++k) {
+            const uint64_t w = x[(size_t)k * stride + t] | z[(size_t)k * stride + t];
+            for (int b = 0; b < 64; ++b)
+                if (((w >> b) & 1ull) && in[64 * k + b]) return true;
+        }
+        return false;
+    };
+    for (int64_t t = 0; t < j.obs_n; ++t) add_words(j.obs_x, j.obs_z, j.obs_n, t);
+    auto rotation = [&](int64_t r) {
+        if (r >= 0 && r < j.n_rot && touches(j.rot_x, j.rot_z, j.n_rot, r))
+            add_words(j.rot_x, j.rot_z, j.n_rot, r);
+    };
+    if (!j.ops) {
+        for (int64_t r = j.n_rot; r-- > 0;) rotation(r);
+    } else {
+        for (int64_t l = j.n_ops; l-- > 0;) {
+            const int kind = j.ops[3 * l], a = j.ops[3 * l + 1], b = j.ops[3 * l + 2];
+            if (kind == PL_OP_ROTATION) {
+                rotation(a);
+            } else if (kind == PL_OP_CNOT ||
+                       (kind > PL_OP_CLIFFORD && kind - PL_OP_CLIFFORD >= PL_GATE_CNOT)) {
+                if (a >= 0 && b >= 0 && a < nq && b < nq && (in[a] || in[b])) in[a] = in[b] = 1;
+            }
+        }
+    }
+    int s = 0;
+    for (char c : in) s += c;
+    return s;
+}
+
+// sum_{k <= kmax} C(s, k) 3^k, saturating
+long double weight_bound(int s, uint64_t w) {
+    const int kmax = (int)std::min<uint64_t>((uint64_t)s, w);
+    long double c = 1.0L, sum = 0.0L;
+    for (int k = 0; k <= kmax; ++k) {
+        sum += c;
+        c = c * (long double)(s - k) / (long double)(k + 1) * 3.0L;
+    }
+    return sum;
+}
+
+void estimate(const pl_job& j, uint64_t* terms, uint64_t* bytes) {
+    const long double kMax = 1.8e19L;
+    long double t = 2.0L * weight_bound(light_cone(j), j.trunc.max_weight);
+    const double eps = j.trunc.coefficient_cutoff;
+    if (eps > 0.0) {
+        long double l1 = 0.0L;
+        for (int64_t i = 0; i < j.obs_n; ++i) l1 += std::fabs((long double)j.obs_val[i]);
+        const long double fro = 2.0L * l1 * l1 / ((long double)eps * (long double)eps);
+        t = std::min(t, std::floor(fro));
+    }
+    t = std::max(t, (long double)j.obs_n);
+    const long double b = 20.0L * (long double)term_bytes(j.array_size) * t + 64.0L * 1048576.0L;
+    *terms = t >= kMax ? ~0ull : (uint64_t)t;
+    *bytes = b >= kMax ? ~0ull : (uint64_t)b;
+}
+
 struct Lane {
     cudaStream_t st = nullptr;
     pl_state* state[kMaxAS + 1] = {};
@@ -44,6 +128,9 @@ struct Lane {
 
 struct Shared {
     const pl_job* jobs = nullptr;
+    std::vector<uint64_t> reserve;   // admission reserve per job (bytes)
+    std::atomic<uint64_t> rejected{0};
+    std::atomic<uint64_t> deferred{0};
     std::vector<int64_t> order;  // job indices in dispatch order
     pl_job_result* results = nullptr;
     pl_batch_opts opts{};
@@ -83,13 +170,18 @@ int64_t take_job(Shared& S) {
     return j;
 }
 
+bool cancelled(const pl_job& job) {
+    return job.cancel && *reinterpret_cast<const volatile int32_t*>(job.cancel) != 0;
+}
+
 int run_job(Shared& S, Lane& L, const pl_job& job, pl_job_result& r) {
     const int as = job.array_size;
     if (as < 1 || as > kMaxAS) return PL_ERR_INVALID_ARG;
+    if (cancelled(job)) return PL_ERR_CANCELLED;
     pl_state*& s = L.state[as];
     int rc = PL_OK;
     if (!s) {
-        rc = pl_state_create(&s, as, 1 << 16, L.st);
+        rc = pl_state_create(&s, as, kFreshTerms, L.st);
         if (rc) return rc;
         state_attach_budget(s, &S.budget);
     }
@@ -97,8 +189,10 @@ int run_job(Shared& S, Lane& L, const pl_job& job, pl_job_result& r) {
     if (rc) return rc;
     rc = pl_state_upload(s, job.obs_x, job.obs_z, job.obs_flags, job.obs_val, job.obs_n);
     if (rc) return rc;
+    pl_state_set_cancel_flag(s, job.cancel);
     rc = pl_propagate(s, job.rot_x, job.rot_z, job.rot_flags, job.rot_theta, job.n_rot, job.ops,
                       job.n_ops, &job.trunc);
+    pl_state_set_cancel_flag(s, nullptr);
     if (rc) return rc;
     rc = pl_state_zero_state_expectation(s, &r.expectation);
     if (rc) return rc;
@@ -129,12 +223,22 @@ void lane_main(Shared& S, int lane) {
         if (j == -1) break;
         if (j == -2) continue;
         pl_job_result& r = S.results[j];
-        S.budget.admit();
         r.lane = lane;
+        if (fresh_bytes(S.jobs[j]) > S.budget.limit) {
+            // a fresh state for this job alone exceeds the budget: refused
+            r.start_s = r.end_s = since(S);
+            r.status = PL_ERR_OOM;
+            S.rejected.fetch_add(1);
+            S.failed.fetch_add(1);
+            continue;
+        }
+        const size_t held = lane_bytes(L);
+        const size_t need = S.reserve[(size_t)j] > held ? S.reserve[(size_t)j] - held : 0;
+        if (S.budget.admit(need)) S.deferred.fetch_add(1);
         r.start_s = since(S);
         r.status = L.st ? run_job(S, L, S.jobs[j], r) : PL_ERR_CUDA;
         r.end_s = since(S);
-        S.budget.leave();
+        S.budget.leave(need);
         if (r.status != PL_OK) S.failed.fetch_add(1);
         // give memory back when over the lane's share or when others wait
         bool others_wait;
@@ -176,6 +280,16 @@ int run_all(const pl_job* jobs, int64_t count, const pl_batch_opts* opts, pl_job
     size_t free_b = 0, total_b = 0;
     PL_CUDA_TRY(cudaMemGetInfo(&free_b, &total_b));
     S.budget.limit = opts->hbm_budget ? (size_t)opts->hbm_budget : (size_t)(0.85 * free_b);
+    // admission reserves: the job's estimate, at most a lane's share of the
+    // budget (online growth monitoring covers the rest), at least a fresh
+    // state
+    S.reserve.resize((size_t)count);
+    for (int64_t i = 0; i < count; ++i) {
+        uint64_t t = 0, b = 0;
+        estimate(jobs[i], &t, &b);
+        const size_t share = S.budget.limit / (size_t)opts->lanes;
+        S.reserve[(size_t)i] = std::max(fresh_bytes(jobs[i]), std::min<size_t>(b, share));
+    }
     S.order.resize((size_t)count);
     for (int64_t i = 0; i < count; ++i) S.order[(size_t)i] = i;
     if (serving) {
@@ -205,6 +319,8 @@ int run_all(const pl_job* jobs, int64_t count, const pl_batch_opts* opts, pl_job
         stats->peak_bytes = S.budget.peak;
         stats->budget_waits = S.budget.waits;
         stats->jobs_failed = S.failed.load();
+        stats->jobs_rejected = S.rejected.load();
+        stats->admission_waits = S.deferred.load();
     }
     if (S.failed.load()) return record_status(PL_ERR_INTERNAL, "batch: a job failed (see results)");
     return record_status(PL_OK, nullptr);
@@ -212,6 +328,16 @@ int run_all(const pl_job* jobs, int64_t count, const pl_batch_opts* opts, pl_job
 
 }  // namespace
 }  // namespace pl
+
+extern "C" int pl_job_estimate(const pl_job* job, uint64_t* terms, uint64_t* bytes) {
+    if (!job || !terms || !bytes || job->array_size < 1 || job->array_size > pl::kMaxAS ||
+        job->obs_n < 0 || job->n_rot < 0 || job->n_ops < 0 ||
+        (job->obs_n > 0 && (!job->obs_x || !job->obs_z || !job->obs_val)) ||
+        (job->n_rot > 0 && (!job->rot_x || !job->rot_z)) || (job->n_ops > 0 && !job->ops))
+        return pl::record_status(PL_ERR_INVALID_ARG, "pl_job_estimate");
+    pl::estimate(*job, terms, bytes);
+    return pl::record_status(PL_OK, nullptr);
+}
 
 extern "C" int pl_batch_propagate(const pl_job* jobs, int64_t count, const pl_batch_opts* opts,
                                   pl_job_result* results, pl_batch_stats* stats) {

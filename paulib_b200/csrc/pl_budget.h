@@ -23,6 +23,7 @@ struct MemBudget {
     int holders = 0;
     int waiting = 0;
     unsigned long long waits = 0;
+    size_t reserved = 0;  // admission reserves of the running jobs
 
     // Replace `old_bytes` held by the caller with `new_bytes`.
     void resize(size_t old_bytes, size_t new_bytes) {
@@ -43,21 +44,30 @@ struct MemBudget {
         if (used > peak) peak = used;
         if (new_bytes < old_bytes) cv.notify_all();
     }
-    // A job starts holding memory: wait while the budget is spent by others.
-    void admit() {
+    // A job starts holding memory: it needs `need` more bytes than its lane
+    // already holds (its admission reserve).  Wait while that does not fit
+    // beside the running jobs -- the larger of what they hold and what they
+    // reserved at admission; a job is always admitted when no other job
+    // runs.  Returns whether the job was deferred.
+    bool admit(size_t need = 0) {
         std::unique_lock<std::mutex> lock(mu);
-        bool counted = false;
-        while (used >= limit && holders > 0) {
-            if (!counted) {
+        bool deferred = false;
+        for (;;) {
+            const size_t busy = used > reserved ? used : reserved;
+            if (holders == 0 || (busy < limit && need <= limit - busy)) break;
+            if (!deferred) {
                 ++waits;
-                counted = true;
+                deferred = true;
             }
             cv.wait_for(lock, std::chrono::milliseconds(50));
         }
+        reserved += need;
         ++holders;
+        return deferred;
     }
-    void leave() {
+    void leave(size_t need = 0) {
         std::lock_guard<std::mutex> lock(mu);
+        reserved -= need;
         --holders;
         cv.notify_all();
     }

@@ -558,7 +558,7 @@ __device__ __forceinline__ u32 lb_walk(u32* lb, u32 tile, u32 stride, u32 cnt, i
         if (done) break;
         t -= k;
         if (k == 0) {
-            if (++spins > kSpinLimit) {
+            if (++spins > g_spin_limit) {
                 raise_status(status, PL_ERR_TIMEOUT);
                 break;
             }
@@ -2030,6 +2030,8 @@ bool try_split(const Src& src, u32 n, const u64* orm, const u64* andm, const Col
 }
 
 }  // namespace
+
+PL_SPIN_LIMIT_SETTER(set_spin_limit_collate)
 
 // ---------------------------------------------------------------------------
 int DevArena::ensure(size_t need) {

@@ -21,8 +21,15 @@ using i64 = long long;
 
 constexpr int kMaxAS = 16;
 // Bound on every spin-wait (decoupled look-back): after this many polls a
-// kernel records PL_ERR_TIMEOUT, publishes what it has and moves on.
+// kernel records PL_ERR_TIMEOUT, publishes what it has and moves on.  The
+// bound in force is g_spin_limit (PL_TUNE_SPIN_LIMIT; kSpinLimit by
+// default): every translation unit that waits holds its own copy, which
+// pl_set_tuning writes for the current device through the unit's
+// PL_SPIN_LIMIT_SETTER function.
 constexpr u32 kSpinLimit = 1u << 20;
+static __device__ u32 g_spin_limit = kSpinLimit;
+#define PL_SPIN_LIMIT_SETTER(name) \
+    cudaError_t name(u32 v) { return cudaMemcpyToSymbol(g_spin_limit, &v, sizeof(v)); }
 
 // ---------------------------------------------------------------------------
 // Device status word: the first non-zero code wins.

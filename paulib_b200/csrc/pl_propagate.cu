@@ -155,7 +155,7 @@ __device__ __forceinline__ u64 lookback2(u64* lb, u32 tile, u64 v, int* status) 
         const u64 w = ld_volatile64(lb + t);
         const u64 fl = w >> 62;
         if (fl == 0) {
-            if (++spins > kSpinLimit) {
+            if (++spins > g_spin_limit) {
                 raise_status(status, PL_ERR_TIMEOUT);
                 break;
             }
@@ -195,7 +195,7 @@ __device__ __forceinline__ u64 warp_lookback2(u64* lb, u32 tile, u64 v, int* sta
         const u32 zero = __ballot_sync(0xffffffffu, fl == 0u);
         const u32 upto = pre ? (pre & (0u - pre)) * 2u - 1u : 0xffffffffu;
         if (zero & upto) {
-            if (++spins > kSpinLimit) {
+            if (++spins > g_spin_limit) {
                 if (lane == 0) raise_status(status, PL_ERR_TIMEOUT);
                 break;
             }
@@ -578,7 +578,7 @@ __device__ __forceinline__ u32 lookback1(u32* lb, u32 tile, u32 cnt, int* status
         const u32 w = ld_volatile(lb + t);
         const u32 fl = w >> 30;
         if (fl == 0) {
-            if (++spins > kSpinLimit) {
+            if (++spins > g_spin_limit) {
                 raise_status(status, PL_ERR_TIMEOUT);
                 break;
             }
@@ -618,7 +618,7 @@ __device__ __forceinline__ u32 warp_lookback1(u32* lb, u32 tile, u32 cnt, int* s
         const u32 zero = __ballot_sync(0xffffffffu, fl == 0u);
         const u32 upto = pre ? (pre & (0u - pre)) * 2u - 1u : 0xffffffffu;  // lanes <= first prefix
         if (zero & upto) {
-            if (++spins > kSpinLimit) {
+            if (++spins > g_spin_limit) {
                 if (lane == 0) raise_status(status, PL_ERR_TIMEOUT);
                 break;
             }
@@ -1964,6 +1964,7 @@ struct pl_state {
     i64* d_log = nullptr;
     i64 log_ops = 0;       // ops the log holds
     i64 log_used = 0;      // ops of the last propagation
+    const volatile int32_t* cancel = nullptr;  // pl_state_set_cancel_flag
 };
 
 namespace pl {
@@ -2575,6 +2576,14 @@ int run_ops(pl_state* s, const std::vector<Rot>& rots, const std::vector<Op>& op
         return PL_OK;
     };
     while (i < ops.size()) {
+        if (s->cancel && *s->cancel) {
+            // drain what is queued (a capacity rewind leaves the failing
+            // gate's input in place), then stop between gates
+            bool rw = false;
+            rc = checkpoint(&rw);
+            if (rc) return rc;
+            return record_status(PL_ERR_CANCELLED, "propagate: cancelled");
+        }
         const Op& op = ops[i];
         bool rewound = false;
         if (op.kind == 2) {
@@ -2764,6 +2773,13 @@ extern "C" int pl_state_set_option(pl_state* s, int option, int64_t value) {
     return record_status(PL_ERR_INVALID_ARG, "pl_state_set_option: unknown option");
 }
 
+extern "C" int pl_state_set_cancel_flag(pl_state* s, const int32_t* flag) {
+    int rc = check_state(s);
+    if (rc) return rc;
+    s->cancel = flag;
+    return record_status(PL_OK, nullptr);
+}
+
 extern "C" int pl_state_gate_log(pl_state* s, int64_t* sizes, int64_t max_ops, int64_t* n_ops) {
     int rc = check_state(s);
     if (rc) return rc;
@@ -2788,6 +2804,8 @@ extern "C" int pl_state_memory(pl_state* s, uint64_t* bytes) {
 }
 
 namespace pl {
+PL_SPIN_LIMIT_SETTER(set_spin_limit_propagate)
+
 // Internal hooks of the sharded collate (pl_shard.cu): the current planes of
 // a state, and making room for / setting its term count.
 int state_planes(pl_state* s, u64** x, u64** z, u8** f, double** v, i64* cap, i64* n) {

@@ -187,8 +187,23 @@ static void keep_pool_cached() {
     cudaGetLastError();
     done[dev] = true;
 }
+static std::atomic<long long> g_tuning[8] = {};
+
+// PL_TUNE_FAIL_ALLOC: the k-th allocation from now fails (then the
+// injection is spent).
+static bool injected_alloc_failure() {
+    long long k = g_tuning[PL_TUNE_FAIL_ALLOC].load();
+    while (k > 0 && !g_tuning[PL_TUNE_FAIL_ALLOC].compare_exchange_weak(k, k - 1)) {
+    }
+    return k == 1;
+}
+
 cudaError_t dev_alloc(void** p, size_t bytes, cudaStream_t st) {
     keep_pool_cached();
+    if (injected_alloc_failure()) {
+        *p = nullptr;
+        return cudaErrorMemoryAllocation;
+    }
     std::lock_guard<std::mutex> lock(g_alloc_mu);
     return cudaMallocAsync(p, bytes, st);
 }
@@ -200,7 +215,6 @@ void dev_free(void* p, cudaStream_t st) {
 void capture_lock() { g_alloc_mu.lock(); }
 void capture_unlock() { g_alloc_mu.unlock(); }
 
-static std::atomic<long long> g_tuning[8] = {};
 long long tuning(int key) { return key >= 0 && key < 8 ? g_tuning[key].load() : 0; }
 
 void note_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
@@ -255,6 +269,7 @@ extern "C" const char* pl_status_string(int status) {
         case PL_ERR_CAPACITY: return "output capacity exceeded";
         case PL_ERR_UNSUPPORTED: return "unsupported";
         case PL_ERR_INTERNAL: return "internal consistency check failed";
+        case PL_ERR_CANCELLED: return "cancelled";
         default: return "unknown status";
     }
 }
@@ -339,7 +354,25 @@ extern "C" int pl_profile_report(char* buf, size_t cap) {
     return pl::record_status(out.size() < cap ? PL_OK : PL_ERR_CAPACITY, nullptr);
 }
 
+namespace pl {
+cudaError_t set_spin_limit_collate(u32 v);
+cudaError_t set_spin_limit_propagate(u32 v);
+cudaError_t set_spin_limit_terms(u32 v);
+}  // namespace pl
+
 extern "C" int pl_set_tuning(int key, int64_t value) {
+    if (key == PL_TUNE_SPIN_LIMIT && value >= 0 && value <= (1ll << 30)) {
+        const pl::u32 v = value == 0 ? pl::kSpinLimit : (pl::u32)value;
+        PL_CUDA_TRY(pl::set_spin_limit_collate(v));
+        PL_CUDA_TRY(pl::set_spin_limit_propagate(v));
+        PL_CUDA_TRY(pl::set_spin_limit_terms(v));
+        pl::g_tuning[key].store(value);
+        return pl::record_status(PL_OK, nullptr);
+    }
+    if (key == PL_TUNE_FAIL_ALLOC && value >= 0) {
+        pl::g_tuning[key].store(value);
+        return pl::record_status(PL_OK, nullptr);
+    }
     if (key == PL_TUNE_RADIX_ITEMS && (value == 0 || value == 8 || value == 12 || value == 16)) {
         pl::g_tuning[key].store(value);
         return pl::record_status(PL_OK, nullptr);

@@ -84,7 +84,7 @@ __device__ __forceinline__ u64 lookback64(u64* lb, u32 tile, u64 cnt, u64 init, 
         const u64 w = ld_volatile64(lb + t);
         const u64 fl = w >> 62;
         if (fl == 0) {
-            if (++spins > kSpinLimit) {
+            if (++spins > g_spin_limit) {
                 raise_status(status, PL_ERR_TIMEOUT);
                 break;
             }
@@ -176,6 +176,12 @@ __global__ void __launch_bounds__(kCThreads)
     }
 }
 
+// A look-back wait whose predecessor never publishes: tile 1 polls tile 0's
+// word, which nothing sets, until the spin limit runs out.
+__global__ void k_wait_check(u64* lb, int* status) {
+    if (threadIdx.x == 0) (void)lookback64(lb, 1u, 1ull, 0ull, status);
+}
+
 // ---------------------------------------------------------------------------
 // apply_CNOT: flags ^= (xc & zt & (1 ^ xt ^ zc)) << 1; x_t ^= x_c; z_c ^= z_t.
 // ---------------------------------------------------------------------------
@@ -226,6 +232,8 @@ __global__ void __launch_bounds__(1024) k_zero_state(const u64* __restrict__ x,
 }
 
 }  // namespace
+
+PL_SPIN_LIMIT_SETTER(set_spin_limit_terms)
 
 // ---------------------------------------------------------------------------
 // Host entry points (internal).
@@ -368,6 +376,26 @@ extern "C" int pl_commutator(int array_size, int multiply_by_i, const uint64_t* 
                            (const u64*)lhs_z, lhs_flags, lhs_val, n, n, (const u64*)rhs_x,
                            (const u64*)rhs_z, rhs_flags, rhs_val, m, m, (u64*)out_x,
                            (u64*)out_z, out_flags, out_val, capacity, d_count, true, stream);
+}
+
+extern "C" int pl_check_bounded_wait(int* device_status) {
+    if (!device_status) return record_status(PL_ERR_INVALID_ARG, "pl_check_bounded_wait");
+    void* p = nullptr;
+    PL_CUDA_TRY(cudaMalloc(&p, 256));
+    u64* lb = static_cast<u64*>(p);
+    int* status = reinterpret_cast<int*>(static_cast<unsigned char*>(p) + 128);
+    cudaError_t e = cudaMemset(p, 0, 256);
+    if (e == cudaSuccess) {
+        k_wait_check<<<1, 32>>>(lb, status);
+        note_launch();
+        e = cudaGetLastError();
+    }
+    int st = 0;
+    if (e == cudaSuccess) e = cudaMemcpy(&st, status, sizeof(int), cudaMemcpyDeviceToHost);
+    cudaFree(p);
+    if (e != cudaSuccess) return record_cuda(e);
+    *device_status = st;
+    return record_status(PL_OK, nullptr);
 }
 
 extern "C" int pl_apply_cnot(int array_size, uint64_t* x, uint64_t* z, uint8_t* flags, int64_t n,

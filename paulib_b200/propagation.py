@@ -60,6 +60,15 @@ class State:
                    "pl_state_set_option")
         return self
 
+    def set_cancel_flag(self, flag: "np.ndarray | None"):
+        """Stop propagate() between gates (PL_ERR_CANCELLED) once flag[0]
+        (an int32 array the caller keeps alive) becomes non-zero; None
+        clears it."""
+        self._cancel = flag
+        p = None if flag is None else flag.ctypes.data_as(C.c_void_p)
+        _abi.check(self._lib.pl_state_set_cancel_flag(self._h, p), "pl_state_set_cancel_flag")
+        return self
+
     def log_gates(self, enable: bool = True):
         """Record (terms in, anticommuting terms, terms out) of every
         fast-path rotation of the next propagate() (PL_OPT_GATE_LOG)."""
