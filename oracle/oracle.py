@@ -373,6 +373,16 @@ class Reference(_Impl):
         self._free(hr)
         return self._take(h, p.array_size)
 
+    def random_pauli_sum(self, array_size: int, terms: int, seed: int, num_qubits: int):
+        """random_pauli_sum<64*array_size, double>(terms, seed, num_qubits)."""
+        fn = self.lib.ref_random_pauli_sum
+        fn.restype = C.c_void_p
+        fn.argtypes = [C.c_int, C.c_int64, C.c_uint64, C.c_uint64]
+        h = fn(int(array_size), int(terms), int(seed), int(num_qubits))
+        if not h:
+            raise ValueError(f"unsupported array size {array_size}")
+        return self._take(h, array_size)
+
     # A handle-level multiply+canonicalize without the intermediate round trip,
     # used to time the reference's product+collate path.
     def multiply_canonicalize(self, a, b):

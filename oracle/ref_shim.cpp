@@ -204,6 +204,13 @@ SumBase* make(const u64* x, const u64* z, const u8* f, const double* v, i64 n) {
     return s;
 }
 
+template <std::size_t N>
+SumBase* make_random(i64 terms, u64 seed, u64 num_qubits) {
+    auto* s = new Sum<N>();
+    s->s = paulib::random_pauli_sum<N, double>((std::size_t)terms, seed, (std::size_t)num_qubits);
+    return s;
+}
+
 }  // namespace
 
 extern "C" {
@@ -217,6 +224,16 @@ __attribute__((visibility("default"))) void* ref_sum_new(int as, const u64* x, c
         case 4: return make<256>(x, z, f, v, n);
         case 8: return make<512>(x, z, f, v, n);
         case 16: return make<1024>(x, z, f, v, n);
+        default: return nullptr;
+    }
+}
+// random_pauli_sum (PauliSumUtils.h:114-154) of capacity 64 * as
+__attribute__((visibility("default"))) void* ref_random_pauli_sum(int as, i64 terms, u64 seed,
+                                                                  u64 num_qubits) {
+    switch (as) {
+        case 1: return make_random<64>(terms, seed, num_qubits);
+        case 2: return make_random<128>(terms, seed, num_qubits);
+        case 4: return make_random<256>(terms, seed, num_qubits);
         default: return nullptr;
     }
 }

@@ -387,3 +387,44 @@ def _serve(args, rank, ws):
                        "plain_fifo_value": ws * len(jobs) / span_f,
                        "plain_service_s": service, "results_identical": same,
                        "peak_device_gb": rs.peak_bytes / 1e9}}
+
+
+def main(argv=None) -> int:
+    """A single workload run for profiling:
+
+        python -m paulib_b200.benchmarks propagation [--layers 20] [--graphs 0|1] [--runs 1]
+
+    propagates sum_i Z_i through the 64-qubit brickwork circuit (cutoff
+    1e-4, max weight 8) `runs` times and prints the time of the last run,
+    the final term count and the expectation."""
+    import argparse
+    import json
+    import torch
+    ap = argparse.ArgumentParser(description=main.__doc__.split("\n\n")[0])
+    ap.add_argument("workload", choices=["propagation"])
+    ap.add_argument("--layers", type=int, default=20)
+    ap.add_argument("--graphs", type=int, default=0)
+    ap.add_argument("--runs", type=int, default=1)
+    a = ap.parse_args(argv)
+    torch.cuda.set_device(0)
+    obs, circ, tr = W.heisenberg_workload(seed=2, num_qubits=64, layers=a.layers)
+    r = circ.rotations
+    with PR.State(1, 1 << 24) as st:
+        st.use_graphs(bool(a.graphs))
+        for _ in range(max(1, a.runs)):
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record()
+            st.upload(obs.x, obs.z, obs.flags, obs.val)
+            st.propagate(r.x, r.z, r.flags, r.val, circ.ops, tr["max_weight"], tr["cutoff"])
+            e = st.zero_state_expectation()
+            e1.record()
+            _sync()
+        print(json.dumps({"workload": f"propagation 64 qubits x {a.layers} layers",
+                          "ms": e0.elapsed_time(e1), "final_terms": st.size(),
+                          "expectation": e}))
+    return 0
+
+
+if __name__ == "__main__":
+    raise SystemExit(main())

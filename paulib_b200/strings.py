@@ -93,3 +93,95 @@ def get_str(x, z, flags, val, num_qubits: int) -> str:
     for i in range(len(val)):
         lines.append(f"{float(val[i]):f} * " + fmt(x[:, i], z[:, i], flags[i], num_qubits) + "\n")
     return "".join(lines)
+
+
+def multiply_words(ax, az, fa: int, bx, bz, fb: int):
+    """(x, z, flags) of the product of two strings given as word lists:
+    x = ax ^ bx, z = az ^ bz, flags = (fa + fb + popc(c1) + 2 parity(c2))
+    mod 4 with the per-word phase accumulators of PauliStringCore.h:150-174.
+    The single-string value algebra of PauliString; sums multiply on the
+    device."""
+    c1 = c2 = 0
+    x, z = [], []
+    for a_x, a_z, b_x, b_z in zip(ax, az, bx, bz):
+        a_x, a_z, b_x, b_z = int(a_x), int(a_z), int(b_x), int(b_z)
+        xbz = a_x & b_z
+        anti = (b_x & a_z) ^ xbz
+        c2 ^= (c1 ^ a_x ^ a_z ^ b_x ^ b_z ^ xbz) & anti
+        c1 ^= anti
+        x.append(a_x ^ b_x)
+        z.append(a_z ^ b_z)
+    f = (int(fa) + int(fb) + bin(c1).count("1") + 2 * (bin(c2).count("1") & 1)) & 3
+    return x, z, f
+
+
+def anticommute_words(ax, az, bx, bz) -> int:
+    """Symplectic inner product (0: commute, 1: anticommute),
+    PauliStringCore.h:126-146."""
+    p = 0
+    for a_x, a_z, b_x, b_z in zip(ax, az, bx, bz):
+        p ^= (int(a_x) & int(b_z)) ^ (int(a_z) & int(b_x))
+    return bin(p).count("1") & 1
+
+
+class MT19937_64:
+    """std::mt19937_64 (the 64-bit Mersenne Twister of Matsumoto and
+    Nishimura, as the C++ standard specifies it), whose raw outputs are what
+    std::uniform_int_distribution<uint64_t> over the full range returns:
+    the generator behind random_pauli_sum (PauliSumUtils.h:114-154)."""
+
+    N, M = 312, 156
+    MATRIX_A = 0xB5026F5AA96619E9
+    UPPER, LOWER = 0xFFFFFFFF80000000, 0x7FFFFFFF
+    MASK = (1 << 64) - 1
+
+    def __init__(self, seed: int = 5489):
+        mt = [int(seed) & self.MASK]
+        for i in range(1, self.N):
+            prev = mt[-1]
+            mt.append((6364136223846793005 * (prev ^ (prev >> 62)) + i) & self.MASK)
+        self.mt = mt
+        self.i = self.N
+
+    def _twist(self):
+        mt, n, m = self.mt, self.N, self.M
+        for k in range(n):
+            y = (mt[k] & self.UPPER) | (mt[(k + 1) % n] & self.LOWER)
+            mt[k] = mt[(k + m) % n] ^ (y >> 1) ^ (self.MATRIX_A if y & 1 else 0)
+        self.i = 0
+
+    def __call__(self) -> int:
+        if self.i >= self.N:
+            self._twist()
+        y = self.mt[self.i]
+        self.i += 1
+        y ^= (y >> 29) & 0x5555555555555555
+        y ^= (y << 17) & 0x71D67FFFEDA60000
+        y ^= (y << 37) & 0xFFF7EEE000000000
+        y ^= y >> 43
+        return y & self.MASK
+
+
+def random_planes(num_terms: int, seed: int, num_qubits: int, words: int):
+    """The terms random_pauli_sum(num_terms, seed, num_qubits) draws
+    (PauliSumUtils.h:114-154): per term the sign bit, the phase bit, then the
+    x and z word of every word covering num_qubits (the last one masked to
+    the remaining qubits), all coefficients 1."""
+    rng = MT19937_64(seed)
+    full, rem = divmod(int(num_qubits), 64)
+    n = int(num_terms)
+    x = np.zeros((words, n), np.uint64)
+    z = np.zeros((words, n), np.uint64)
+    f = np.zeros(n, np.uint8)
+    for t in range(n):
+        sign = rng() & 1
+        phase = rng() & 1
+        f[t] = (sign << 1) | phase
+        for w in range(full):
+            x[w, t] = rng()
+            z[w, t] = rng()
+        if rem:
+            pad = (1 << rem) - 1
+            x[full, t] = rng() & pad
+            z[full, t] = rng() & pad
+    return x, z, f, np.ones(n, np.float64)
