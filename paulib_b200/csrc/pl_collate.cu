@@ -780,7 +780,9 @@ struct FoldFilter {
     int on;
     double cutoff;
     u32* tile_kept;
-    double2* seg2;  // kCanonSplit: (phase-0 sum, phase-1 sum) at each head
+    double2* seg2;   // kCanonSplit: (phase-0 sum, phase-1 sum) at each head
+    double2* rpre;   // per fold range: the sums of its terms before its first head
+    double2* ptail;  // per pending segment: its sums at the end of its range
 };
 
 // canonicalize() on index-packed keys: the sort key is (x, z) only and the
@@ -793,16 +795,19 @@ constexpr int kCanonSplit = 3;
 
 // Segment fold.  A warp owns 1024 consecutive sorted terms, staged in shared
 // memory; lane L folds its own 32 terms left to right (32 independent
-// chains per warp).  Carries then cross lane borders: a lane holding a head
-// is resolved at once, a headless lane continues its left neighbour's open
-// segment over its whole span as soon as that neighbour is resolved, and
-// finally each lane folds its prefix (the terms before its first head) onto
-// the carry it received and closes that segment.  Every segment is therefore
-// summed in exactly the reference's left-to-right order
-// (PauliSumOperations.h:443-455).  The warp that holds a segment's head owns
-// it; an owned segment still open at the end of the range is continued chunk
-// by chunk (up to kExtChunks) and otherwise handed to the long-run kernels.
-// segflag[head] = 1 kept, 3 dropped, 2 long (pending); non-heads get 0.
+// chains per warp), the reference's order (PauliSumOperations.h:443-455).
+// Segments that cross lane borders: a lane with a head knows the segment
+// open at the end of its span; the lane after it continues that segment
+// over its span term by term; longer chains of headless lanes combine the
+// lanes' partial sums in a fixed tree, and the lane that closes the segment
+// folds its own terms onto the result term by term.  Every segment within
+// three lanes is therefore summed exactly in the reference's order, and
+// every other one in a fixed order (deterministic; within 1e-12 of the
+// summed magnitudes).  The warp that holds a segment's head owns it; one
+// still open at the end of the range continues over the staged lookahead
+// (term by term) and otherwise goes to the carry pass (k_fold_carry), which
+// adds the following ranges' prefix partials.
+// segflag[head] = 1 kept, 3 dropped, 2 pending; non-heads get 0.
 // wfirst[warp] = offset of the range's first head, kNoHead if none.
 constexpr int kFoldWarps = 4;
 constexpr int kLaneSpan = 32;
@@ -810,14 +815,12 @@ constexpr u32 kFoldSpan = 32u * kLaneSpan;  // 1024 terms per warp
 constexpr u32 kLook = 64;                   // terms after the range staged as well
 constexpr u32 kLookSlot = 33u * 32u;        // lane spans padded to 33 slots (no bank conflicts)
 constexpr u32 kFoldSlots = kLookSlot + kLook;
-constexpr int kExtChunks = 32;              // at most 1024 more
 constexpr u32 kFoldChunks = 32u + kLook / 32u;
 // per warp: the staged values, then per 32-term chunk a word of head bits and
 // a word of sign bits (chunk c < 32 is lane c's span)
 constexpr size_t kFoldWarpSmem = kFoldSlots * 8 + kFoldChunks * 8;
 constexpr size_t kFoldSmem = ((kFoldWarpSmem + 15) & ~size_t(15)) * kFoldWarps;
 constexpr u32 kNoHead = 0xffffffffu;
-constexpr u32 kPiece = 4096;  // terms per partial sum of a long run
 constexpr int kEItems = 8;
 constexpr u32 kETile = kThreads * kEItems;  // 2048 terms per emit tile
 
@@ -1007,7 +1010,9 @@ __global__ void __launch_bounds__(32 * kFoldWarps, 5)
     }
     if (lane == 0) wfirst[gwarp] = first;
     __syncwarp();
-    // ---- phase 1: each lane folds the segments that start inside its span
+    // ---- phase 1: each lane folds the segments that start inside its span,
+    // and the terms before its first head (its whole span when it has none)
+    // from zero: its prefix partial
     const u32 a = (u32)lane * kLaneSpan;
     const u32 sa = (u32)lane * 33u;
     const u32 lcnt = cnt > a ? min(cnt - a, (u32)kLaneSpan) : 0u;
@@ -1015,7 +1020,7 @@ __global__ void __launch_bounds__(32 * kFoldWarps, 5)
     const u32 NB = lcnt ? nbw[lane] : 0u;
     u32 fh = lcnt;  // prefix length (terms before the lane's first head)
     i64 h = -1;
-    double r0 = 0.0, r1 = 0.0;
+    double r0 = 0.0, r1 = 0.0, p0 = 0.0, p1 = 0.0;
     u32 kept = 0;
     for (u32 i = 0; i < lcnt; ++i) {
         const double v = sv[sa + i];
@@ -1027,114 +1032,104 @@ __global__ void __launch_bounds__(32 * kFoldWarps, 5)
             r1 = 0.0;
         }
         if (h >= 0) fold_term<MODE>(r0, r1, v, (NB >> i) & 1u);
+        else fold_term<MODE>(p0, p1, v, (NB >> i) & 1u);
     }
-    // ---- phase 2: carries across lane borders.  (oh, o0, o1) is the segment
-    // open at the end of the lane's span; oh = -1 when it belongs to an
-    // earlier warp.
+    // ---- phase 2: the segment open at the end of each lane's span, (oh, o0,
+    // o1) with oh = -1 for one that began before the range.  A lane with a
+    // head knows it.  A headless lane right after a lane with a head folds its
+    // span onto that segment term by term (the reference's order); every
+    // longer chain of headless lanes adds the lanes' prefix partials in a
+    // fixed tree (segmented scan over the lanes), so results are
+    // deterministic and equal the reference's order for every segment that
+    // spans at most three lanes.
     const bool hh = fh < lcnt;
     i64 oh = hh ? h : -1;
-    double o0 = hh ? r0 : 0.0, o1 = hh ? r1 : 0.0;
-    bool ready = hh || lane == 0;
-    for (int it = 0; it < 32; ++it) {
-        if (__all_sync(0xffffffffu, ready)) break;
+    double o0 = hh ? r0 : p0, o1 = hh ? r1 : p1;
+    bool known = hh;
+    {
         const i64 ph = __shfl_up_sync(0xffffffffu, oh, 1);
-        const double p0 = __shfl_up_sync(0xffffffffu, o0, 1);
-        const double p1 = __shfl_up_sync(0xffffffffu, o1, 1);
-        const int pr = __shfl_up_sync(0xffffffffu, (int)ready, 1);
-        if (!ready && pr) {
+        const double q0 = __shfl_up_sync(0xffffffffu, o0, 1);
+        const double q1 = __shfl_up_sync(0xffffffffu, o1, 1);
+        const int pk = __shfl_up_sync(0xffffffffu, (int)hh, 1);
+        if (lane > 0 && !hh && pk) {
             oh = ph;
-            o0 = p0;
-            o1 = p1;
-            if (ph >= 0)
-                for (u32 i = 0; i < lcnt; ++i) fold_term<MODE>(o0, o1, sv[sa + i], (NB >> i) & 1u);
-            ready = true;
+            o0 = q0;
+            o1 = q1;
+            for (u32 i = 0; i < lcnt; ++i) fold_term<MODE>(o0, o1, sv[sa + i], (NB >> i) & 1u);
+            known = true;
         }
     }
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+        const i64 ph = __shfl_up_sync(0xffffffffu, oh, d);
+        const double q0 = __shfl_up_sync(0xffffffffu, o0, d);
+        const double q1 = __shfl_up_sync(0xffffffffu, o1, d);
+        const int pk = __shfl_up_sync(0xffffffffu, (int)known, d);
+        if (lane >= d && !known) {
+            oh = ph;
+            o0 = dadd(q0, o0);
+            o1 = dadd(q1, o1);
+            known = pk != 0;
+        }
+    }
+    // ---- close: a lane with a head folds the terms before it onto the
+    // segment coming in from the left (term by term); the warp's first head
+    // gets the range's prefix partial instead (the terms of a segment that
+    // began in an earlier range), which the carry pass adds to it.
+    double rp0 = 0.0, rp1 = 0.0;
     {
         i64 cin = __shfl_up_sync(0xffffffffu, oh, 1);
         double q0 = __shfl_up_sync(0xffffffffu, o0, 1);
         double q1 = __shfl_up_sync(0xffffffffu, o1, 1);
-        if (lane == 0) cin = -1;
-        if (hh && cin >= 0) {
+        if (lane == 0) {
+            cin = -1;
+            q0 = 0.0;
+            q1 = 0.0;
+        }
+        if (hh) {
             for (u32 i = 0; i < fh; ++i) fold_term<MODE>(q0, q1, sv[sa + i], (NB >> i) & 1u);
-            kept += fold_close<MODE>(segval, segflag, cin, q0, q1, F);
+            if (cin >= 0) {
+                kept += fold_close<MODE>(segval, segflag, cin, q0, q1, F);
+            } else {
+                rp0 = q0;
+                rp1 = q1;
+            }
         }
     }
     const i64 ch = __shfl_sync(0xffffffffu, oh, 31);
-    double c0 = __shfl_sync(0xffffffffu, o0, 31);
-    double c1 = __shfl_sync(0xffffffffu, o1, 31);
-    // ---- the open segment at the end of the range, when this warp owns it
-    if (ch >= 0) {
+    const double c0 = __shfl_sync(0xffffffffu, o0, 31);
+    const double c1 = __shfl_sync(0xffffffffu, o1, 31);
+    {
+        // the range's prefix partial, for the carry pass of an earlier range
+        const u32 fl = first == kNoHead ? 31u : first / kLaneSpan;
+        const double e0 = __shfl_sync(0xffffffffu, first == kNoHead ? o0 : rp0, (int)fl);
+        const double e1 = __shfl_sync(0xffffffffu, first == kNoHead ? o1 : rp1, (int)fl);
+        if (lane == 0) F.rpre[gwarp] = make_double2(e0, e1);
+    }
+    // ---- the open segment at the end of the range, when this warp owns it:
+    // the staged lookahead continues it term by term; one still open after
+    // it goes to the carry pass with its value before the lookahead.
+    if (ch >= 0 && lane == 0) {
         if (w1 == C.n) {
-            if (lane == 0) kept += fold_close<MODE>(segval, segflag, ch, c0, c1, F);
+            kept += fold_close<MODE>(segval, segflag, ch, c0, c1, F);
         } else {
-            // continuation: first the staged lookahead terms, in order, on
-            // lane 0; a segment still open after them continues from global
-            // memory, 32 terms at a time, up to kExtChunks * 32 terms past the
-            // range in all (longer ones go to the long-run kernels)
-            int closed = 0;
-            if (lane == 0) {
-                for (u32 q = 0; q < look; ++q) {
-                    const u32 wq = 32u + (q >> 5), bq = q & 31u;
-                    if ((hbw[wq] >> bq) & 1u) {
-                        kept += fold_close<MODE>(segval, segflag, ch, c0, c1, F);
-                        closed = 1;
-                        break;
-                    }
-                    fold_term<MODE>(c0, c1, sv[kLookSlot + q], (nbw[wq] >> bq) & 1u);
+            double d0 = c0, d1 = c1;
+            bool closed = false;
+            for (u32 q = 0; q < look; ++q) {
+                const u32 wq = 32u + (q >> 5), bq = q & 31u;
+                if ((hbw[wq] >> bq) & 1u) {
+                    closed = true;
+                    break;
                 }
-                if (!closed && w1 + look == C.n) {
-                    kept += fold_close<MODE>(segval, segflag, ch, c0, c1, F);
-                    closed = 1;
-                }
+                fold_term<MODE>(d0, d1, sv[kLookSlot + q], (nbw[wq] >> bq) & 1u);
             }
-            closed = __shfl_sync(0xffffffffu, closed, 0);
-            c0 = __shfl_sync(0xffffffffu, c0, 0);
-            c1 = __shfl_sync(0xffffffffu, c1, 0);
-            const u32 gs = w1 + look;  // look == kLook here (a shorter one reaches the end)
-            if (!closed) {
-                ck = C.keys[gs - 1];
-                cp = fold_word<MODE>(C, gs - 1, ck);
-            }
-            for (int ext = 0; !closed; ++ext) {
-                const u32 cb = gs + (u32)ext * 32u;
-                if (cb >= C.n) {
-                    if (lane == 0) kept += fold_close<MODE>(segval, segflag, ch, c0, c1, F);
-                    break;
-                }
-                if (ext >= kExtChunks - (int)(kLook / 32)) {
-                    if (lane == 0) {
-                        segflag[ch] = 2;
-                        long_list[atomicAdd(&counters[2], 1u)] = (u32)ch;
-                    }
-                    break;
-                }
-                const u32 e = cb + lane;
-                const bool valid = e < C.n;
-                const u64 ke = valid ? C.keys[e] : 0ull;
-                const u32 pe = valid ? fold_word<MODE>(C, e, ke) : 0u;
-                const double ve = valid ? C.vals[e] : 0.0;
-                u64 kp = __shfl_up_sync(0xffffffffu, ke, 1);
-                u32 pp = __shfl_up_sync(0xffffffffu, pe, 1);
-                if (lane == 0) {
-                    kp = ck;
-                    pp = cp;
-                }
-                const bool head = valid && !lane_same_key(C, e, ke, kp, pe, pp);
-                const u32 hb = __ballot_sync(0xffffffffu, head || !valid);
-                const u32 lim = hb ? (u32)(__ffs(hb) - 1) : 32u;
-                // the tail lanes [0, lim) continue the segment, in order
-                for (u32 k = 0; k < lim; ++k) {
-                    const double vk = __shfl_sync(0xffffffffu, ve, k);
-                    const u32 pk = __shfl_sync(0xffffffffu, pe, k);
-                    fold_add<MODE>(c0, c1, vk, pk);
-                }
-                if (lim < 32) {
-                    if (lane == 0) kept += fold_close<MODE>(segval, segflag, ch, c0, c1, F);
-                    break;
-                }
-                ck = __shfl_sync(0xffffffffu, ke, 31);
-                cp = __shfl_sync(0xffffffffu, pe, 31);
+            if (closed || w1 + look == C.n) {
+                kept += fold_close<MODE>(segval, segflag, ch, d0, d1, F);
+            } else {
+                segflag[ch] = 2;
+                const u32 k = atomicAdd(&counters[2], 1u);
+                long_list[k] = (u32)ch;
+                F.ptail[k] = make_double2(c0, c1);
             }
         }
     }
@@ -1145,43 +1140,41 @@ __global__ void __launch_bounds__(32 * kFoldWarps, 5)
     }
 }
 
-// Long runs (segflag 2): a run [h, end) ends at the next head, found in the
-// per-warp first-head table; it is cut into kPiece-term pieces.  One warp
-// per run.  counters: [2] runs.
-__global__ void __launch_bounds__(256) k_long_ends(const u32* wfirst, u32 ngw, u32 n,
-                                                   const u32* long_list, const u32* counters,
-                                                   u32* long_end, u32* long_np) {
-    const u32 nlong = counters[2];
+// Carry pass: a segment still open after its range and the lookahead (the
+// pending list, counters[2]) continues through the following ranges up to
+// the first one with a head; its sum is its value at the end of its range
+// plus those ranges' prefix partials, added 32 ranges at a time in a fixed
+// tree.  One warp per pending segment.
+template <int MODE>
+__global__ void __launch_bounds__(256) k_fold_carry(const u32* wfirst, u32 ngw,
+                                                    const u32* long_list, const u32* counters,
+                                                    double* segval, u8* segflag, FoldFilter F) {
+    const u32 npend = counters[2];
     const int lane = threadIdx.x & 31;
     const u32 nw = (gridDim.x * blockDim.x) >> 5;
-    for (u32 li = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; li < nlong; li += nw) {
+    for (u32 li = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; li < npend; li += nw) {
         const u32 h = long_list[li];
-        u32 end = n;
-        for (u32 g0 = h / kFoldSpan + 1; g0 < ngw; g0 += 32u * 8u) {
-            u32 f[8];
+        const double2 t = F.ptail[li];
+        double a0 = t.x, a1 = t.y;
+        for (u32 g0 = h / kFoldSpan + 1;; g0 += 32u) {
+            const u32 g = g0 + (u32)lane;
+            const bool end = g >= ngw || wfirst[g] != kNoHead;
+            const u32 bal = __ballot_sync(0xffffffffu, end);
+            const u32 last = bal ? (u32)(__ffs(bal) - 1) : 31u;
+            double2 pr = make_double2(0.0, 0.0);
+            if ((u32)lane <= last && g < ngw) pr = F.rpre[g];
 #pragma unroll
-            for (int b = 0; b < 8; ++b) {
-                const u32 g = g0 + (u32)b * 32u + lane;
-                f[b] = g < ngw ? wfirst[g] : kNoHead;
+            for (int o = 16; o > 0; o >>= 1) {
+                pr.x = dadd(pr.x, __shfl_xor_sync(0xffffffffu, pr.x, o));
+                pr.y = dadd(pr.y, __shfl_xor_sync(0xffffffffu, pr.y, o));
             }
-            u32 found = kNoHead;
-#pragma unroll
-            for (int b = 0; b < 8; ++b) {
-                const u32 bal = __ballot_sync(0xffffffffu, f[b] != kNoHead);
-                if (found == kNoHead && bal) {
-                    const int l = __ffs(bal) - 1;
-                    found = (g0 + (u32)b * 32u + (u32)l) * kFoldSpan +
-                            __shfl_sync(0xffffffffu, f[b], l);
-                }
-            }
-            if (found != kNoHead) {
-                end = found;
-                break;
-            }
+            a0 = dadd(a0, pr.x);
+            a1 = dadd(a1, pr.y);
+            if (bal) break;
         }
         if (lane == 0) {
-            long_end[li] = end;
-            long_np[li] = (end - h + kPiece - 1) / kPiece;
+            const u32 keep = fold_close<MODE>(segval, segflag, h, a0, a1, F);
+            if (F.on && keep) atomicAdd(&F.tile_kept[h / kETile], keep);
         }
     }
 }
@@ -1214,105 +1207,6 @@ __device__ __forceinline__ u32 block_scan_n(u32 v, u32* s_warp, u32& total) {
     const u32 r = s_warp[32 + warp] + inc - v;
     __syncthreads();
     return r;
-}
-
-// Piece offsets of the long runs (exclusive scan of long_np; one CTA).
-// counters: [4] pieces.
-__global__ void __launch_bounds__(1024) k_long_scan(const u32* long_np, u32* long_poff,
-                                                    u32* long_tick, u32* counters) {
-    __shared__ u32 sw[65];
-    const u32 nlong = counters[2];
-    const u32 per = (nlong + 1023u) / 1024u;
-    const u32 b = threadIdx.x * per, e = min(b + per, nlong);
-    u32 s = 0;
-    for (u32 i = b; i < e; ++i) s += long_np[i];
-    u32 total;
-    u32 run = block_scan_n<32>(s, sw, total);
-    for (u32 i = b; i < e; ++i) {
-        long_poff[i] = run;
-        run += long_np[i];
-        long_tick[i] = 0;
-    }
-    if (threadIdx.x == 0) {
-        long_poff[nlong] = total;
-        counters[4] = total;
-    }
-}
-
-// One CTA per piece: thread t sums terms t, t+256, ... of the piece in order
-// and the partial sums meet in a fixed binary tree; the last piece of a run
-// to finish sums the run's pieces the same way and closes the run.  The
-// order depends only on the run, so results are deterministic.
-template <int MODE>
-__device__ __forceinline__ void tree_sum(double* s0, double* s1, double a0, double a1) {
-    s0[threadIdx.x] = a0;
-    s1[threadIdx.x] = a1;
-    __syncthreads();
-    for (int st = kThreads / 2; st > 0; st >>= 1) {
-        if ((int)threadIdx.x < st) {
-            s0[threadIdx.x] = dadd(s0[threadIdx.x], s0[threadIdx.x + st]);
-            if (MODE == kProp || MODE == kCanonSplit)
-                s1[threadIdx.x] = dadd(s1[threadIdx.x], s1[threadIdx.x + st]);
-        }
-        __syncthreads();
-    }
-}
-
-template <int MODE>
-__global__ void __launch_bounds__(kThreads)
-    k_long_pieces(SegCtx C, const u32* long_list, const u32* long_end, const u32* long_poff,
-                  u32* long_tick, const u32* counters, double* partials, double* segval,
-                  u8* segflag, FoldFilter F) {
-    __shared__ double s0[kThreads], s1[kThreads];
-    __shared__ u32 s_last;
-    constexpr int kPer = kPiece / kThreads;
-    const u32 nlong = counters[2], npieces = counters[4];
-    for (u32 p = blockIdx.x; p < npieces; p += gridDim.x) {
-        u32 lo = 0, hi = nlong;  // long_poff[lo] <= p < long_poff[hi]
-        while (hi - lo > 1) {
-            const u32 mid = (lo + hi) >> 1;
-            if (long_poff[mid] <= p) lo = mid;
-            else hi = mid;
-        }
-        const u32 h = long_list[lo], end = long_end[lo];
-        const u32 pb = long_poff[lo], pe = long_poff[lo + 1];
-        const u32 s = h + (p - pb) * kPiece, e = min(s + kPiece, end);
-        u32 q[kPer];
-        double v[kPer];
-#pragma unroll
-        for (int j = 0; j < kPer; ++j) {
-            const u32 t = s + threadIdx.x + (u32)j * kThreads;
-            q[j] = t >= e ? 0u
-                          : (MODE == kCanonSplit ? ((u32)C.keys[t] & 1u) << 31 : C.pay[t]);
-            v[j] = t < e ? C.vals[t] : 0.0;
-        }
-        double a0 = 0.0, a1 = 0.0;
-#pragma unroll
-        for (int j = 0; j < kPer; ++j)
-            if (s + threadIdx.x + (u32)j * kThreads < e) fold_add<MODE>(a0, a1, v[j], q[j]);
-        tree_sum<MODE>(s0, s1, a0, a1);
-        if (threadIdx.x == 0) {
-            partials[2 * (size_t)p] = s0[0];
-            partials[2 * (size_t)p + 1] = s1[0];
-            __threadfence();
-            s_last = (atomicAdd(&long_tick[lo], 1u) + 1u == pe - pb) ? 1u : 0u;
-        }
-        __syncthreads();
-        if (s_last) {
-            __threadfence();
-            double b0 = 0.0, b1 = 0.0;
-            for (u32 r = pb + threadIdx.x; r < pe; r += kThreads) {
-                b0 = dadd(b0, __ldcg(partials + 2 * (size_t)r));
-                b1 = dadd(b1, __ldcg(partials + 2 * (size_t)r + 1));
-            }
-            tree_sum<MODE>(s0, s1, b0, b1);
-            if (threadIdx.x == 0) {
-                const u32 keep = fold_close<MODE>(segval, segflag, h, s0[0], s1[0], F);
-                if (F.on && keep) atomicAdd(&F.tile_kept[h / kETile], keep);
-            }
-        }
-        __syncthreads();
-    }
 }
 
 // Output offsets of the emit tiles (exclusive scan of the kept counts; one
@@ -1580,8 +1474,9 @@ struct Bufs {
     u64 *ka, *kb, *planes;
     u32 *pa, *pb, *hist, *lb, *counters;
     u8* segflag;
-    double *seg_sum, *sv, *partials;
-    u32 *wfirst, *long_list, *long_end, *long_np, *long_poff, *long_tick;
+    double *seg_sum, *sv;
+    u32 *wfirst, *long_list;
+    double2 *rpre, *ptail;
     u32 *tile_kept, *tile_off, *lb_emit;
     u64 *orm, *andm;
     i64* d_count;
@@ -1592,8 +1487,7 @@ struct Bufs {
 void carve_all(Carve& c, i64 n, int nch, Bufs& B) {
     const i64 rtiles = (n + kRTileMin - 1) / kRTileMin + 1;
     const i64 etiles = (n + kETile - 1) / kETile + 1;
-    const i64 ngw = (n + kFoldSpan - 1) / kFoldSpan + 16;  // fold warps; also bounds long runs
-    const i64 npieces = n / kPiece + ngw;
+    const i64 ngw = (n + kFoldSpan - 1) / kFoldSpan + 16;  // fold ranges; also bounds pending runs
     B.ka = c.take<u64>(n);
     B.kb = c.take<u64>(n);
     B.pa = c.take<u32>(n);
@@ -1607,11 +1501,8 @@ void carve_all(Carve& c, i64 n, int nch, Bufs& B) {
     B.seg_sum = c.take<double>(n);
     B.wfirst = c.take<u32>(ngw);
     B.long_list = c.take<u32>(ngw);
-    B.long_end = c.take<u32>(ngw);
-    B.long_np = c.take<u32>(ngw);
-    B.long_poff = c.take<u32>(ngw + 1);
-    B.long_tick = c.take<u32>(ngw);
-    B.partials = c.take<double>(2 * npieces);
+    B.rpre = c.take<double2>(ngw);
+    B.ptail = c.take<double2>(ngw);
     B.tile_kept = c.take<u32>(etiles);
     B.tile_off = c.take<u32>(etiles);
     B.lb_emit = c.take<u32>(etiles);
@@ -1722,8 +1613,8 @@ bool build_layout_split(int as, const u64* orm, const u64* andm, u32 n, KeyLayou
     return true;
 }
 
-// Segment sums: the warp fold, then the long runs (ends, piece offsets,
-// pieces with the last piece of each run closing it).
+// Segment sums: the warp fold, then the carry pass for the segments still
+// open after their range and its lookahead.
 template <int MODE>
 int fold_segments(const SegCtx& C, Bufs& B, const FoldFilter& F, int nsm, cudaStream_t st) {
     const u32 n = C.n;
@@ -1733,18 +1624,10 @@ int fold_segments(const SegCtx& C, Bufs& B, const FoldFilter& F, int nsm, cudaSt
                                      (int)kFoldSmem));
     k_fold<MODE><<<fold_blocks, 32 * kFoldWarps, kFoldSmem, st>>>(
         C, B.seg_sum, B.segflag, B.wfirst, B.long_list, B.counters, F), pl::note_launch();
-    // a long run is longer than kFoldSpan terms, so there are fewer than ngw
-    const int lw_blocks = (int)std::min<u32>((ngw + 7) / 8, (u32)nsm * 4);
-    k_long_ends<<<lw_blocks, 256, 0, st>>>(B.wfirst, ngw, n, B.long_list, B.counters,
-                                           B.long_end, B.long_np), pl::note_launch();
-    k_long_scan<<<1, 1024, 0, st>>>(B.long_np, B.long_poff, B.long_tick, B.counters),
-        pl::note_launch();
-    const u32 max_pieces = n / kPiece + ngw;
-    const int lp_blocks = (int)std::min<u32>(max_pieces, (u32)nsm * 8);
-    k_long_pieces<MODE><<<lp_blocks, kThreads, 0, st>>>(C, B.long_list, B.long_end, B.long_poff,
-                                                        B.long_tick, B.counters, B.partials,
-                                                        B.seg_sum, B.segflag, F),
-        pl::note_launch();
+    // at most one pending segment per fold range
+    const int cw_blocks = (int)std::min<u32>((ngw + 7) / 8, (u32)nsm * 4);
+    k_fold_carry<MODE><<<cw_blocks, 256, 0, st>>>(B.wfirst, ngw, B.long_list, B.counters,
+                                                  B.seg_sum, B.segflag, F), pl::note_launch();
     return PL_OK;
 }
 
@@ -1902,7 +1785,7 @@ int run_collate(const Src& src, u32 n, int mode, const KeyLayout& L, const PassP
     // Without a weight filter the fold decides the zero / cutoff filters and
     // counts survivors per emit tile, so the emit needs no look-back.
     const bool counted = a.max_weight == ~0ull;
-    const FoldFilter F{counted ? 1 : 0, a.cutoff, B.tile_kept};
+    const FoldFilter F{counted ? 1 : 0, a.cutoff, B.tile_kept, nullptr, B.rpre, B.ptail};
     if (counted) PL_CUDA_TRY(fill32_async(B.tile_kept, 0u, sizeof(u32) * etiles, st));
     e0 = timed_begin(st);
     int rc = PL_OK;
@@ -1992,7 +1875,7 @@ int run_collate_split(const Src& src, u32 n, const KeyLayout& L, const PassPlan&
     }
     SegCtx C{kin, nullptr, B.sv, B.planes, n, 1, L.seg_mask0, kCanon};
     const u32 etiles = (n + kETile - 1) / kETile;
-    const FoldFilter F{1, a.cutoff, B.tile_kept, seg2};
+    const FoldFilter F{1, a.cutoff, B.tile_kept, seg2, B.rpre, B.ptail};
     e0 = timed_begin(st);
     int rc = fold_segments<kCanonSplit>(C, B, F, nsm, st);
     if (rc != PL_OK) return rc;
