@@ -901,7 +901,7 @@ __device__ __forceinline__ u32 fold_close(double* segval, u8* segflag, i64 h, do
 }
 
 template <int MODE>
-__global__ void __launch_bounds__(32 * kFoldWarps, 5)
+__global__ void __launch_bounds__(32 * kFoldWarps, 6)
     k_fold(SegCtx C, double* segval, u8* segflag, u32* wfirst, u32* long_list, u32* counters,
            FoldFilter F) {
     extern __shared__ __align__(16) unsigned char fsm[];
@@ -1622,6 +1622,10 @@ int fold_segments(const SegCtx& C, Bufs& B, const FoldFilter& F, int nsm, cudaSt
     const u32 fold_blocks = (ngw + kFoldWarps - 1) / kFoldWarps;
     PL_CUDA_TRY(cudaFuncSetAttribute(k_fold<MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      (int)kFoldSmem));
+    // six CTAs (24 warps) per SM: 6 x 37 KB of staging
+    PL_CUDA_TRY(cudaFuncSetAttribute(k_fold<MODE>,
+                                     cudaFuncAttributePreferredSharedMemoryCarveout,
+                                     cudaSharedmemCarveoutMaxShared));
     k_fold<MODE><<<fold_blocks, 32 * kFoldWarps, kFoldSmem, st>>>(
         C, B.seg_sum, B.segflag, B.wfirst, B.long_list, B.counters, F), pl::note_launch();
     // at most one pending segment per fold range

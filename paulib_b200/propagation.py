@@ -69,6 +69,37 @@ class State:
         _abi.check(self._lib.pl_state_set_cancel_flag(self._h, p), "pl_state_set_cancel_flag")
         return self
 
+    # -- sharded sums (pl_state_shard_pack / _unpack, MpiPauliSum.h) -------
+    def shard_pack(self, ranks: int):
+        """This state's terms as (n, 2*AS + 2) int64 records on the device,
+        grouped by owner rank FNV-1a(x, z) mod ranks in term order, and the
+        per-owner counts."""
+        import torch
+        n = self.size()
+        W = 2 * self.array_size + 2
+        recs = torch.empty((max(n, 1), W), dtype=torch.int64, device="cuda")
+        counts = (C.c_int64 * int(ranks))()
+        _abi.check(self._lib.pl_state_shard_pack(self._h, int(ranks), recs.data_ptr(), n,
+                                                 counts), "pl_state_shard_pack")
+        return recs, [int(c) for c in counts]
+
+    def shard_unpack(self, recs):
+        """Replace the terms by the records received (an (m, W) tensor)."""
+        m = int(recs.shape[0])
+        _abi.check(self._lib.pl_state_shard_unpack(self._h, recs.data_ptr() if m else None, m),
+                   "pl_state_shard_unpack")
+
+    def max_abs(self) -> float:
+        r = C.c_double()
+        _abi.check(self._lib.pl_state_max_abs(self._h, C.byref(r)), "pl_state_max_abs")
+        return r.value
+
+    def count_above(self, threshold: float) -> int:
+        c = C.c_int64()
+        _abi.check(self._lib.pl_state_count_above(self._h, float(threshold), C.byref(c)),
+                   "pl_state_count_above")
+        return int(c.value)
+
     def log_gates(self, enable: bool = True):
         """Record (terms in, anticommuting terms, terms out) of every
         fast-path rotation of the next propagate() (PL_OPT_GATE_LOG)."""

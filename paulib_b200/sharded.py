@@ -13,9 +13,6 @@ collective definitions (MpiPauliSum.h:86-97, 187-210).
 """
 from __future__ import annotations
 
-import ctypes as C
-
-from . import _abi
 from .propagation import State
 
 
@@ -46,7 +43,11 @@ def exchange_records(send, counts, group=None):
 
 
 class ShardedPauliSum:
-    """This rank's share of a sum distributed over the ranks of `group`."""
+    """This rank's share of a sum distributed over the ranks of `group`.
+
+    `state` is a propagation.State (device-resident); the class uses only its
+    size, shard_pack, shard_unpack, canonicalize, frobenius_norm2, max_abs,
+    count_above and cutoff."""
 
     def __init__(self, state: State, num_qubits: int, group=None):
         import torch.distributed as dist
@@ -67,19 +68,10 @@ class ShardedPauliSum:
     def exchange_and_combine(self):
         """Route every local term to its owner, then combine locally
         (MpiPauliSum.h:101-181)."""
-        import torch
-        st = self.state
-        n = st.size()
-        W = record_words(st.array_size)
-        send = torch.empty((max(n, 1), W), dtype=torch.int64, device="cuda")
-        counts = (C.c_int64 * self.ranks)()
-        _abi.check(st._lib.pl_state_shard_pack(st._h, self.ranks, send.data_ptr(), n, counts),
-                   "pl_state_shard_pack")
-        recv, _ = exchange_records(send, list(counts), self.group)
-        m = recv.shape[0]
-        _abi.check(st._lib.pl_state_shard_unpack(st._h, recv.data_ptr() if m else None, m),
-                   "pl_state_shard_unpack")
-        st.canonicalize()
+        send, counts = self.state.shard_pack(self.ranks)
+        recv, _ = exchange_records(send, counts, self.group)
+        self.state.shard_unpack(recv)
+        self.state.canonicalize()
 
     def global_terms(self) -> int:
         import torch.distributed as dist
@@ -97,16 +89,11 @@ class ShardedPauliSum:
         if self.global_terms() <= max_terms:
             return
         st = self.state
-        r = C.c_double()
-        _abi.check(st._lib.pl_state_max_abs(st._h, C.byref(r)), "pl_state_max_abs")
-        hi = self._allreduce(r.value, dist.ReduceOp.MAX)
+        hi = self._allreduce(st.max_abs(), dist.ReduceOp.MAX)
         lo = 0.0
 
         def count_at(t):
-            c = C.c_int64()
-            _abi.check(st._lib.pl_state_count_above(st._h, float(t), C.byref(c)),
-                       "pl_state_count_above")
-            return int(self._allreduce(float(c.value), dist.ReduceOp.SUM))
+            return int(self._allreduce(float(st.count_above(t)), dist.ReduceOp.SUM))
 
         for _ in range(60):
             if not hi - lo > 0.0:
