@@ -699,22 +699,6 @@ __global__ void __launch_bounds__(kPT, AS == 1 ? 4 : 2)
                                                          b0);
         }
         __syncthreads();
-        if (!bad && mode != kSkip) {
-            for (int i = tid; i < cb; i += kPT) {
-                u64 x[AS], z[AS];
-#pragma unroll
-                for (int w = 0; w < AS; ++w) {
-                    x[w] = S.x[w * S.cap + i];
-                    z[w] = S.z[w * S.cap + i];
-                }
-                if (anticommutes<AS>(x, z, g)) {
-                    if (mode == kGeneral) S.v[i] = dmul(S.v[i], c);
-                    else if (mode == kNegate) S.v[i] = -S.v[i];
-                    else S.f[i] |= 4u;  // +-pi/2: the old term moved to its child
-                }
-            }
-        }
-        __syncthreads();
         // this thread's merged positions [d, d + IT) of the tile
         const int d = tid * IT;
         const int L = bad ? 0 : la + lbn;
@@ -748,10 +732,19 @@ __global__ void __launch_bounds__(kPT, AS == 1 ? 4 : 2)
             if (take_a) {
                 e = ha + ai;
                 ke = ka;
-                const u32 fa = S.f[e];
-                if (!(fa & 4u)) {
+                // an anticommuting old term is scaled by cos(theta), negated
+                // (theta ~ pi) or moved to its child (theta ~ +-pi/2) here,
+                // where its merge takes it
+                double va = S.v[e];
+                bool kept_a = true;
+                if (mode != kSkip && anticommutes<AS>(ka.x, ka.z, g)) {
+                    if (mode == kGeneral) va = dmul(va, c);
+                    else if (mode == kNegate) va = -va;
+                    else kept_a = false;
+                }
+                if (kept_a) {
                     has = true;
-                    sp = dadd(sp, S.v[e]);  // canonical A terms carry sign 0
+                    sp = dadd(sp, va);  // canonical A terms carry sign 0
                 }
                 // the C twin follows directly (ties take A first)
                 if (bi < lbn + hc && same_string<AS>(ka, kc)) {
