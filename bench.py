@@ -421,6 +421,7 @@ def run_product_collate(args, rank, local, ws):
         torch.cuda.empty_cache()
         line["propagation"] = propagation_extra(args, peak)
         line["served"] = served_extra(args)
+        line["batch"] = batch_extra(args)
     return line
 
 
@@ -617,6 +618,23 @@ def served_extra(args):
             "speedup_vs_plain_fifo": line["value"] / c["plain_fifo_value"],
             "results_identical": c["results_identical"],
             "peak_device_gb": c["peak_device_gb"]}
+
+
+def batch_extra(args):
+    """Batched propagation (every 16th job of the 512-job mixed set, the
+    autotuned executor) against the plain one-at-a-time path on the same
+    jobs, with the bound the longest job puts on any schedule."""
+    from paulib_b200 import benchmarks
+    ns = argparse.Namespace(batch_stride=args.batch_stride, steps=1, warmup=1)
+    line = benchmarks.run("batch", ns, 0, torch_local_rank(), 1)
+    c = line["config"]
+    return {"workload": c["workload"], "jobs": c["jobs"], "stride_of_512": c["stride_of_512"],
+            "value": line["value"], "unit": line["unit"], "plain_value": c["plain_value"],
+            "speedup_vs_plain": c["speedup_vs_plain"],
+            "longest_job_s": c["longest_job_s"],
+            "speedup_bound_by_longest_job": c["speedup_bound_by_longest_job"],
+            "results_identical_to_plain": c["results_identical_to_plain"],
+            "tuned": c["tuned"], "timing": c["timing"]}
 
 
 def torch_local_rank():

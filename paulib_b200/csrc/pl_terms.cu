@@ -176,6 +176,140 @@ __global__ void __launch_bounds__(kCThreads)
     }
 }
 
+// ---------------------------------------------------------------------------
+// Commutator in two passes, for large n*m.  Pass 1 (k_comm_mask): a CTA
+// holds 256 rhs terms in registers (one per thread) and streams a tile of
+// lhs terms from shared memory (every lane reads the same word: a
+// broadcast); each warp's ballot is the anticommutation mask of one lhs
+// term against its 32 rhs terms, stored as word (i, j / 32) of a row-major
+// bitmask -- pair order i*m + j is the bitmask's bit order.  Pass 2
+// (k_comm_emit): tiles of mask words in order, per-tile popcounts, a
+// decoupled look-back for the output offsets, and each set bit emitted as
+// 2 * lhs_i * rhs_j -- the same terms in the same order as k_commutator.
+// The operands are read from L2 once per (lhs tile, rhs tile) instead of
+// once per pair.
+// ---------------------------------------------------------------------------
+constexpr int kMThreads = 256;  // rhs terms per CTA of the mask pass
+constexpr int kMLhs = 128;      // lhs terms per CTA of the mask pass
+constexpr int kEWords = 8;      // mask words per thread of the emit pass
+constexpr u64 kETileW = (u64)kMThreads * kEWords;
+
+template <int AS>
+__global__ void __launch_bounds__(kMThreads)
+    k_comm_mask(const u64* __restrict__ ax, const u64* __restrict__ az, u64 n, u64 sa,
+                const u64* __restrict__ bx, const u64* __restrict__ bz, u64 m, u64 sb,
+                u32* __restrict__ mask, u64 mw) {
+    __shared__ u64 sx[AS][kMLhs], sz[AS][kMLhs];
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const u64 j = (u64)blockIdx.x * kMThreads + tid;
+    const u64 i0 = (u64)blockIdx.y * kMLhs;
+    const u64 ni = n - i0 < (u64)kMLhs ? n - i0 : (u64)kMLhs;
+    for (int t = tid; t < (int)ni * AS; t += kMThreads) {
+        const int k = t / (int)ni, r = t - k * (int)ni;
+        sx[k][r] = __ldg(ax + (u64)k * sa + i0 + r);
+        sz[k][r] = __ldg(az + (u64)k * sa + i0 + r);
+    }
+    u64 rx[AS], rz[AS];
+#pragma unroll
+    for (int k = 0; k < AS; ++k) {
+        rx[k] = j < m ? __ldg(bx + (u64)k * sb + j) : 0ull;
+        rz[k] = j < m ? __ldg(bz + (u64)k * sb + j) : 0ull;
+    }
+    __syncthreads();
+    const u64 w = (u64)blockIdx.x * (kMThreads / 32) + warp;
+    if (w >= mw) return;
+    u32* row = mask + i0 * mw + w;
+#pragma unroll 4
+    for (int r = 0; r < (int)ni; ++r) {
+        u64 par = 0;
+#pragma unroll
+        for (int k = 0; k < AS; ++k) par ^= anti_word(sx[k][r], sz[k][r], rx[k], rz[k]);
+        const bool anti = j < m && (__popcll(par) & 1);
+        const u32 bal = __ballot_sync(0xffffffffu, anti);
+        if (lane == 0) row[(u64)r * mw] = bal;
+    }
+}
+
+template <int AS>
+__global__ void __launch_bounds__(kMThreads)
+    k_comm_emit(const u64* __restrict__ ax, const u64* __restrict__ az,
+                const u8* __restrict__ af, const double* __restrict__ av, u64 sa,
+                const u64* __restrict__ bx, const u64* __restrict__ bz,
+                const u8* __restrict__ bf, const double* __restrict__ bv, u64 sb, u64 m,
+                const u32* __restrict__ mask, u64 nwords, u64 mw, int mul_i,
+                u64* __restrict__ ox, u64* __restrict__ oz, u8* __restrict__ of,
+                double* __restrict__ ov, i64 capacity, unsigned long long* d_count, u64* lb,
+                u32* tile_ctr, int* status) {
+    __shared__ u32 s_warp[kMThreads / 32];
+    __shared__ u32 s_tile;
+    __shared__ u64 s_base;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    if (tid == 0) s_tile = atomicAdd(tile_ctr, 1u);
+    __syncthreads();
+    const u32 tile = s_tile;
+    const u64 w0 = (u64)tile * kETileW + (u64)tid * kEWords;
+    u32 words[kEWords];
+    u32 cnt = 0;
+#pragma unroll
+    for (int e = 0; e < kEWords; ++e) {
+        words[e] = w0 + e < nwords ? __ldg(mask + w0 + e) : 0u;
+        cnt += __popc(words[e]);
+    }
+    u32 inc = cnt;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const u32 t = __shfl_up_sync(0xffffffffu, inc, o);
+        if (lane >= o) inc += t;
+    }
+    if (lane == 31) s_warp[warp] = inc;
+    __syncthreads();
+    u32 wpre = 0, tot = 0;
+#pragma unroll
+    for (int q = 0; q < kMThreads / 32; ++q) {
+        const u32 c = s_warp[q];
+        if (q < warp) wpre += c;
+        tot += c;
+    }
+    if (tid == 0) {
+        const u64 init = tile == 0 ? (u64)*d_count : 0ull;
+        s_base = lookback64(lb, tile, tot, init, status);
+        if (tile == gridDim.x - 1) *d_count = (unsigned long long)(s_base + tot);
+    }
+    __syncthreads();
+    u64 slot = s_base + wpre + (inc - cnt);
+#pragma unroll
+    for (int e = 0; e < kEWords; ++e) {
+        u32 bits = words[e];
+        if (!bits) continue;
+        const u64 wi = w0 + e;
+        const u64 i = wi / mw;
+        const u64 jb = (wi - i * mw) * 32;
+        while (bits) {
+            const int b = __ffs(bits) - 1;
+            bits &= bits - 1;
+            const u64 j = jb + (u64)b;
+            if ((i64)slot >= capacity) {
+                raise_status(status, PL_ERR_CAPACITY);
+                ++slot;
+                continue;
+            }
+            PhaseAcc acc;
+#pragma unroll
+            for (int k = 0; k < AS; ++k) {
+                const u64 lx = __ldg(ax + k * sa + i), lz = __ldg(az + k * sa + i);
+                const u64 rx = __ldg(bx + k * sb + j), rz = __ldg(bz + k * sb + j);
+                ox[(i64)k * capacity + (i64)slot] = lx ^ rx;
+                oz[(i64)k * capacity + (i64)slot] = lz ^ rz;
+                acc.step(lx, lz, rx, rz);
+            }
+            of[slot] = (u8)((acc.phase(__ldg(af + i), __ldg(bf + j)) + (u32)mul_i) & 3u);
+            ov[slot] = dmul(dmul(2.0, __ldg(av + i)), __ldg(bv + j));
+            ++slot;
+        }
+    }
+    (void)m;
+}
+
 // A look-back wait whose predecessor never publishes: tile 1 polls tile 0's
 // word, which nothing sets, until the spin limit runs out.
 __global__ void k_wait_check(u64* lb, int* status) {
@@ -205,14 +339,34 @@ __global__ void __launch_bounds__(256) k_cnot(u64* x, u64* z, u8* f, u64 n, u64 
 // zero_state_expectation: one CTA, each thread sums a strided subsequence
 // in order, then a fixed binary tree -- deterministic for a given n.
 // ---------------------------------------------------------------------------
+// zero_state_expectation (PauliSumUtils.h:163-177) over many CTAs: CTA b
+// sums the contiguous range [b*per, (b+1)*per) (each thread a strided
+// share in order, then a fixed tree) into partial[b]; k_zero_state_total
+// adds the partials in a fixed tree.  The grid depends only on the device,
+// so the result is deterministic; its order differs from the reference's
+// left-to-right sum (1e-10 absolute is the bar).
+constexpr int kZThreads = 256;
+
+__device__ __forceinline__ double block_sum_256(double a, double* s) {
+    s[threadIdx.x] = a;
+    __syncthreads();
+    for (int st = kZThreads / 2; st > 0; st >>= 1) {
+        if ((int)threadIdx.x < st) s[threadIdx.x] = dadd(s[threadIdx.x], s[threadIdx.x + st]);
+        __syncthreads();
+    }
+    return s[0];
+}
+
 template <int AS>
-__global__ void __launch_bounds__(1024) k_zero_state(const u64* __restrict__ x,
-                                                     const u8* __restrict__ f,
-                                                     const double* __restrict__ v, u64 n,
-                                                     u64 stride, double* out) {
-    __shared__ double s[1024];
+__global__ void __launch_bounds__(kZThreads) k_zero_state(const u64* __restrict__ x,
+                                                          const u8* __restrict__ f,
+                                                          const double* __restrict__ v, u64 n,
+                                                          u64 stride, u64 per, double* partial) {
+    __shared__ double s[kZThreads];
+    const u64 b0 = (u64)blockIdx.x * per;
+    const u64 b1 = b0 + per < n ? b0 + per : n;
     double acc = 0.0;
-    for (u64 i = threadIdx.x; i < n; i += blockDim.x) {
+    for (u64 i = b0 + threadIdx.x; i < b1; i += kZThreads) {
         u64 any = 0;
 #pragma unroll
         for (int k = 0; k < AS; ++k) any |= __ldg(x + k * stride + i);
@@ -222,13 +376,17 @@ __global__ void __launch_bounds__(1024) k_zero_state(const u64* __restrict__ x,
             acc = dadd(acc, (fl & 2u) ? -val : val);
         }
     }
-    s[threadIdx.x] = acc;
-    __syncthreads();
-    for (int st = blockDim.x / 2; st > 0; st >>= 1) {
-        if ((int)threadIdx.x < st) s[threadIdx.x] = dadd(s[threadIdx.x], s[threadIdx.x + st]);
-        __syncthreads();
-    }
-    if (threadIdx.x == 0) *out = s[0];
+    const double t = block_sum_256(acc, s);
+    if (threadIdx.x == 0) partial[blockIdx.x] = t;
+}
+
+__global__ void __launch_bounds__(kZThreads) k_zero_state_total(const double* partial, int np,
+                                                                double* out) {
+    __shared__ double s[kZThreads];
+    double acc = 0.0;
+    for (int i = threadIdx.x; i < np; i += kZThreads) acc = dadd(acc, partial[i]);
+    const double t = block_sum_256(acc, s);
+    if (threadIdx.x == 0) *out = t;
 }
 
 }  // namespace
@@ -259,6 +417,46 @@ int multiply_impl(int as, const u64* ax, const u64* az, const u8* af, const doub
 size_t commutator_scratch_bytes(u64 npairs) {
     const u64 tiles = (npairs + kCTile - 1) / kCTile;
     return (size_t)tiles * 8 + 256;
+}
+
+// The two-pass form needs a bitmask of n * ceil(m/32) words; it is used when
+// there are enough pairs to fill the device and the mask stays modest.
+constexpr u64 kMaskMaxBytes = 1ull << 30;
+bool use_mask_form(u64 n, u64 m) {
+    const u64 mw = (m + 31) / 32;
+    return n * m >= (1ull << 22) && n * mw * 4 <= kMaskMaxBytes && n <= (1ull << 31) &&
+           m <= (1ull << 31);
+}
+size_t commutator_mask_scratch_bytes(u64 n, u64 m) {
+    const u64 mw = (m + 31) / 32;
+    const u64 tiles = (n * mw + kETileW - 1) / kETileW;
+    return (size_t)(256 + tiles * 8 + 256) + (size_t)(n * mw * 4);
+}
+
+int commutator_launch_mask(int as, int mul_i, const u64* ax, const u64* az, const u8* af,
+                           const double* av, i64 n, i64 sa, const u64* bx, const u64* bz,
+                           const u8* bf, const double* bv, i64 m, i64 sb, u64* ox, u64* oz,
+                           u8* of, double* ov, i64 capacity, unsigned long long* d_count,
+                           void* scratch, int* d_status, cudaStream_t st) {
+    const u64 mw = ((u64)m + 31) / 32;
+    const u64 nwords = (u64)n * mw;
+    const u64 tiles = (nwords + kETileW - 1) / kETileW;
+    unsigned char* s = (unsigned char*)scratch;
+    u32* tile_ctr = (u32*)s;
+    u64* lb = (u64*)(s + 256);
+    u32* mask = (u32*)(s + 256 + tiles * 8 + 256);
+    PL_CUDA_TRY(fill32_async(scratch, 0u, 256 + tiles * 8, st));
+    const dim3 mgrid((unsigned)((m + kMThreads - 1) / kMThreads),
+                     (unsigned)((n + kMLhs - 1) / kMLhs));
+    PL_DISPATCH_AS(as, k_comm_mask<AS><<<mgrid, kMThreads, 0, st>>>(
+                           ax, az, (u64)n, (u64)sa, bx, bz, (u64)m, (u64)sb, mask, mw),
+                   pl::note_launch());
+    PL_DISPATCH_AS(as, k_comm_emit<AS><<<(unsigned)tiles, kMThreads, 0, st>>>(
+                           ax, az, af, av, (u64)sa, bx, bz, bf, bv, (u64)sb, (u64)m, mask,
+                           nwords, mw, mul_i, ox, oz, of, ov, capacity, d_count, lb, tile_ctr,
+                           d_status), pl::note_launch());
+    PL_CUDA_TRY(cudaGetLastError());
+    return PL_OK;
 }
 
 int commutator_launch(int as, int mul_i, const u64* ax, const u64* az, const u8* af,
@@ -299,14 +497,19 @@ int commutator_impl(int as, int mul_i, const u64* ax, const u64* az, const u8* a
     if (!ax || !az || !af || !av || !bx || !bz || !bf || !bv || !ox || !oz || !of || !ov)
         return record_status(PL_ERR_INVALID_ARG, "commutator: null pointer");
     // Stream-ordered scratch: safe when several streams call concurrently.
-    const size_t bytes = commutator_scratch_bytes((u64)n * (u64)m) + 256;
+    const bool two_pass = use_mask_form((u64)n, (u64)m);
+    const size_t bytes = (two_pass ? commutator_mask_scratch_bytes((u64)n, (u64)m)
+                                   : commutator_scratch_bytes((u64)n * (u64)m)) + 256;
     void* scratch = nullptr;
     PL_CUDA_TRY(cudaMallocAsync(&scratch, bytes, st));
     int* d_status = (int*)((unsigned char*)scratch + bytes - 256);
     int rc = PL_OK;
     cudaError_t e = fill32_async(d_status, 0u, sizeof(int), st);
     if (e != cudaSuccess) rc = record_cuda(e);
-    if (rc == PL_OK)
+    if (rc == PL_OK && two_pass)
+        rc = commutator_launch_mask(as, mul_i, ax, az, af, av, n, sa, bx, bz, bf, bv, m, sb, ox,
+                                    oz, of, ov, capacity, d_count, scratch, d_status, st);
+    else if (rc == PL_OK)
         rc = commutator_launch(as, mul_i, ax, az, af, av, n, sa, bx, bz, bf, bv, m, sb, ox, oz,
                                of, ov, capacity, d_count, scratch, d_status, st);
     int dstat = 0;
@@ -420,9 +623,19 @@ extern "C" int pl_zero_state_expectation(int array_size, const uint64_t* x, cons
         return record_status(PL_ERR_INVALID_ARG, "pl_zero_state_expectation: bad argument");
     if (n > 0 && (!x || !flags || !val))
         return record_status(PL_ERR_INVALID_ARG, "pl_zero_state_expectation: null");
-    PL_DISPATCH_AS(array_size, k_zero_state<AS><<<1, 1024, 0, stream>>>(
-                                   (const u64*)x, flags, val, (u64)n, (u64)stride, d_result), pl::note_launch());
-    PL_CUDA_TRY(cudaGetLastError());
+    // one partial per CTA, in stream-ordered scratch from the device pool
+    const int nb = std::max(1, std::min(2 * sm_count(), (int)((n + kZThreads - 1) / kZThreads)));
+    const u64 per = ((u64)n + nb - 1) / (u64)nb;
+    void* scratch = nullptr;
+    PL_CUDA_TRY(cudaMallocAsync(&scratch, sizeof(double) * (size_t)nb, stream));
+    double* partial = static_cast<double*>(scratch);
+    PL_DISPATCH_AS(array_size, k_zero_state<AS><<<nb, kZThreads, 0, stream>>>(
+                                   (const u64*)x, flags, val, (u64)n, (u64)stride, per, partial),
+                   pl::note_launch());
+    k_zero_state_total<<<1, kZThreads, 0, stream>>>(partial, nb, d_result), pl::note_launch();
+    const cudaError_t e = cudaGetLastError();
+    cudaFreeAsync(scratch, stream);
+    PL_CUDA_TRY(e);
     return record_status(PL_OK, nullptr);
 }
 

@@ -73,6 +73,30 @@ def test_commutator_windowed(cuda, oracle, terms):
     assert bit_identical(g, o)
 
 
+@pytest.mark.parametrize("n,m,words,nq", [(2500, 1777, 4, 256), (4099, 1031, 1, 40),
+                                         (1024, 4096, 2, 100)])
+@pytest.mark.parametrize("mul_i", [False, True])
+def test_commutator_two_pass_form(cuda, oracle, n, m, words, nq, mul_i):
+    # n * m >= 2^22 pairs take the bitmask form (k_comm_mask + k_comm_emit):
+    # same terms, same order, same values as the single-threaded CPU
+    # commutator; sizes not multiples of the tile shapes
+    a = random_sum(n, words, 5 + n, nq, "normal")
+    b = random_sum(m, words, 6 + m, nq, "normal")
+    # random strings anticommute about half the time: room for every pair
+    g, o = gpu_commutator(a, b, mul_i, capacity=n * m), oracle.commutator(a, b, mul_i)
+    assert_keys_equal(g, o)
+    assert bit_identical(g, o)
+
+
+def test_commutator_two_pass_capacity(cuda, oracle):
+    from paulib_b200 import _abi
+    a, b = random_sum(2100, 1, 5, 20), random_sum(2100, 1, 6, 20)
+    full = oracle.commutator(a, b)
+    with pytest.raises(_abi.PLError) as e:
+        gpu_commutator(a, b, capacity=full.n // 2)
+    assert e.value.status == _abi.PL_ERR_CAPACITY
+
+
 def test_commutator_commuting_inputs(cuda):
     # GpuPauliSumTests.cpp:339-343.
     g = gpu_commutator(planes([("ZI", 1.0)]), planes([("IZ", 1.0)]))
