@@ -454,6 +454,13 @@ PL_API int pl_serve(const pl_job* jobs, int64_t count, const pl_batch_opts* opts
  * segment sums.  0 (default) or 1: used where it fits; -1: never (the
  * general key + payload sort).  Results are identical either way. */
 #define PL_TUNE_INDEX_KEYS 2
+/* canonicalize() / sort_and_combine() of a sum whose plain key needs more
+ * than 16 digit passes: when every term's x and z bits lie in two
+ * consecutive words and within 16 consecutive bits of each (strings on a
+ * window of adjacent qubits), sort an order-preserving compression of the
+ * key instead.  0 (default) or 1: used where it fits and saves passes; -1:
+ * never.  Results are identical either way. */
+#define PL_TUNE_WINDOW_KEYS 5
 /* Polls a cross-CTA wait (decoupled look-back) makes before it records
  * PL_ERR_TIMEOUT and returns: 1 .. 2^30, 0 = the default 2^20 (with a 64 ns
  * back-off past 64 polls: well under a second).  Written into the device

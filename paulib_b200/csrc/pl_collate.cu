@@ -163,6 +163,82 @@ struct SoASrc {
         fl = phase_bits(phs, i);
         val = __ldg(v + i);
     }
+    // the term as it is output (the sort key above is the term itself)
+    static constexpr bool kVirtualKey = false;
+    __device__ __forceinline__ void orig_key(u32 i, u64* xw, u64* zw, u32& fl) const {
+        key(i, xw, zw, fl);
+    }
+};
+
+// ---------------------------------------------------------------------------
+// Windowed keys.  When every term's x bits (and z bits) lie in two
+// consecutive words and, in each word, within kWinSpan consecutive bits --
+// Pauli strings supported on a window of adjacent qubits -- the sort key
+// (x[0..AS), z[0..AS), flags) compresses, order preserving, to two virtual
+// words per plane:
+//   x'[0] = (AS - f) << 22 | win(x[f]),  x'[1] = win(x[f + 1]),  x'[k] = 0
+// with f the first nonzero word (f = AS, x'[0] = 0 for x == 0) and win(w) =
+// (msb + 1) << (kWinSpan - 1) | the kWinSpan - 1 bits below w's msb.  A
+// smaller f means a larger x, and within one f the two words compare as
+// their win() values; likewise for z.  The varying-bit analysis then runs
+// on the virtual words: for the windowed commutator workload (supports of
+// <= 11 qubits on 256) about 80 varying bits instead of 513.  Sort and
+// segment detection use the virtual key (it is injective on such terms);
+// the emit writes each term's original words, fetched by its index.
+// ---------------------------------------------------------------------------
+constexpr int kWinSpan = 16;
+
+__device__ __forceinline__ u64 win_word(u64 w) {
+    if (!w) return 0;
+    const int msb = 63 - __clzll((long long)w);
+    const u64 below = msb >= kWinSpan - 1 ? (w >> (msb - (kWinSpan - 1)))
+                                          : (w << ((kWinSpan - 1) - msb));
+    return ((u64)(msb + 1) << (kWinSpan - 1)) | (below & ((1ull << (kWinSpan - 1)) - 1ull));
+}
+
+// Virtual words of one plane; returns false when the plane does not fit the
+// window form (nonzero words beyond f + 1, or a word wider than kWinSpan).
+template <int AS>
+__device__ __forceinline__ bool win_plane(const u64* w, u64* out) {
+    int f = AS;
+#pragma unroll
+    for (int k = AS - 1; k >= 0; --k)
+        if (w[k]) f = k;
+    bool ok = true;
+    u64 w0 = 0, w1 = 0;
+#pragma unroll
+    for (int k = 0; k < AS; ++k) {
+        const u64 v = w[k];
+        if (k == f) w0 = v;
+        else if (k == f + 1) w1 = v;
+        else if (v) ok = false;
+        if (v && (63 - __clzll((long long)v)) - (__ffsll((long long)v) - 1) >= kWinSpan)
+            ok = false;
+    }
+    out[0] = f < AS ? ((u64)(AS - f) << 22) | win_word(w0) : 0ull;
+#pragma unroll
+    for (int k = 1; k < AS; ++k) out[k] = k == 1 ? win_word(w1) : 0ull;
+    return ok;
+}
+
+template <int AS>
+struct WinSrc {
+    SoASrc<AS> s;
+    __device__ __forceinline__ bool vkey(u32 i, u64* xw, u64* zw, u32& fl) const {
+        u64 ox[AS], oz[AS];
+        s.key(i, ox, oz, fl);
+        const bool a = win_plane<AS>(ox, xw);
+        const bool b = win_plane<AS>(oz, zw);
+        return a && b;
+    }
+    __device__ __forceinline__ void key(u32 i, u64* xw, u64* zw, u32& fl) const {
+        (void)vkey(i, xw, zw, fl);
+    }
+    __device__ __forceinline__ double value(u32 i) const { return s.value(i); }
+    static constexpr bool kVirtualKey = true;
+    __device__ __forceinline__ void orig_key(u32 i, u64* xw, u64* zw, u32& fl) const {
+        s.key(i, xw, zw, fl);
+    }
 };
 
 // Division by a loop-invariant u32 d via a 32-bit magic multiplier
@@ -226,6 +302,10 @@ struct ProdSrc {
         fl = phase_bits(phs, p);
         val = value(p);
     }
+    static constexpr bool kVirtualKey = false;
+    __device__ __forceinline__ void orig_key(u32 p, u64* xw, u64* zw, u32& fl) const {
+        key(p, xw, zw, fl);
+    }
 };
 
 // ---------------------------------------------------------------------------
@@ -268,6 +348,42 @@ __global__ void __launch_bounds__(256) k_masks(SoASrc<AS> src, u32 n, int mode, 
 //    chunk planes when the key spans several chunks, and the digit
 //    histograms of chunk 0's passes.
 // ---------------------------------------------------------------------------
+// Masks of the windowed virtual key (as k_masks) and whether every term fits
+// the window form (bad[0] != 0: some term does not).
+template <int AS>
+__global__ void __launch_bounds__(256) k_win_masks(WinSrc<AS> src, u32 n, int mode, u64* orm,
+                                                   u64* andm, u32* bad) {
+    u64 o[2 * AS + 1], a[2 * AS + 1];
+#pragma unroll
+    for (int f = 0; f < 2 * AS + 1; ++f) { o[f] = 0; a[f] = ~0ull; }
+    bool fits = true;
+    for (u32 i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        u64 xw[AS], zw[AS];
+        u32 fl;
+        fits = src.vkey(i, xw, zw, fl) && fits;
+#pragma unroll
+        for (int k = 0; k < AS; ++k) {
+            o[k] |= xw[k]; a[k] &= xw[k];
+            o[AS + k] |= zw[k]; a[AS + k] &= zw[k];
+        }
+        const u64 fv = flags_field(fl, mode);
+        o[2 * AS] |= fv;
+        a[2 * AS] &= fv;
+    }
+#pragma unroll
+    for (int f = 0; f < 2 * AS + 1; ++f) {
+        for (int s2 = 16; s2 > 0; s2 >>= 1) {
+            o[f] |= __shfl_xor_sync(0xffffffffu, o[f], s2);
+            a[f] &= __shfl_xor_sync(0xffffffffu, a[f], s2);
+        }
+        if ((threadIdx.x & 31) == 0) {
+            atomicOr(orm + f, o[f]);
+            atomicAnd(andm + f, a[f]);
+        }
+    }
+    if (!__all_sync(0xffffffffu, fits) && (threadIdx.x & 31) == 0) atomicOr(bad, 1u);
+}
+
 template <int AS, class Src>
 __global__ void __launch_bounds__(256) k_pack(Src src, u32 n, int mode, KeyLayout L,
                                               PassPlan P, u32 count_mask, u64* keys, u32* pay,
@@ -1248,12 +1364,12 @@ template <int AS, class Src>
 __device__ __forceinline__ void emit_key(const Src& src, const KeyLayout& L, u64 packed,
                                          const u32* pay, u32 pos, int mode, u64* xw, u64* zw,
                                          u32& fl) {
-    if (L.nchunks == 1) {
+    if (L.nchunks == 1 && !Src::kVirtualKey) {
         u32 fv;
         unpack_key<AS>(L, packed, xw, zw, fv);
         fl = out_flags(fv, mode);
     } else {
-        src.key(pay[pos] & kIdxMask, xw, zw, fl);
+        src.orig_key(pay[pos] & kIdxMask, xw, zw, fl);
         fl = mode == kCombine ? (fl & 3u) : (fl & 1u);
     }
 }
@@ -1641,6 +1757,11 @@ u32 derive_histograms(const SoASrc<AS>&, const KeyLayout&, const PassPlan&, Bufs
                       cudaStream_t) {
     return 0u;
 }
+template <int AS>
+u32 derive_histograms(const WinSrc<AS>&, const KeyLayout&, const PassPlan&, Bufs&,
+                      cudaStream_t) {
+    return 0u;
+}
 
 // Products: chunk-0 passes free of flags bits come from operand histograms.
 template <int AS>
@@ -1916,6 +2037,48 @@ bool try_split(const Src& src, u32 n, const u64* orm, const u64* andm, const Col
     return true;
 }
 
+// The windowed layout (WinSrc) for a wide key: taken when every term fits
+// the window form and it needs fewer digit passes than the plain layout
+// (canonicalize and sort_and_combine without a weight filter; results are
+// identical either way, PL_TUNE_WINDOW_KEYS = -1 switches it off).
+template <int AS>
+bool try_window(const SoASrc<AS>& src, u32 n, const PassPlan& P0, const CollateArgs& a,
+                const SoAOut& out, i64* out_count, Bufs& B, cudaStream_t st, int* rc) {
+    if (AS < 2 || P0.npasses <= 16 || a.max_weight != ~0ull || a.mode == kProp ||
+        tuning(PL_TUNE_WINDOW_KEYS) < 0)
+        return false;
+    const WinSrc<AS> ws{src};
+    u64* vor = B.orm + kMaxFields;
+    u64* vand = B.andm + kMaxFields;
+    u32* bad = B.counters + 127;
+    const FillReq fm[3] = {{vor, 0u, 8 * kMaxFields},
+                           {vand, 0xffffffffu, 8 * kMaxFields},
+                           {bad, 0u, sizeof(u32)}};
+    cudaError_t e = fill32_multi(fm, 3, st);
+    if (e == cudaSuccess) {
+        k_win_masks<AS><<<grid_for(n, 256, sm_count() * 4), 256, 0, st>>>(ws, n, a.mode, vor,
+                                                                         vand, bad);
+        pl::note_launch();
+        e = cudaGetLastError();
+    }
+    u64 hor[kMaxFields], hand[kMaxFields];
+    u32 hbad = 1;
+    const ReadReq rr[3] = {{hor, vor, 8 * kMaxFields}, {hand, vand, 8 * kMaxFields},
+                           {&hbad, bad, sizeof(u32)}};
+    if (e == cudaSuccess) e = readback_sync(rr, 3, st);
+    if (e != cudaSuccess) {
+        *rc = record_cuda(e);
+        return true;
+    }
+    if (hbad) return false;
+    KeyLayout L;
+    PassPlan P;
+    build_layout(AS, a.mode, hor, hand, L, P);
+    if (P.npasses >= P0.npasses) return false;
+    *rc = run_collate<AS>(ws, n, a.mode, L, P, a, out, out_count, B, st);
+    return true;
+}
+
 }  // namespace
 
 PL_SPIN_LIMIT_SETTER(set_spin_limit_collate)
@@ -1967,7 +2130,8 @@ int collate_soa(int as, const SoAView& in, const SoAOut& out, const CollateArgs&
             KeyLayout L;
             PassPlan P;
             build_layout(AS, a.mode, hor, hand, L, P);
-            rc = run_collate<AS>(src, n, a.mode, L, P, a, out, out_count, B, st);
+            if (!try_window<AS>(src, n, P, a, out, out_count, B, st, &rc))
+                rc = run_collate<AS>(src, n, a.mode, L, P, a, out, out_count, B, st);
         }
     });
     return rc;

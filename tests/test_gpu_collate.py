@@ -136,3 +136,45 @@ def test_commutator_workload_collate(cuda, oracle):
     oc = oracle.commutator(a, b)
     o = oracle.cutoff(oracle.canonicalize(oc), 1e-14)
     _check(g, o, oc, oracle)
+
+
+def _windowed(n, nq, seed, lo=2, hi=6):
+    from paulib_b200.workloads import window_sums
+    a, b = window_sums(seed=seed, terms=n, num_qubits=nq, min_len=lo, max_len=hi)
+    return Planes(a.x, a.z, a.flags, a.val), Planes(b.x, b.z, b.flags, b.val)
+
+
+def _with_window_keys(value, fn):
+    from paulib_b200 import _abi
+    L = _abi.lib()
+    _abi.check(L.pl_set_tuning(_abi.PL_TUNE_WINDOW_KEYS, value))
+    try:
+        return fn()
+    finally:
+        _abi.check(L.pl_set_tuning(_abi.PL_TUNE_WINDOW_KEYS, 0))
+
+
+@pytest.mark.parametrize("mode", [CANON, COMBINE])
+@pytest.mark.parametrize("nq,n", [(256, 40000), (128, 30000), (1000, 20000)])
+def test_window_keys_match_plain_layout_and_oracle(cuda, oracle, mode, nq, n):
+    # commutator output of windowed sums: products of overlapping windows,
+    # every term's support within <= 11 adjacent qubits (PL_TUNE_WINDOW_KEYS)
+    a, b = _windowed(1500, nq, seed=n)
+    raw = oracle.commutator(a, b)
+    rng = np.random.default_rng(n)
+    raw = Planes(raw.x, raw.z, rng.integers(0, 4, raw.n).astype(np.uint8), raw.val)
+    on = _with_window_keys(0, lambda: gpu_collate(raw, mode))
+    off = _with_window_keys(-1, lambda: gpu_collate(raw, mode))
+    o = oracle.canonicalize(raw) if mode == CANON else oracle.sort_and_combine(raw)
+    assert_keys_equal(on, o)
+    assert bit_identical(on, off)
+    assert_values_close(on, o, abs_scale(oracle, raw))
+
+
+def test_window_keys_fall_back_on_wide_supports(cuda, oracle):
+    # random strings over 256 qubits do not fit the window form
+    p = random_sum(20000, 4, 31, 256, "normal")
+    g = _with_window_keys(0, lambda: gpu_collate(p, CANON, cutoff=1e-3))
+    o = oracle.cutoff(oracle.canonicalize(p), 1e-3)
+    assert_keys_equal(g, o)
+    assert_values_close(g, o, abs_scale(oracle, p))
