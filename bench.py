@@ -422,6 +422,7 @@ def run_product_collate(args, rank, local, ws):
         line["propagation"] = propagation_extra(args, peak)
         line["served"] = served_extra(args)
         line["batch"] = batch_extra(args)
+        line["commutator"] = commutator_extra(args, peak)
     return line
 
 
@@ -635,6 +636,39 @@ def batch_extra(args):
             "speedup_bound_by_longest_job": c["speedup_bound_by_longest_job"],
             "results_identical_to_plain": c["results_identical_to_plain"],
             "tuned": c["tuned"], "timing": c["timing"]}
+
+
+def commutator_extra(args, peak):
+    """Commutator + canonicalize + cutoff(1e-14) of two 16384-term sums on
+    256 qubits (windowed supports, array_size 4), with the collate's byte
+    models: B_canon over the plain key's varying bits (the reference
+    algorithm's sort), and the digit passes actually run."""
+    import numpy as np
+    from paulib_b200 import benchmarks
+    ns = argparse.Namespace(steps=10, warmup=3)
+    line, emitted_planes = benchmarks.run_commutator_with_output(ns)
+    c = line["config"]
+    x, z = emitted_planes
+    var = 0
+    for w in range(x.shape[0]):
+        var += bin(int(np.bitwise_or.reduce(x[w]) ^ np.bitwise_and.reduce(x[w]))).count("1")
+        var += bin(int(np.bitwise_or.reduce(z[w]) ^ np.bitwise_and.reduce(z[w]))).count("1")
+    bits = var + 1  # the phase after the sign fold
+    s_term = 16 * 4 + 9
+    collate_ms = line["ms_per_step"] - c["commutator_ms"]
+    bc = b_canon(c["emitted"], c["terms_out"], bits, s_term, s_term)
+    return {"workload": c["workload"], "pairs": c["pairs"], "emitted": c["emitted"],
+            "terms_out": c["terms_out"], "ms_per_step": line["ms_per_step"],
+            "commutator_ms": c["commutator_ms"], "collate_ms": collate_ms,
+            "value": line["value"], "unit": line["unit"],
+            "digit_passes_per_step": c["radix_passes_per_step"],
+            "collate_kernels": c["collate_kernels"],
+            "digit_pass_ms": c["radix_pass_ms"], "digit_pass_gbs": c["radix_pass_gbs"],
+            "plain_key_varying_bits": bits,
+            "b_canon": {"bytes_model": "B_canon(emitted, terms_out, b) with S = 73 B",
+                        "bits": bits, "bytes": bc,
+                        "equivalent_gbs": bc / (collate_ms / 1e3) / 1e9,
+                        "equivalent_frac": bc / (collate_ms / 1e3) / 1e9 / peak}}
 
 
 def torch_local_rank():

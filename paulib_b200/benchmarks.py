@@ -231,7 +231,15 @@ def propagation_summary(seed=2, num_qubits=64, layers=20, steps=3, warmup=2, pea
     return out
 
 
-def _commutator(args, rank, ws):
+def run_commutator_with_output(args):
+    """The commutator workload on this process's GPU (rank 0 operands); also
+    returns the emitted terms' x and z planes (host copies) of the last step."""
+    line, out, emitted = _commutator(args, 0, 1, keep=True)
+    x, z, _, _ = out.to_host(emitted)
+    return line, (x, z)
+
+
+def _commutator(args, rank, ws, keep=False):
     import torch
     a, b = W.window_sums(seed=3 + rank)
     L = _abi.lib()
@@ -280,10 +288,12 @@ def _commutator(args, rank, ws):
         t_comm.append(e0.elapsed_time(e1))
         t_all.append(e0.elapsed_time(e2))
     launches, tn, tms, tb = _abi.profile_read()
+    kernels = {k: {"launches": c // steps, "ms_per_step": t / steps}
+               for k, (c, t, _) in _abi.profile_report().items()}
     _abi.profile_reset(False)
     ms = sum(t_all) / steps
     pairs = a.n * b.n
-    return {"metric": "Pauli products collated/s", "value": ws * pairs / (ms / 1e3),
+    line = {"metric": "Pauli products collated/s", "value": ws * pairs / (ms / 1e3),
             "unit": "pairs/s", "n_gpus": ws, "steps": steps, "warmup": args.warmup,
             "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "u64 keys / f64 coefficients",
@@ -294,8 +304,13 @@ def _commutator(args, rank, ws):
                        "commutator_ms": sum(t_comm) / steps,
                        "radix_passes_per_step": tn // steps,
                        "radix_pass_ms": tms / max(tn, 1),
-                       "radix_pass_gbs": (tb / max(tn, 1)) / (tms / max(tn, 1) / 1e3) / 1e9},
+                       "radix_pass_gbs": (tb / max(tn, 1)) / (tms / max(tn, 1) / 1e3) / 1e9
+                       if tn else None,
+                       "collate_kernels": kernels},
             "gpu_launches": int(launches // steps)}
+    if keep:
+        return line, out, emitted
+    return line
 
 
 def _batch_jobs(args, rank):

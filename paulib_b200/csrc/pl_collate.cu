@@ -46,7 +46,9 @@ constexpr int kWarps = kThreads / 32;
 constexpr u32 kIdxMask = 0x7fffffffu;
 constexpr u32 kSentinel = 0xffffffffu;
 constexpr int kMaxFields = 2 * kMaxAS + 1;
-constexpr int kMaxPasses = 72;
+// Digit passes of the widest key: 2 * 64 * kMaxAS x / z bits and the flags
+// field, in chunks of 64 bits of up to 8 passes each.
+constexpr int kMaxPasses = 8 * ((2 * 64 * kMaxAS + 2 + 63) / 64);
 constexpr u32 kFlagAgg = 1u << 30;
 constexpr u32 kFlagPre = 2u << 30;
 constexpr u32 kCountMask = (1u << 30) - 1;
@@ -1568,6 +1570,11 @@ __global__ void __launch_bounds__(kThreads) k_emit(Src src, KeyLayout L, const u
 // Host side.
 // ---------------------------------------------------------------------------
 inline size_t al(size_t b) { return (b + 255) & ~size_t(255); }
+// counters: [2] pending segments, [3] emit tiles, [8 + p] tile counter of
+// digit pass p; then the operand histograms of a product (kHistScratch,
+// 16 * kRadix words); the last word is the windowed-key check.
+constexpr int kHistScratch = 8 + kMaxPasses;
+constexpr int kCounterWords = kHistScratch + 16 * 256 + 8;
 
 // Bump allocator over the workspace; with base == nullptr it only measures.
 struct Carve {
@@ -1622,7 +1629,7 @@ void carve_all(Carve& c, i64 n, int nch, Bufs& B) {
     B.tile_kept = c.take<u32>(etiles);
     B.tile_off = c.take<u32>(etiles);
     B.lb_emit = c.take<u32>(etiles);
-    B.counters = c.take<u32>(128 + 16 * kRadix);
+    B.counters = c.take<u32>(kCounterWords);
     B.orm = c.take<u64>(2 * kMaxFields);   // one set per operand of a product
     B.andm = c.take<u64>(2 * kMaxFields);
     B.d_count = c.take<i64>(1);
@@ -1773,7 +1780,7 @@ u32 derive_histograms(const ProdSrc<AS>& src, const KeyLayout& L, const PassPlan
     for (int p = 0; p < np0; ++p)
         if (P.shift[p] >= wf) mask |= 1u << p;
     if (!mask) return 0u;
-    u32* hA = B.counters + 128;                   // scratch after the counters
+    u32* hA = B.counters + kHistScratch;          // scratch after the pass counters
     u32* hB = hA + 8 * kRadix;
     if (fill32_async(hA, 0u, sizeof(u32) * 16 * kRadix, st) != cudaSuccess) return 0u;
     const SoASrc<AS> a{src.ax, src.az, src.af, src.av, src.sa};
@@ -1852,8 +1859,8 @@ int run_collate(const Src& src, u32 n, int mode, const KeyLayout& L, const PassP
     const int items = radix_items();
     const u32 rtiles = (n + kThreads * items - 1) / (kThreads * items);
     const int nsm = sm_count();
-    const FillReq fr[4] = {{B.hist, 0u, sizeof(u32) * kMaxPasses * kRadix},
-                           {B.counters, 0u, sizeof(u32) * (kMaxPasses + 8)},
+    const FillReq fr[4] = {{B.hist, 0u, sizeof(u32) * (size_t)std::max(P.npasses, 1) * kRadix},
+                           {B.counters, 0u, sizeof(u32) * (size_t)(P.npasses + 8)},
                            {B.d_status, 0u, sizeof(int)},
                            {B.d_count, 0u, sizeof(i64)}};
     PL_CUDA_TRY(fill32_multi(fr, 4, st));
@@ -1958,8 +1965,8 @@ int run_collate_split(const Src& src, u32 n, const KeyLayout& L, const PassPlan&
     uint2* phs = reinterpret_cast<uint2*>(B.planes);
     double2* seg2 = reinterpret_cast<double2*>(reinterpret_cast<unsigned char*>(B.planes) + al(n));
     const u32 etiles0 = (n + kETile - 1) / kETile;
-    const FillReq fr[5] = {{B.hist, 0u, sizeof(u32) * kMaxPasses * kRadix},
-                           {B.counters, 0u, sizeof(u32) * (kMaxPasses + 8)},
+    const FillReq fr[5] = {{B.hist, 0u, sizeof(u32) * (size_t)std::max(P.npasses, 1) * kRadix},
+                           {B.counters, 0u, sizeof(u32) * (size_t)(P.npasses + 8)},
                            {B.d_status, 0u, sizeof(int)},
                            {B.d_count, 0u, sizeof(i64)},
                            {B.tile_kept, 0u, sizeof(u32) * etiles0}};
@@ -2050,7 +2057,7 @@ bool try_window(const SoASrc<AS>& src, u32 n, const PassPlan& P0, const CollateA
     const WinSrc<AS> ws{src};
     u64* vor = B.orm + kMaxFields;
     u64* vand = B.andm + kMaxFields;
-    u32* bad = B.counters + 127;
+    u32* bad = B.counters + kCounterWords - 1;  // past every pass counter
     const FillReq fm[3] = {{vor, 0u, 8 * kMaxFields},
                            {vand, 0xffffffffu, 8 * kMaxFields},
                            {bad, 0u, sizeof(u32)}};

@@ -501,7 +501,12 @@ int commutator_impl(int as, int mul_i, const u64* ax, const u64* az, const u8* a
     const size_t bytes = (two_pass ? commutator_mask_scratch_bytes((u64)n, (u64)m)
                                    : commutator_scratch_bytes((u64)n * (u64)m)) + 256;
     void* scratch = nullptr;
-    PL_CUDA_TRY(cudaMallocAsync(&scratch, bytes, st));
+    // from the device pool with its cached blocks kept (dev_alloc): a call
+    // then maps no fresh memory
+    if (dev_alloc(&scratch, bytes, st) != cudaSuccess) {
+        cudaGetLastError();
+        return record_status(PL_ERR_OOM, "commutator scratch");
+    }
     int* d_status = (int*)((unsigned char*)scratch + bytes - 256);
     int rc = PL_OK;
     cudaError_t e = fill32_async(d_status, 0u, sizeof(int), st);
@@ -519,7 +524,7 @@ int commutator_impl(int as, int mul_i, const u64* ax, const u64* az, const u8* a
         e = readback_sync(rr, 1, st);
         if (e != cudaSuccess) rc = record_cuda(e);
     }
-    cudaFreeAsync(scratch, st);
+    dev_free(scratch, st);
     if (rc != PL_OK) return rc;
     if (dstat != 0) return record_status(dstat, "commutator: device-side check");
     return record_status(PL_OK, nullptr);
@@ -627,14 +632,17 @@ extern "C" int pl_zero_state_expectation(int array_size, const uint64_t* x, cons
     const int nb = std::max(1, std::min(2 * sm_count(), (int)((n + kZThreads - 1) / kZThreads)));
     const u64 per = ((u64)n + nb - 1) / (u64)nb;
     void* scratch = nullptr;
-    PL_CUDA_TRY(cudaMallocAsync(&scratch, sizeof(double) * (size_t)nb, stream));
+    if (dev_alloc(&scratch, sizeof(double) * (size_t)nb, stream) != cudaSuccess) {
+        cudaGetLastError();
+        return record_status(PL_ERR_OOM, "zero_state_expectation scratch");
+    }
     double* partial = static_cast<double*>(scratch);
     PL_DISPATCH_AS(array_size, k_zero_state<AS><<<nb, kZThreads, 0, stream>>>(
                                    (const u64*)x, flags, val, (u64)n, (u64)stride, per, partial),
                    pl::note_launch());
     k_zero_state_total<<<1, kZThreads, 0, stream>>>(partial, nb, d_result), pl::note_launch();
     const cudaError_t e = cudaGetLastError();
-    cudaFreeAsync(scratch, stream);
+    dev_free(scratch, stream);
     PL_CUDA_TRY(e);
     return record_status(PL_OK, nullptr);
 }
