@@ -1958,6 +1958,10 @@ struct pl_state {
     i64 log_ops = 0;       // ops the log holds
     i64 log_used = 0;      // ops of the last propagation
     const volatile int32_t* cancel = nullptr;  // pl_state_set_cancel_flag
+    // Terms at the last host read of the size: the chain kernels' grids are
+    // sized from it (their tile loops cover any size, so a stale value only
+    // costs speed, never correctness).
+    i64 size_hint = 0;
 };
 
 namespace pl {
@@ -2099,6 +2103,21 @@ int state_grow(pl_state* s, i64 need) {
 int read_size(pl_state* s, i64* n) {
     PL_CUDA_TRY(cudaMemcpyAsync(n, s->d_size + s->cur, sizeof(i64), cudaMemcpyDeviceToHost, s->st));
     PL_CUDA_TRY(cudaStreamSynchronize(s->st));
+    s->size_hint = *n;
+    return PL_OK;
+}
+
+// Status word, failing op and the current size in one synchronisation.
+int read_status_size(pl_state* s, int* status, int* fail) {
+    int v[2] = {0, 0};
+    i64 n = 0;
+    PL_CUDA_TRY(cudaMemcpyAsync(v, s->d_status, sizeof(v), cudaMemcpyDeviceToHost, s->st));
+    PL_CUDA_TRY(cudaMemcpyAsync(&n, s->d_size + s->cur, sizeof(i64), cudaMemcpyDeviceToHost,
+                                s->st));
+    PL_CUDA_TRY(cudaStreamSynchronize(s->st));
+    *status = v[0];
+    *fail = v[1];
+    if (v[0] == 0) s->size_hint = n;
     return PL_OK;
 }
 
@@ -2220,26 +2239,40 @@ int rotation_chain(pl_state* s, int in, int op, const pl_truncation& tr, bool ti
     const int outb = 1 - in;
     constexpr int T = ptile<AS>();
     const auto* table = static_cast<const GateRec<AS>*>(s->d_table);
-    const int pgrid = std::max(1, std::min((int)((s->max_tiles + 8) / 8), sm_count() * 8));
+    int pgrid = std::max(1, std::min((int)((s->max_tiles + 8) / 8), sm_count() * 8));
+    const int full = grid_persistent(AS == 1 ? 4 : 2);
+    int gexp = full, gruns = full, gred = full;
+    if (timed) {
+        // launched kernel by kernel: grids for the terms the chain can meet
+        // before the next size read (a small state leaves the SMs to other
+        // lanes' kernels); a captured chain keeps full grids, as it is
+        // replayed at every size
+        const i64 est = 4 * s->size_hint + 65536;
+        auto cl = [](i64 v, int hi) { return (int)std::max<i64>(1, std::min<i64>(v, hi)); };
+        gexp = cl((est + kExpTile - 1) / kExpTile, full);
+        gruns = cl((est + T - 1) / T, full);
+        gred = cl((2 * est + T - 1) / T, full);
+        pgrid = cl((2 * est / T + 8) / 8 + 1, pgrid);
+    }
     const u64 mw = tr.max_weight;
     const double cut = tr.coefficient_cutoff > 0.0 ? tr.coefficient_cutoff : 0.0;
     cudaEvent_t e0 = timed ? timed_begin(s->st) : nullptr;
     k_rot_begin<<<sm_count(), 256, 0, s->st>>>(reinterpret_cast<uint4*>(s->lbA), s->zero_bytes / 16,
                                                s->d_cursor, op);
-    k_expand<AS><<<grid_persistent(AS == 1 ? 4 : 2), kPT, 0, s->st>>>(
+    k_expand<AS><<<gexp, kPT, 0, s->st>>>(
         s->S[in], s->d_size + in, table, s->d_cursor, s->R0, s->R1, s->d_k, s->lbA, s->ctr + 0,
         s->d_status, s->cap, s->d_fail);
     if (timed) timed_end(e0, s->st, "k_expand", 0ull);
     e0 = timed ? timed_begin(s->st) : nullptr;
     k_partition<AS><<<pgrid, 256, 0, s->st>>>(s->R0, s->d_k, s->R1, s->d_k + 1, nullptr, T,
                                               s->spB_lo, s->spB_hi, s->max_tiles, s->d_status);
-    k_merge_runs<AS><<<grid_persistent(AS == 1 ? 4 : 2), kPT, tile_smem_bytes<AS>(T), s->st>>>(
+    k_merge_runs<AS><<<gruns, kPT, tile_smem_bytes<AS>(T), s->st>>>(
         s->R0, s->R1, s->d_k, s->spB_lo, s->spB_hi, s->N, s->ctr + 1, s->d_status);
     k_partition<AS><<<pgrid, 256, 0, s->st>>>(s->S[in], s->d_size + in, s->N, s->d_k, s->d_k + 1,
                                               T, s->spC_lo, s->spC_hi, s->max_tiles, s->d_status);
     if (timed) timed_end(e0, s->st, "k_merge_runs+partitions", 0ull);
     e0 = timed ? timed_begin(s->st) : nullptr;
-    k_merge_reduce<AS><<<grid_persistent(AS == 1 ? 4 : 2), kPT, tile_smem_bytes<AS>(T + 2), s->st>>>(
+    k_merge_reduce<AS><<<gred, kPT, tile_smem_bytes<AS>(T + 2), s->st>>>(
         s->S[in], s->d_size + in, s->N, s->d_k, s->spC_lo, s->spC_hi, table, s->d_cursor,
         s->S[outb], s->d_size + outb, mw, cut, s->lbC, s->ctr + 2, s->d_status, s->d_fail);
     if (timed) timed_end(e0, s->st, "k_merge_reduce", 0ull);
@@ -2500,6 +2533,11 @@ int run_ops(pl_state* s, const std::vector<Rot>& rots, const std::vector<Op>& op
         modes[r] = classify(rots[r].theta, &cs[r], &sns[r]);
     }
     if (ops.empty()) return PL_OK;
+    {
+        i64 n0 = 0;  // the size the first chains' grids are sized from
+        rc = read_size(s, &n0);
+        if (rc) return rc;
+    }
     if (s->gate_log) {
         if (s->log_ops < (i64)ops.size()) {
             // captured chains hold the log's address
@@ -2547,7 +2585,7 @@ int run_ops(pl_state* s, const std::vector<Rot>& rots, const std::vector<Op>& op
     auto checkpoint = [&](bool* rewound) -> int {
         *rewound = false;
         int st = 0, fail = 0;
-        int r = read_status(s, &st, &fail);
+        int r = read_status_size(s, &st, &fail);
         if (r) return r;
         since_sync = 0;
         pending = false;
@@ -2876,6 +2914,7 @@ extern "C" int pl_state_upload(pl_state* s, const uint64_t* x, const uint64_t* z
     PL_CUDA_TRY(cudaMemsetAsync(s->d_status, 0, 2 * sizeof(int), s->st));
     PL_CUDA_TRY(cudaStreamSynchronize(s->st));
     s->cls = 0;
+    s->size_hint = n;
     return record_status(PL_OK, nullptr);
 }
 
