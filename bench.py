@@ -246,27 +246,30 @@ def run_product_collate(args, rank, local, ws):
 
     # ---- autotune: keys per thread of the digit pass -------------------
     tune_trials = []
-    for items in (8, 12, 16):
-        _abi.check(L.pl_set_tuning(_abi.PL_TUNE_RADIX_ITEMS, items), "pl_set_tuning")
-        step()
-        torch.cuda.synchronize()
-        t0 = torch.cuda.Event(enable_timing=True)
-        t1 = torch.cuda.Event(enable_timing=True)
-        t0.record(stream)
-        for _ in range(3):
+    for prefetch in (0, -1):  # L2 prefetch one wave ahead / off
+        for items in (8, 12, 16):
+            _abi.check(L.pl_set_tuning(_abi.PL_TUNE_RADIX_ITEMS, items), "pl_set_tuning")
+            _abi.check(L.pl_set_tuning(_abi.PL_TUNE_RADIX_PREFETCH, prefetch), "pl_set_tuning")
             step()
-        t1.record(stream)
-        torch.cuda.synchronize()
-        tune_trials.append({"radix_items": items, "ms_per_step": t0.elapsed_time(t1) / 3})
+            torch.cuda.synchronize()
+            t0 = torch.cuda.Event(enable_timing=True)
+            t1 = torch.cuda.Event(enable_timing=True)
+            t0.record(stream)
+            for _ in range(3):
+                step()
+            t1.record(stream)
+            torch.cuda.synchronize()
+            tune_trials.append({"radix_items": items, "radix_prefetch": prefetch,
+                                "ms_per_step": t0.elapsed_time(t1) / 3})
     best = min(tune_trials, key=lambda t: t["ms_per_step"])
-    tune_ms = [t["ms_per_step"] for t in tune_trials]
-    best_items = best["radix_items"]
+    best_items, best_pf = best["radix_items"], best["radix_prefetch"]
     if ws > 1:  # every rank uses rank 0's choice
         import torch.distributed as dist
-        t = torch.tensor([best_items], device="cuda")
+        t = torch.tensor([best_items, best_pf], device="cuda")
         dist.broadcast(t, 0)
-        best_items = int(t.item())
+        best_items, best_pf = int(t[0].item()), int(t[1].item())
     _abi.check(L.pl_set_tuning(_abi.PL_TUNE_RADIX_ITEMS, best_items), "pl_set_tuning")
+    _abi.check(L.pl_set_tuning(_abi.PL_TUNE_RADIX_PREFETCH, best_pf), "pl_set_tuning")
     for _ in range(args.warmup):
         n_out = step()
     torch.cuda.synchronize()
@@ -392,8 +395,10 @@ def run_product_collate(args, rank, local, ws):
                 "product+collate benchmark",
         "config": product_config(ws, n, m),
         "result": {"terms_out": n_out},
-        "tuned": {"radix_items": best_items,
-                  "trials_ms_per_step": dict(zip(("8", "12", "16"), tune_ms))},
+        "tuned": {"radix_items": best_items, "radix_l2_prefetch": best_pf == 0,
+                  "trials_ms_per_step": {
+                      f"{'prefetch' if t['radix_prefetch'] == 0 else 'plain'}-{t['radix_items']}":
+                      t["ms_per_step"] for t in tune_trials}},
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d,
                 "d2h_bytes_per_step": int(statistics.mean(d2h)),
                 "path": "pinned host planes -> H2D -> pl_multiply_collate (C ABI) -> D2H of "

@@ -707,6 +707,12 @@ struct RadixSmem {
     u32 tile;
 };
 
+// Bulk prefetch of [p, p + bytes) into L2 (a hint; p 16-byte aligned, bytes a
+// multiple of 16).
+__device__ __forceinline__ void prefetch_l2(const void* p, u32 bytes) {
+    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(p), "r"(bytes) : "memory");
+}
+
 // LAST: the final pass also fetches each term's coefficient from the source
 // and writes it in sorted order, so the segment sums read contiguous values.
 // KONLY: index-packed keys (the term index in the bits below the digits) and
@@ -719,13 +725,25 @@ __global__ void __launch_bounds__(kThreads, KONLY ? (ITEMS <= 12 ? 4 : 3)
     k_radix_pass(const u64* __restrict__ kin, const u32* __restrict__ vin, u64* __restrict__ kout,
                  u32* __restrict__ vout, u32 n, int shift, int bits,
                  const u32* __restrict__ bstart, u32* lb, u32* tile_ctr, int* status, Src src,
-                 double* __restrict__ val_out, const uint2* __restrict__ phs, u64 imask) {
+                 double* __restrict__ val_out, const uint2* __restrict__ phs, u64 imask,
+                 u32 pf_ahead) {
     extern __shared__ __align__(16) unsigned char dsm[];
     u64* skeys = reinterpret_cast<u64*>(dsm);
     u32* svals = reinterpret_cast<u32*>(dsm + sizeof(u64) * (kThreads * ITEMS));
     __shared__ RadixSmem S;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    if (tid == 0) S.tile = atomicAdd(tile_ctr, 1u);
+    if (tid == 0) {
+        const u32 t = atomicAdd(tile_ctr, 1u);
+        S.tile = t;
+        // The tile about one wave ahead goes to L2 now, so the CTA that takes
+        // it finds its keys there instead of waiting on DRAM.
+        const u32 pt = t + pf_ahead;
+        if (pf_ahead && (u64)(pt + 1) * (kThreads * ITEMS) <= n) {
+            prefetch_l2(kin + (size_t)pt * (kThreads * ITEMS), 8u * (kThreads * ITEMS));
+            if constexpr (!KONLY)
+                prefetch_l2(vin + (size_t)pt * (kThreads * ITEMS), 4u * (kThreads * ITEMS));
+        }
+    }
     for (int i = tid; i < kWarps * kRadix; i += kThreads) S.whist[i] = 0;
     __syncthreads();
     const u32 tile = S.tile;
@@ -876,6 +894,293 @@ constexpr size_t radix_smem(int items) { return (sizeof(u64) + sizeof(u32)) * kT
 constexpr size_t radix_smem_konly(int items) { return sizeof(u64) * kThreads * items; }
 
 // ---------------------------------------------------------------------------
+// 3b. Warp-specialised digit pass over index-packed keys.  A persistent CTA
+//     holds two tile buffers in shared memory.  Two producer warps take the
+//     next tile from the pass counter as soon as a buffer is free, bulk-copy
+//     its keys in (the TMA engine: cp.async.bulk, completion counted on an
+//     mbarrier), count its digit histogram and publish the tile's look-back
+//     aggregate at once.  Eight consumer warps meanwhile rank, scatter,
+//     walk the look-back and write out the previous tile.  Because every
+//     taken tile publishes its aggregate one copy and one count after it is
+//     taken -- never after a whole tile of other work -- taking tiles ahead
+//     does not stall anyone's look-back, and the DRAM latency of the key
+//     load overlaps the consumers' work.  Nothing waits on an unstarted CTA,
+//     so the grid need not be co-resident.  Same results as
+//     k_radix_pass<..., KONLY>: the same stable ranking and scatter.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ u32 smem_u32(const void* p) {
+    return (u32)__cvta_generic_to_shared(p);
+}
+__device__ __forceinline__ void mbar_init(u64* bar, u32 count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count)
+                 : "memory");
+}
+__device__ __forceinline__ void mbar_arrive(u64* bar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(u64* bar, u32 bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)),
+                 "r"(bytes)
+                 : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(u64* bar, u32 parity) {
+    u32 ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+// Bounded wait for the completion of the phase with the given parity; false
+// (and PL_ERR_TIMEOUT recorded) once g_spin_limit polls have run out.
+__device__ __forceinline__ bool mbar_wait(u64* bar, u32 parity, int* status) {
+    for (u32 spins = 0; !mbar_try_wait(bar, parity);) {
+        if (++spins > g_spin_limit) {
+            raise_status(status, PL_ERR_TIMEOUT);
+            return false;
+        }
+    }
+    return true;
+}
+// Global -> shared bulk copy without multicast; dst and src 16-byte aligned,
+// bytes a multiple of 16; completion counted on `bar` as transaction bytes.
+__device__ __forceinline__ void bulk_load(void* dst, const void* src, u32 bytes, u64* bar) {
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+        ::"r"(smem_u32(dst)), "l"(src), "r"(bytes), "r"(smem_u32(bar))
+        : "memory");
+}
+// Named barriers: 1 = the consumer warps, 2 = the producer warps.
+__device__ __forceinline__ void bar_consumers() { asm volatile("bar.sync 1, 256;" ::: "memory"); }
+__device__ __forceinline__ void bar_producers() { asm volatile("bar.sync 2, 64;" ::: "memory"); }
+
+constexpr int kWsProducers = 2;
+constexpr int kWsThreads = kThreads + 32 * kWsProducers;
+
+struct WsSmem {
+    u16 whist[kWarps * kRadix];  // per consumer warp: digit counts, then tile positions
+    u32 gofs[kRadix];
+    u32 swarp[kWarps];
+    u32 phist[kWsProducers * kRadix];  // per producer warp: digit counts
+    u64 full[2], empty[2], counted[2];
+    u32 tile[2];  // tile held by each buffer (>= ntiles: the end)
+    u32 ctile;    // the consumers' current tile, as consumer thread 0 read it
+};
+
+template <class Src, bool LAST, int ITEMS>
+__global__ void __launch_bounds__(kWsThreads, 3)
+    k_radix_pass_ws(const u64* __restrict__ kin, u64* __restrict__ kout, u32 n, u32 ntiles,
+                    int shift, int bits, const u32* __restrict__ bstart, u32* lb, u32* tile_ctr,
+                    int* status, Src src, double* __restrict__ val_out,
+                    const uint2* __restrict__ phs, u64 imask) {
+    constexpr u32 kTile = (u32)(kThreads * ITEMS);
+    extern __shared__ __align__(128) unsigned char dsm[];
+    u64* bufs = reinterpret_cast<u64*>(dsm);  // two tiles of kTile keys
+    __shared__ __align__(16) WsSmem S;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const u32 dmask = (1u << bits) - 1u;
+    if (tid == 0) {
+        for (int b = 0; b < 2; ++b) {
+            mbar_init(&S.full[b], 1);
+            mbar_init(&S.empty[b], 1);
+            mbar_init(&S.counted[b], 1);
+            S.tile[b] = 0xffffffffu;  // the end mark until a tile is taken
+        }
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+
+    if (warp >= kWarps) {
+        // ---------------- producers ----------------
+        const int pw = warp - kWarps;
+        u32* ph = S.phist + pw * kRadix;
+        for (int k = 0;; ++k) {
+            const int b = k & 1;
+            // A wait that runs out records PL_ERR_TIMEOUT and goes on: every
+            // iteration takes a new tile, so the loop still ends, and the
+            // group's barriers stay uniform.
+            if (k >= 2) mbar_wait(&S.empty[b], ((k >> 1) - 1) & 1, status);
+            if (pw == 0 && lane == 0) {
+                const u32 t = atomicAdd(tile_ctr, 1u);
+                S.tile[b] = t;
+                const u32 cnt = t < ntiles ? (min(kTile, n - t * kTile) & ~1u) : 0u;
+                if (cnt) {
+                    mbar_expect_tx(&S.full[b], cnt * 8u);
+                    bulk_load(bufs + (size_t)b * kTile, kin + (size_t)t * kTile, cnt * 8u,
+                              &S.full[b]);
+                } else {
+                    mbar_arrive(&S.full[b]);  // the end, or a one-key final tile
+                }
+            }
+            bar_producers();
+            const u32 tile = S.tile[b];
+            if (tile >= ntiles) break;
+            const u32 base = tile * kTile;
+            const u32 tile_n = min(kTile, n - base);
+            const u32 cpn = tile_n & ~1u;
+            for (int d = lane; d < kRadix; d += 32) ph[d] = 0;
+            __syncwarp();
+            mbar_wait(&S.full[b], (k >> 1) & 1, status);  // every issued copy is waited for
+            const u64* sk = bufs + (size_t)b * kTile;
+            for (u32 p0 = (u32)pw * 32; p0 < tile_n; p0 += 32 * kWsProducers) {
+                const u32 p = p0 + lane;
+                const bool valid = p < tile_n;
+                const u64 key = p < cpn ? sk[p] : (valid ? kin[base + p] : 0ull);
+                const u32 d = valid ? ((u32)(key >> shift) & dmask) : kSentinel;
+                const u32 peers = __match_any_sync(0xffffffffu, d);
+                if (valid && lane == __ffs(peers) - 1) atomicAdd(&ph[d], (u32)__popc(peers));
+            }
+            bar_producers();
+            // the aggregate goes out before the consumers may overwrite the
+            // buffer or publish this tile's inclusive prefix
+            for (int d = pw * 32 + lane; d < kRadix; d += 32 * kWsProducers) {
+                u32 c = 0;
+#pragma unroll
+                for (int q = 0; q < kWsProducers; ++q) c += S.phist[q * kRadix + d];
+                lb_publish(lb + d, tile, kRadix, c);
+            }
+            bar_producers();
+            if (pw == 0 && lane == 0) mbar_arrive(&S.counted[b]);
+        }
+        return;
+    }
+
+    // ---------------- consumers ----------------
+    // A wait that runs out records PL_ERR_TIMEOUT and goes on; the loop ends
+    // at the producers' end mark, which consumer thread 0 reads for all.
+    for (int k = 0;; ++k) {
+        const int b = k & 1;
+        mbar_wait(&S.full[b], (k >> 1) & 1, status);
+        if (tid == 0) S.ctile = S.tile[b];
+        reinterpret_cast<uint4*>(S.whist)[tid] = make_uint4(0, 0, 0, 0);  // 4 KB, 16 B each
+        bar_consumers();
+        const u32 tile = S.ctile;
+        if (tile >= ntiles) break;
+        u64* skeys = bufs + (size_t)b * kTile;
+        const u32 base = tile * kTile;
+        const u32 tile_n = min(kTile, n - base);
+        const u32 cpn = tile_n & ~1u;
+
+        u64 keys[ITEMS];
+        u32 rank[(ITEMS + 1) / 2];
+        const u32 wloc = (u32)warp * (ITEMS * 32);
+#pragma unroll
+        for (int t = 0; t < ITEMS; ++t) {
+            const u32 li = wloc + t * 32 + lane;
+            keys[t] = li < cpn ? skeys[li] : (li < tile_n ? kin[base + li] : 0ull);
+        }
+        u16* wh = S.whist + warp * kRadix;
+#pragma unroll
+        for (int t = 0; t < ITEMS; ++t) {
+            const bool valid = (wloc + t * 32 + lane) < tile_n;
+            const u32 d = valid ? ((u32)(keys[t] >> shift) & dmask) : kSentinel;
+            const u32 peers = __match_any_sync(0xffffffffu, d);
+            const int leader = __ffs(peers) - 1;
+            u32 before = 0;
+            if (valid && lane == leader) {
+                before = wh[d];
+                wh[d] = (u16)(before + __popc(peers));
+            }
+            before = __shfl_sync(0xffffffffu, before, leader);
+            const u32 r = before + __popc(peers & lanemask_lt());
+            rank[t / 2] = (t & 1) ? (rank[t / 2] | (r << 16)) : r;
+            __syncwarp();
+        }
+        bar_consumers();
+        const u32 d = tid;
+        u32 run = 0;
+#pragma unroll
+        for (int w = 0; w < kWarps; ++w) {
+            const u32 c = S.whist[w * kRadix + d];
+            S.whist[w * kRadix + d] = (u16)run;
+            run += c;
+        }
+        // exclusive scan of run over the 256 consumer threads
+        u32 inc = run;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const u32 t = __shfl_up_sync(0xffffffffu, inc, o);
+            if (lane >= o) inc += t;
+        }
+        if (lane == 31) S.swarp[warp] = inc;
+        bar_consumers();
+        u32 wpre = 0;
+#pragma unroll
+        for (int w = 0; w < kWarps; ++w) wpre += (w < warp) ? S.swarp[w] : 0u;
+        const u32 bl = wpre + inc - run;
+#pragma unroll
+        for (int w = 0; w < kWarps; ++w) S.whist[w * kRadix + d] += (u16)bl;
+        bar_consumers();
+        // the producers must be done reading the buffer before the in-place
+        // scatter (and have published this tile's aggregate)
+        mbar_wait(&S.counted[b], (k >> 1) & 1, status);
+#pragma unroll
+        for (int t = 0; t < ITEMS; ++t) {
+            if (wloc + t * 32 + lane < tile_n) {
+                const u32 dd = (u32)(keys[t] >> shift) & dmask;
+                const u32 pos = (u32)S.whist[warp * kRadix + dd] +
+                                ((rank[t / 2] >> ((t & 1) * 16)) & 0xffffu);
+                skeys[pos] = keys[t];
+            }
+        }
+        const u32 excl = lb_walk<4>(lb + d, tile, kRadix, run, status);
+        S.gofs[d] = bstart[d] + excl - bl;
+        bar_consumers();
+        if constexpr (LAST) {
+            constexpr int kGather = 8;
+            for (u32 p0 = 0; p0 < tile_n; p0 += kGather * kThreads) {
+                u64 kk[kGather];
+                u32 gg[kGather], pb[kGather];
+                double vv[kGather];
+#pragma unroll
+                for (int q = 0; q < kGather; ++q) {
+                    const u32 p = p0 + (u32)q * kThreads + tid;
+                    gg[q] = 0xffffffffu;
+                    kk[q] = 0;
+                    pb[q] = 0;
+                    vv[q] = 0.0;
+                    if (p < tile_n) {
+                        const u64 kv = skeys[p];
+                        const u32 idx = (u32)(kv & imask);
+                        kk[q] = kv;
+                        gg[q] = S.gofs[(u32)(kv >> shift) & dmask] + p;
+                        if (idx < n) src.flags_value(idx, phs, pb[q], vv[q]);
+                        else gg[q] = n;  // reported below
+                    }
+                }
+#pragma unroll
+                for (int q = 0; q < kGather; ++q) {
+                    if (gg[q] < n) {
+                        kout[gg[q]] = (kk[q] & ~imask) | (u64)(pb[q] & 1u);
+                        val_out[gg[q]] = (pb[q] & 2u) ? -vv[q] : vv[q];
+                    } else if (gg[q] != 0xffffffffu) {
+                        raise_status(status, PL_ERR_INTERNAL);
+                    }
+                }
+            }
+        } else {
+            for (u32 p = tid; p < tile_n; p += kThreads) {
+                const u64 kv = skeys[p];
+                const u32 g = S.gofs[(u32)(kv >> shift) & dmask] + p;
+                if (g >= n) raise_status(status, PL_ERR_INTERNAL);
+                else kout[g] = kv;
+            }
+        }
+        // generic-proxy accesses of the buffer are ordered before the next
+        // bulk copy into it
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        bar_consumers();
+        if (tid == 0) mbar_arrive(&S.empty[b]);
+    }
+}
+
+constexpr size_t radix_smem_ws(int items) { return 2 * sizeof(u64) * kThreads * items; }
+
+
+// ---------------------------------------------------------------------------
 // 4. Segments: equal-key runs of the sorted order.
 // ---------------------------------------------------------------------------
 struct SegCtx {
@@ -898,9 +1203,16 @@ struct FoldFilter {
     int on;
     double cutoff;
     u32* tile_kept;
-    double2* seg2;   // kCanonSplit: (phase-0 sum, phase-1 sum) at each head
+    double2* seg2;   // kCanonSplit: (phase-0 sum, phase-1 sum) of each head's record
     double2* rpre;   // per fold range: the sums of its terms before its first head
     double2* ptail;  // per pending segment: its sums at the end of its range
+    // kCanonSplit head records: the heads of fold range g sit at slots
+    // [g * kFoldSpan, g * kFoldSpan + rng_heads[g]) in key order -- the sorted
+    // key in rkey, the two sums in seg2 -- and rng_kept[g] counts the output
+    // terms they give.
+    u64* rkey;
+    u32* rng_heads;
+    u32* rng_kept;
 };
 
 // canonicalize() on index-packed keys: the sort key is (x, z) only and the
@@ -996,16 +1308,19 @@ __device__ __forceinline__ u32 fold_word(const SegCtx& C, u32 e, u64 key) {
     return C.pay[e];
 }
 
+// One of a kCanonSplit head's two sums gives an output term: zero and cutoff
+// filters of canonicalize() + cutoff().
+__device__ __forceinline__ u32 split_kept(double r, double cutoff) {
+    return (r != 0.0 && (cutoff <= 0.0 || fabs(r) >= cutoff)) ? 1u : 0u;
+}
+
 template <int MODE>
 __device__ __forceinline__ u32 fold_close(double* segval, u8* segflag, i64 h, double r0,
                                           double r1, const FoldFilter& F) {
     if (MODE == kCanonSplit) {
-        // segflag 0x10 | kept phase 0 | kept phase 1 << 1 (the filters are on)
-        const bool k0 = r0 != 0.0 && (F.cutoff <= 0.0 || fabs(r0) >= F.cutoff);
-        const bool k1 = r1 != 0.0 && (F.cutoff <= 0.0 || fabs(r1) >= F.cutoff);
+        // h is the head's record slot; the emit re-applies the same filters
         F.seg2[h] = make_double2(r0, r1);
-        segflag[h] = (u8)(0x10u | (k0 ? 1u : 0u) | (k1 ? 2u : 0u));
-        return (k0 ? 1u : 0u) + (k1 ? 1u : 0u);
+        return split_kept(r0, F.cutoff) + split_kept(r1, F.cutoff);
     }
     const double v = MODE == kProp ? dadd(r0, -r1) : r0;
     segval[h] = v;
@@ -1041,6 +1356,7 @@ __global__ void __launch_bounds__(32 * kFoldWarps, 6)
         cp = fold_word<MODE>(C, w0 - 1, ck);
     }
     u32 first = kNoHead;
+    u32 nhead = 0;  // kCanonSplit: heads of the range so far (their record slots)
     // kBatch chunks of loads in flight per lane, then the head flags of those
     // chunks; per chunk, a word of head bits and a word of sign bits
     constexpr int kBatch = 8;
@@ -1072,10 +1388,14 @@ __global__ void __launch_bounds__(32 * kFoldWarps, 6)
                 head = (e == 0) || !lane_same_key(C, e, ke[b], kp, pe[b], pp);
                 neg = (pe[b] >> 31) != 0;
                 sv[c * 33 + lane] = (MODE == kCanon && neg) ? -ve[b] : ve[b];
-                if (!head) segflag[e] = 0;
+                if (MODE != kCanonSplit && !head) segflag[e] = 0;
             }
             const u32 hb = __ballot_sync(0xffffffffu, head);
             const u32 nb = __ballot_sync(0xffffffffu, neg);
+            if (MODE == kCanonSplit) {
+                if (head) F.rkey[w0 + nhead + __popc(hb & lanemask_lt())] = ke[b];
+                nhead += __popc(hb);
+            }
             if (lane == 0 && c < 32) {
                 hbw[c] = hb;
                 nbw[c] = nb;
@@ -1140,12 +1460,28 @@ __global__ void __launch_bounds__(32 * kFoldWarps, 6)
     i64 h = -1;
     double r0 = 0.0, r1 = 0.0, p0 = 0.0, p1 = 0.0;
     u32 kept = 0;
+    // kCanonSplit closes a head by its record slot: w0 + (heads of the range
+    // before it), i.e. the heads of the earlier lanes' spans plus the lane's
+    // own earlier heads
+    i64 hs = -1;
+    u32 nslot = 0;
+    if (MODE == kCanonSplit) {
+        const u32 c = (u32)__popc(HB);
+        u32 inc = c;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const u32 t = __shfl_up_sync(0xffffffffu, inc, o);
+            if (lane >= o) inc += t;
+        }
+        nslot = w0 + inc - c;
+    }
     for (u32 i = 0; i < lcnt; ++i) {
         const double v = sv[sa + i];
         if ((HB >> i) & 1u) {
-            if (h >= 0) kept += fold_close<MODE>(segval, segflag, h, r0, r1, F);
+            if (h >= 0) kept += fold_close<MODE>(segval, segflag, MODE == kCanonSplit ? hs : h, r0, r1, F);
             else fh = i;
             h = (i64)(w0 + a + i);
+            hs = (i64)(nslot++);
             r0 = 0.0;
             r1 = 0.0;
         }
@@ -1161,7 +1497,8 @@ __global__ void __launch_bounds__(32 * kFoldWarps, 6)
     // deterministic and equal the reference's order for every segment that
     // spans at most three lanes.
     const bool hh = fh < lcnt;
-    i64 oh = hh ? h : -1;
+    // kCanonSplit: oh travels as the head's record slot
+    i64 oh = hh ? (MODE == kCanonSplit ? hs : h) : -1;
     double o0 = hh ? r0 : p0, o1 = hh ? r1 : p1;
     bool known = hh;
     {
@@ -1244,7 +1581,7 @@ __global__ void __launch_bounds__(32 * kFoldWarps, 6)
             if (closed || w1 + look == C.n) {
                 kept += fold_close<MODE>(segval, segflag, ch, d0, d1, F);
             } else {
-                segflag[ch] = 2;
+                if (MODE != kCanonSplit) segflag[ch] = 2;
                 const u32 k = atomicAdd(&counters[2], 1u);
                 long_list[k] = (u32)ch;
                 F.ptail[k] = make_double2(c0, c1);
@@ -1254,7 +1591,14 @@ __global__ void __launch_bounds__(32 * kFoldWarps, 6)
     if (F.on) {
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) kept += __shfl_xor_sync(0xffffffffu, kept, o);
-        if (lane == 0 && kept) atomicAdd(&F.tile_kept[w0 / kETile], kept);
+        if (MODE == kCanonSplit) {
+            if (lane == 0) {
+                F.rng_heads[gwarp] = nhead;
+                F.rng_kept[gwarp] = kept;
+            }
+        } else if (lane == 0 && kept) {
+            atomicAdd(&F.tile_kept[w0 / kETile], kept);
+        }
     }
 }
 
@@ -1292,7 +1636,11 @@ __global__ void __launch_bounds__(256) k_fold_carry(const u32* wfirst, u32 ngw,
         }
         if (lane == 0) {
             const u32 keep = fold_close<MODE>(segval, segflag, h, a0, a1, F);
-            if (F.on && keep) atomicAdd(&F.tile_kept[h / kETile], keep);
+            if (MODE == kCanonSplit) {
+                if (keep) atomicAdd(&F.rng_kept[h / kFoldSpan], keep);  // h: a record slot
+            } else if (F.on && keep) {
+                atomicAdd(&F.tile_kept[h / kETile], keep);
+            }
         }
     }
 }
@@ -1396,60 +1744,65 @@ __device__ __forceinline__ void emit_term(const Src& src, const KeyLayout& L, u6
     out.v[o] = v;
 }
 
-// kCanonSplit emit: a kept head writes its phase-0 term, then its phase-1
-// term (the canonical order: phase is the last key field), at the offsets
-// k_tile_scan gave its tile.
+// kCanonSplit emit from the fold's head records: one warp per fold range
+// copies its kept terms -- a head's phase-0 term, then its phase-1 term (the
+// canonical order: phase is the last key field) -- to the offset
+// k_tile_scan gave the range.  The records are dense, so a range reads
+// 24 bytes per head and nothing per non-head term.
+constexpr int kRecBatch = 4;  // 32-head chunks whose loads are in flight at once
 template <int AS>
 __global__ void __launch_bounds__(kThreads)
-    k_emit_split(KeyLayout L, const u64* keys, const double2* seg2, const u8* segflag, u32 n,
-                 const u32* tile_off, SoAOut out, int* status) {
-    __shared__ u32 swarp[kWarps];
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    const u32 tile = blockIdx.x;
-    const u32 wbase = tile * kETile + (u32)warp * (kEItems * 32);
-    u32 kb[kEItems];  // bit 0: phase-0 term kept, bit 1: phase-1 term kept
+    k_emit_records(KeyLayout L, const u64* __restrict__ rkey, const double2* __restrict__ rs,
+                   const u32* __restrict__ rng_heads, const u32* __restrict__ rng_off, u32 ngw,
+                   double cutoff, SoAOut out, int* status) {
+    const int lane = threadIdx.x & 31;
+    const u32 g = blockIdx.x * kWarps + (threadIdx.x >> 5);
+    if (g >= ngw) return;
+    const u32 nh = rng_heads[g];
+    const u32 w0 = g * kFoldSpan;
+    i64 o = rng_off[g];
+    for (u32 k0 = 0; k0 < nh; k0 += 32 * kRecBatch) {
+        u64 key[kRecBatch];
+        double2 v[kRecBatch];
 #pragma unroll
-    for (int t = 0; t < kEItems; ++t) {
-        const u32 e = wbase + t * 32 + lane;
-        const u32 sf = e < n ? segflag[e] : 0u;
-        kb[t] = (sf & 0x10u) ? (sf & 3u) : 0u;
-    }
-    u32 wcount = 0;
-    u32 myoff[kEItems];
+        for (int b = 0; b < kRecBatch; ++b) {
+            const u32 k = k0 + (u32)b * 32 + lane;
+            key[b] = k < nh ? rkey[w0 + k] : 0ull;
+            v[b] = k < nh ? rs[w0 + k] : make_double2(0.0, 0.0);
+        }
 #pragma unroll
-    for (int t = 0; t < kEItems; ++t) {
-        const u32 b0 = __ballot_sync(0xffffffffu, (kb[t] & 1u) != 0);
-        const u32 b1 = __ballot_sync(0xffffffffu, (kb[t] & 2u) != 0);
-        const u32 lt = lanemask_lt();
-        myoff[t] = wcount + __popc(b0 & lt) + __popc(b1 & lt);
-        wcount += __popc(b0) + __popc(b1);
-    }
-    u32 total;
-    const u32 wexcl = block_excl_scan(lane == 0 ? wcount : 0u, swarp, total);
-    const u32 base_o = tile_off[tile] + __shfl_sync(0xffffffffu, wexcl, 0);
+        for (int b = 0; b < kRecBatch; ++b) {
+            const u32 k0b = split_kept(v[b].x, cutoff), k1b = split_kept(v[b].y, cutoff);
+            const u32 c = k0b + k1b;
+            u32 inc = c;
 #pragma unroll
-    for (int t = 0; t < kEItems; ++t) {
-        if (!kb[t]) continue;
-        const u32 e = wbase + t * 32 + lane;
-        u64 xw[AS], zw[AS];
-        u32 fv;
-        unpack_key<AS>(L, keys[e], xw, zw, fv);
-        const double2 sv = seg2[e];
-        i64 o = (i64)base_o + myoff[t];
-        for (u32 ph = 0; ph < 2; ++ph) {
-            if (!((kb[t] >> ph) & 1u)) continue;
-            if (o >= out.capacity) {
-                raise_status(status, PL_ERR_CAPACITY);
-                break;
+            for (int d = 1; d < 32; d <<= 1) {
+                const u32 t = __shfl_up_sync(0xffffffffu, inc, d);
+                if (lane >= d) inc += t;
             }
+            const u32 tot = __shfl_sync(0xffffffffu, inc, 31);
+            if (c) {
+                u64 xw[AS], zw[AS];
+                u32 fv;
+                unpack_key<AS>(L, key[b], xw, zw, fv);
+                i64 p = o + (inc - c);
+                for (u32 ph = 0; ph < 2; ++ph) {
+                    if (!(ph ? k1b : k0b)) continue;
+                    if (p >= out.capacity) {
+                        raise_status(status, PL_ERR_CAPACITY);
+                        break;
+                    }
 #pragma unroll
-            for (int k = 0; k < AS; ++k) {
-                out.x[(i64)k * out.capacity + o] = xw[k];
-                out.z[(i64)k * out.capacity + o] = zw[k];
+                    for (int w = 0; w < AS; ++w) {
+                        out.x[(i64)w * out.capacity + p] = xw[w];
+                        out.z[(i64)w * out.capacity + p] = zw[w];
+                    }
+                    out.f[p] = (u8)ph;
+                    out.v[p] = ph ? v[b].y : v[b].x;
+                    ++p;
+                }
             }
-            out.f[o] = (u8)ph;
-            out.v[o] = ph ? sv.y : sv.x;
-            ++o;
+            o += tot;
         }
     }
 }
@@ -1601,6 +1954,7 @@ struct Bufs {
     u32 *wfirst, *long_list;
     double2 *rpre, *ptail;
     u32 *tile_kept, *tile_off, *lb_emit;
+    u32 *rng_heads, *rng_kept, *rng_off;  // per fold range (index-packed path)
     u64 *orm, *andm;
     i64* d_count;
     int* d_status;
@@ -1629,6 +1983,9 @@ void carve_all(Carve& c, i64 n, int nch, Bufs& B) {
     B.tile_kept = c.take<u32>(etiles);
     B.tile_off = c.take<u32>(etiles);
     B.lb_emit = c.take<u32>(etiles);
+    B.rng_heads = c.take<u32>(ngw);
+    B.rng_kept = c.take<u32>(ngw);
+    B.rng_off = c.take<u32>(ngw);
     B.counters = c.take<u32>(kCounterWords);
     B.orm = c.take<u64>(2 * kMaxFields);   // one set per operand of a product
     B.andm = c.take<u64>(2 * kMaxFields);
@@ -1807,22 +2164,90 @@ cudaError_t radix_attrs(K* kernel, int smem) {
     return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
 }
 
+// L2 prefetch distance of the digit passes in tiles (PL_TUNE_RADIX_PREFETCH):
+// by default one wave -- resident CTAs per SM (looked up once per kernel
+// instantiation into `per_sm`) times SMs; -1 off; k > 0 exactly k tiles.
+template <class K>
+u32 prefetch_ahead(K* kernel, size_t smem, int& per_sm) {
+    const long long v = tuning(PL_TUNE_RADIX_PREFETCH);
+    if (v < 0) return 0u;
+    if (v > 0) return (u32)v;
+    if (per_sm == 0) {
+        int b = 0;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, kernel, kThreads, smem) !=
+                cudaSuccess ||
+            b < 1)
+            b = 1;
+        per_sm = b;
+    }
+    return (u32)(per_sm * sm_count());
+}
+
 template <class Src, int ITEMS>
 int radix_pass(bool last, const u64* kin, const u32* vin, u64* kout, u32* vout, u32 n, int shift,
                int bits, const u32* bstart, Bufs& B, u32* ctr, const Src& src, cudaStream_t st) {
     const u32 tiles = (n + kThreads * ITEMS - 1) / (kThreads * ITEMS);
     const SoASrc<1> nosrc{nullptr, nullptr, nullptr, nullptr, 0};
+    const size_t sm = radix_smem(ITEMS);
+    static int occ_last = 0, occ_mid = 0;
     if (last) {
-        PL_CUDA_TRY(radix_attrs(k_radix_pass<Src, true, ITEMS, false>, (int)radix_smem(ITEMS)));
-        k_radix_pass<Src, true, ITEMS, false><<<tiles, kThreads, radix_smem(ITEMS), st>>>(
-            kin, vin, kout, vout, n, shift, bits, bstart, B.lb, ctr, B.d_status, src, B.sv,
-            nullptr, 0ull),
+        auto* k = k_radix_pass<Src, true, ITEMS, false>;
+        PL_CUDA_TRY(radix_attrs(k, (int)sm));
+        k<<<tiles, kThreads, sm, st>>>(kin, vin, kout, vout, n, shift, bits, bstart, B.lb, ctr,
+                                       B.d_status, src, B.sv, nullptr, 0ull,
+                                       prefetch_ahead(k, sm, occ_last)),
             pl::note_launch();
     } else {
-        PL_CUDA_TRY(radix_attrs(k_radix_pass<SoASrc<1>, false, ITEMS, false>, (int)radix_smem(ITEMS)));
-        k_radix_pass<SoASrc<1>, false, ITEMS, false><<<tiles, kThreads, radix_smem(ITEMS), st>>>(
-            kin, vin, kout, vout, n, shift, bits, bstart, B.lb, ctr, B.d_status, nosrc, nullptr,
-            nullptr, 0ull),
+        auto* k = k_radix_pass<SoASrc<1>, false, ITEMS, false>;
+        PL_CUDA_TRY(radix_attrs(k, (int)sm));
+        k<<<tiles, kThreads, sm, st>>>(kin, vin, kout, vout, n, shift, bits, bstart, B.lb, ctr,
+                                       B.d_status, nosrc, nullptr, nullptr, 0ull,
+                                       prefetch_ahead(k, sm, occ_mid)),
+            pl::note_launch();
+    }
+    return PL_OK;
+}
+
+// Warp-specialised digit passes (k_radix_pass_ws) for index-packed keys:
+// PL_TUNE_RADIX_WS 1 on, 0 (default) / -1 off.
+bool radix_ws() { return tuning(PL_TUNE_RADIX_WS) > 0; }
+
+// One wave of k_radix_pass_ws: resident CTAs per SM (looked up once per
+// kernel instantiation into `per_sm`) x SMs, at most a CTA per tile.
+template <class K>
+int ws_grid(K* kernel, size_t smem, u32 tiles, int& per_sm) {
+    if (per_sm == 0) {
+        int b = 0;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, kernel, kWsThreads, smem) !=
+                cudaSuccess ||
+            b < 1)
+            b = 1;
+        per_sm = b;
+    }
+    return (int)std::min<u32>(tiles, (u32)(per_sm * sm_count()));
+}
+
+template <class Src, int ITEMS>
+int radix_pass_ws(bool last, const u64* kin, u64* kout, u32 n, int shift, int bits,
+                  const u32* bstart, Bufs& B, u32* ctr, const Src& src, const uint2* phs,
+                  u64 imask, cudaStream_t st) {
+    const u32 tiles = (n + kThreads * ITEMS - 1) / (kThreads * ITEMS);
+    const size_t sm = radix_smem_ws(ITEMS);
+    static int occ_last = 0, occ_mid = 0;
+    if (last) {
+        auto* k = k_radix_pass_ws<Src, true, ITEMS>;
+        PL_CUDA_TRY(radix_attrs(k, (int)sm));
+        k<<<ws_grid(k, sm, tiles, occ_last), kWsThreads, sm, st>>>(
+            kin, kout, n, tiles, shift, bits, bstart, B.lb, ctr, B.d_status, src, B.sv, phs,
+            imask),
+            pl::note_launch();
+    } else {
+        const SoASrc<1> nosrc{nullptr, nullptr, nullptr, nullptr, 0};
+        auto* k = k_radix_pass_ws<SoASrc<1>, false, ITEMS>;
+        PL_CUDA_TRY(radix_attrs(k, (int)sm));
+        k<<<ws_grid(k, sm, tiles, occ_mid), kWsThreads, sm, st>>>(
+            kin, kout, n, tiles, shift, bits, bstart, B.lb, ctr, B.d_status, nosrc, nullptr,
+            nullptr, imask),
             pl::note_launch();
     }
     return PL_OK;
@@ -1833,20 +2258,26 @@ template <class Src, int ITEMS>
 int radix_pass_konly(bool last, const u64* kin, u64* kout, u32 n, int shift, int bits,
                      const u32* bstart, Bufs& B, u32* ctr, const Src& src, const uint2* phs,
                      u64 imask, cudaStream_t st) {
+    if (radix_ws())
+        return radix_pass_ws<Src, ITEMS>(last, kin, kout, n, shift, bits, bstart, B, ctr, src,
+                                         phs, imask, st);
     const u32 tiles = (n + kThreads * ITEMS - 1) / (kThreads * ITEMS);
     const size_t sm = radix_smem_konly(ITEMS);
+    static int occ_last = 0, occ_mid = 0;
     if (last) {
-        PL_CUDA_TRY(radix_attrs(k_radix_pass<Src, true, ITEMS, true>, (int)sm));
-        k_radix_pass<Src, true, ITEMS, true><<<tiles, kThreads, sm, st>>>(
-            kin, nullptr, kout, nullptr, n, shift, bits, bstart, B.lb, ctr, B.d_status, src, B.sv,
-            phs, imask),
+        auto* k = k_radix_pass<Src, true, ITEMS, true>;
+        PL_CUDA_TRY(radix_attrs(k, (int)sm));
+        k<<<tiles, kThreads, sm, st>>>(kin, nullptr, kout, nullptr, n, shift, bits, bstart, B.lb,
+                                       ctr, B.d_status, src, B.sv, phs, imask,
+                                       prefetch_ahead(k, sm, occ_last)),
             pl::note_launch();
     } else {
         const SoASrc<1> nosrc{nullptr, nullptr, nullptr, nullptr, 0};
-        PL_CUDA_TRY(radix_attrs(k_radix_pass<SoASrc<1>, false, ITEMS, true>, (int)sm));
-        k_radix_pass<SoASrc<1>, false, ITEMS, true><<<tiles, kThreads, sm, st>>>(
-            kin, nullptr, kout, nullptr, n, shift, bits, bstart, B.lb, ctr, B.d_status, nosrc,
-            nullptr, nullptr, imask),
+        auto* k = k_radix_pass<SoASrc<1>, false, ITEMS, true>;
+        PL_CUDA_TRY(radix_attrs(k, (int)sm));
+        k<<<tiles, kThreads, sm, st>>>(kin, nullptr, kout, nullptr, n, shift, bits, bstart, B.lb,
+                                       ctr, B.d_status, nosrc, nullptr, nullptr, imask,
+                                       prefetch_ahead(k, sm, occ_mid)),
             pl::note_launch();
     }
     return PL_OK;
@@ -1917,7 +2348,8 @@ int run_collate(const Src& src, u32 n, int mode, const KeyLayout& L, const PassP
     // Without a weight filter the fold decides the zero / cutoff filters and
     // counts survivors per emit tile, so the emit needs no look-back.
     const bool counted = a.max_weight == ~0ull;
-    const FoldFilter F{counted ? 1 : 0, a.cutoff, B.tile_kept, nullptr, B.rpre, B.ptail};
+    const FoldFilter F{counted ? 1 : 0, a.cutoff, B.tile_kept, nullptr, B.rpre, B.ptail,
+                       nullptr, nullptr, nullptr};
     if (counted) PL_CUDA_TRY(fill32_async(B.tile_kept, 0u, sizeof(u32) * etiles, st));
     e0 = timed_begin(st);
     int rc = PL_OK;
@@ -1964,13 +2396,11 @@ int run_collate_split(const Src& src, u32 n, const KeyLayout& L, const PassPlan&
     // then the (phase-0, phase-1) sums of the segments
     uint2* phs = reinterpret_cast<uint2*>(B.planes);
     double2* seg2 = reinterpret_cast<double2*>(reinterpret_cast<unsigned char*>(B.planes) + al(n));
-    const u32 etiles0 = (n + kETile - 1) / kETile;
-    const FillReq fr[5] = {{B.hist, 0u, sizeof(u32) * (size_t)std::max(P.npasses, 1) * kRadix},
+    const FillReq fr[4] = {{B.hist, 0u, sizeof(u32) * (size_t)std::max(P.npasses, 1) * kRadix},
                            {B.counters, 0u, sizeof(u32) * (size_t)(P.npasses + 8)},
                            {B.d_status, 0u, sizeof(int)},
-                           {B.d_count, 0u, sizeof(i64)},
-                           {B.tile_kept, 0u, sizeof(u32) * etiles0}};
-    PL_CUDA_TRY(fill32_multi(fr, 5, st));
+                           {B.d_count, 0u, sizeof(i64)}};
+    PL_CUDA_TRY(fill32_multi(fr, 4, st));
     const int gblocks = grid_for(n, 256, nsm * 8);
     cudaEvent_t e0 = timed_begin(st);
     const u32 derived = derive_histograms<AS>(src, L, P, B, st);
@@ -2006,17 +2436,18 @@ int run_collate_split(const Src& src, u32 n, const KeyLayout& L, const PassPlan&
         std::swap(kin, kout);
     }
     SegCtx C{kin, nullptr, B.sv, B.planes, n, 1, L.seg_mask0, kCanon};
-    const u32 etiles = (n + kETile - 1) / kETile;
-    const FoldFilter F{1, a.cutoff, B.tile_kept, seg2, B.rpre, B.ptail};
+    const u32 ngw = (n + kFoldSpan - 1) / kFoldSpan;
+    const FoldFilter F{1,      a.cutoff,    nullptr,    seg2,      B.rpre,
+                       B.ptail, reinterpret_cast<u64*>(B.seg_sum), B.rng_heads, B.rng_kept};
     e0 = timed_begin(st);
     int rc = fold_segments<kCanonSplit>(C, B, F, nsm, st);
     if (rc != PL_OK) return rc;
     timed_end(e0, st, "k_fold", 16ull * n);
     e0 = timed_begin(st);
-    k_tile_scan<<<1, 1024, 0, st>>>(B.tile_kept, etiles, B.tile_off, B.d_count),
-        pl::note_launch();
-    k_emit_split<AS><<<etiles, kThreads, 0, st>>>(L, kin, seg2, B.segflag, n, B.tile_off, out,
-                                                  B.d_status),
+    k_tile_scan<<<1, 1024, 0, st>>>(B.rng_kept, ngw, B.rng_off, B.d_count), pl::note_launch();
+    k_emit_records<AS><<<(ngw + kWarps - 1) / kWarps, kThreads, 0, st>>>(
+        L, reinterpret_cast<const u64*>(B.seg_sum), seg2, B.rng_heads, B.rng_off, ngw, a.cutoff,
+        out, B.d_status),
         pl::note_launch();
     timed_end(e0, st, "k_emit", 0ull);
     PL_CUDA_TRY(cudaGetLastError());

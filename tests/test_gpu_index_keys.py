@@ -139,3 +139,55 @@ def test_product_full_size(cuda):
     same = (np.diff(on.x[0].astype(np.int64)) == 0) & (np.diff(on.z[0].astype(np.int64)) == 0) \
         & (np.diff(on.flags.astype(np.int64)) == 0)
     assert not same.any()
+
+
+@contextlib.contextmanager
+def tuned(key, value):
+    L = _abi.lib()
+    old = ctypes.c_int64()
+    _abi.check(L.pl_get_tuning(key, ctypes.byref(old)), "pl_get_tuning")
+    _abi.check(L.pl_set_tuning(key, value), "pl_set_tuning")
+    try:
+        yield
+    finally:
+        _abi.check(L.pl_set_tuning(key, old.value), "pl_set_tuning")
+
+
+def _bits_equal(a, b):
+    return (a.n == b.n and np.array_equal(a.x, b.x) and np.array_equal(a.z, b.z)
+            and np.array_equal(a.flags, b.flags)
+            and np.array_equal(a.val.view(np.uint64), b.val.view(np.uint64)))
+
+
+@pytest.mark.parametrize("items", [8, 12, 16])
+@pytest.mark.parametrize("n,nq,seed", [(1, 3, 31), (2, 4, 32), (3, 5, 33), (2049, 10, 34),
+                                       (4097, 12, 35), (12289, 12, 36), (300001, 12, 37)])
+@pytest.mark.parametrize("ahead", [0, 1, 7])
+def test_l2_prefetch_digit_pass(cuda, oracle, items, n, nq, seed, ahead):
+    # Digit passes that prefetch the tile `ahead` places on into L2 (0: one
+    # wave) against passes without prefetch: bit-identical results, down to
+    # one-key and odd-length final tiles (never prefetched: only whole tiles
+    # are).
+    p = random_sum(n, 1, seed, nq, "normal")
+    with tuned(_abi.PL_TUNE_RADIX_ITEMS, items):
+        with tuned(_abi.PL_TUNE_RADIX_PREFETCH, ahead):
+            on = gpu_collate(p, CANON)
+        with tuned(_abi.PL_TUNE_RADIX_PREFETCH, -1):
+            off = gpu_collate(p, CANON)
+    assert _bits_equal(on, off)
+    o = oracle.canonicalize(p)
+    assert_keys_equal(on, o)
+    assert_values_close(on, o, abs_scale(oracle, p))
+
+
+@pytest.mark.parametrize("items", [8, 16])
+def test_l2_prefetch_digit_pass_product(cuda, items):
+    # the 4096 x 4096 product of the benchmark with and without the prefetch
+    a, b = W.product_operands(seed=0, terms=4096)
+    a, b = as_planes(a), as_planes(b)
+    with tuned(_abi.PL_TUNE_RADIX_ITEMS, items):
+        with tuned(_abi.PL_TUNE_RADIX_PREFETCH, 0):
+            on = gpu_multiply_collate(a, b)
+        with tuned(_abi.PL_TUNE_RADIX_PREFETCH, -1):
+            off = gpu_multiply_collate(a, b)
+    assert on.n > 0 and _bits_equal(on, off)
