@@ -246,7 +246,8 @@ def run_product_collate(args, rank, local, ws):
 
     # ---- autotune: keys per thread of the digit pass -------------------
     tune_trials = []
-    for prefetch in (0, -1):  # L2 prefetch one wave ahead / off
+    # (L2 prefetch one wave ahead / off) x keys per thread
+    for prefetch in (0, -1):
         for items in (8, 12, 16):
             _abi.check(L.pl_set_tuning(_abi.PL_TUNE_RADIX_ITEMS, items), "pl_set_tuning")
             _abi.check(L.pl_set_tuning(_abi.PL_TUNE_RADIX_PREFETCH, prefetch), "pl_set_tuning")
@@ -267,7 +268,7 @@ def run_product_collate(args, rank, local, ws):
         import torch.distributed as dist
         t = torch.tensor([best_items, best_pf], device="cuda")
         dist.broadcast(t, 0)
-        best_items, best_pf = int(t[0].item()), int(t[1].item())
+        best_items, best_pf = (int(v) for v in t.tolist())
     _abi.check(L.pl_set_tuning(_abi.PL_TUNE_RADIX_ITEMS, best_items), "pl_set_tuning")
     _abi.check(L.pl_set_tuning(_abi.PL_TUNE_RADIX_PREFETCH, best_pf), "pl_set_tuning")
     for _ in range(args.warmup):
@@ -397,8 +398,8 @@ def run_product_collate(args, rank, local, ws):
         "result": {"terms_out": n_out},
         "tuned": {"radix_items": best_items, "radix_l2_prefetch": best_pf == 0,
                   "trials_ms_per_step": {
-                      f"{'prefetch' if t['radix_prefetch'] == 0 else 'plain'}-{t['radix_items']}":
-                      t["ms_per_step"] for t in tune_trials}},
+                      ("prefetch" if t["radix_prefetch"] == 0 else "plain")
+                      + f"-{t['radix_items']}": t["ms_per_step"] for t in tune_trials}},
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d,
                 "d2h_bytes_per_step": int(statistics.mean(d2h)),
                 "path": "pinned host planes -> H2D -> pl_multiply_collate (C ABI) -> D2H of "

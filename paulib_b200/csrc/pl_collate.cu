@@ -476,9 +476,12 @@ __global__ void __launch_bounds__(256) k_pack_split(Src src, u32 n, KeyLayout L,
 // operands' packed keys.  Needs n % 32 == 0 so each warp's 32 products are
 // one bit-plane word.
 constexpr int kPackPerThread = 8;
+//
+// opk (optional): the operands' packed keys, lhs then rhs, as k_operand_hist
+// stored them -- one load per product instead of re-packing the lhs words.
 template <int AS>
 __global__ void __launch_bounds__(256) k_pack_split_prod(ProdSrc<AS> src, KeyLayout L, u64* keys,
-                                                         uint2* phs) {
+                                                         uint2* phs, const u64* __restrict__ opk) {
     const u32 i = blockIdx.y;
     const u32 j = blockIdx.x * blockDim.x * kPackPerThread + threadIdx.x;
     u64 bxw[AS], bzw[AS];
@@ -487,7 +490,7 @@ __global__ void __launch_bounds__(256) k_pack_split_prod(ProdSrc<AS> src, KeyLay
         bxw[k] = __ldg(src.bx + (i64)k * src.sb + i);
         bzw[k] = __ldg(src.bz + (i64)k * src.sb + i);
     }
-    const u64 kb = pack_chunk<AS>(L, bxw, bzw, 0u, 0);
+    const u64 kb = opk ? __ldg(opk + src.n + i) : pack_chunk<AS>(L, bxw, bzw, 0u, 0);
     const u32 bfl = __ldg(src.bf + i);
 #pragma unroll
     for (int r = 0; r < kPackPerThread; ++r) {
@@ -503,7 +506,8 @@ __global__ void __launch_bounds__(256) k_pack_split_prod(ProdSrc<AS> src, KeyLay
         }
         const u32 fl = acc.phase(__ldg(src.af + jj), bfl);
         const u32 p = i * src.n + jj;
-        keys[p] = (pack_chunk<AS>(L, axw, azw, 0u, 0) ^ kb) | (u64)p;
+        const u64 ka = opk ? __ldg(opk + jj) : pack_chunk<AS>(L, axw, azw, 0u, 0);
+        keys[p] = (ka ^ kb) | (u64)p;
         const u32 im = __ballot_sync(0xffffffffu, (fl & 1u) != 0);
         const u32 sg = __ballot_sync(0xffffffffu, (fl & 2u) != 0);
         if ((threadIdx.x & 31) == 0) phs[p >> 5] = make_uint2(im, sg);
@@ -512,15 +516,16 @@ __global__ void __launch_bounds__(256) k_pack_split_prod(ProdSrc<AS> src, KeyLay
 
 // Generic pack unless the product fast path applies.
 template <int AS>
-bool pack_split_fast(const SoASrc<AS>&, u32, const KeyLayout&, u32, u64*, uint2*, cudaStream_t) {
+bool pack_split_fast(const SoASrc<AS>&, u32, const KeyLayout&, u32, u64*, uint2*, const u64*,
+                     cudaStream_t) {
     return false;
 }
 template <int AS>
 bool pack_split_fast(const ProdSrc<AS>& src, u32, const KeyLayout& L, u32 count_mask, u64* keys,
-                     uint2* phs, cudaStream_t st) {
+                     uint2* phs, const u64* opk, cudaStream_t st) {
     if (count_mask != 0 || src.n % 32 != 0 || src.m > 65535u) return false;
     const dim3 grid((src.n + 256 * kPackPerThread - 1) / (256 * kPackPerThread), src.m);
-    k_pack_split_prod<AS><<<grid, 256, 0, st>>>(src, L, keys, phs), pl::note_launch();
+    k_pack_split_prod<AS><<<grid, 256, 0, st>>>(src, L, keys, phs, opk), pl::note_launch();
     return true;
 }
 
@@ -529,9 +534,21 @@ bool pack_split_fast(const ProdSrc<AS>& src, u32, const KeyLayout& L, u32 count_
 // (x = ax ^ bx, z = az ^ bz), so the histogram over all n*m products is the
 // XOR-convolution of the two operand histograms; only digits that include
 // the phase bit must be counted product by product.
+// Both operands in one launch: blockIdx.y 0 counts (src, n) into h, 1 counts
+// (src2, n2) into h2.
+// With pk set, each term's packed key is stored as well: lhs at pk[0, n),
+// rhs at pk[n, n + n2).
 template <int AS>
-__global__ void __launch_bounds__(256) k_operand_hist(SoASrc<AS> src, u32 n, KeyLayout L,
-                                                      PassPlan P, u32 conv_mask, u32* h) {
+__global__ void __launch_bounds__(256) k_operand_hist(SoASrc<AS> src, u32 n, u32* h,
+                                                      SoASrc<AS> src2, u32 n2, u32* h2,
+                                                      KeyLayout L, PassPlan P, u32 conv_mask,
+                                                      u64* pk) {
+    if (blockIdx.y == 1) {
+        src = src2;
+        if (pk) pk += n;
+        n = n2;
+        h = h2;
+    }
     __shared__ u32 sh[8 * kRadix];
     const int np0 = P.first[1] - P.first[0];
     for (int i = threadIdx.x; i < np0 * kRadix; i += blockDim.x) sh[i] = 0;
@@ -541,6 +558,7 @@ __global__ void __launch_bounds__(256) k_operand_hist(SoASrc<AS> src, u32 n, Key
         u32 fl;
         src.key(i, xw, zw, fl);
         const u64 k0 = pack_chunk<AS>(L, xw, zw, 0u, 0);
+        if (pk) pk[i] = k0;
         for (int p = 0; p < np0; ++p)
             if ((conv_mask >> p) & 1u)
                 atomicAdd(&sh[p * kRadix + ((u32)(k0 >> P.shift[p]) & ((1u << P.bits[p]) - 1u))],
@@ -551,17 +569,31 @@ __global__ void __launch_bounds__(256) k_operand_hist(SoASrc<AS> src, u32 n, Key
         if (sh[i]) atomicAdd(&h[i], sh[i]);
 }
 
-// hist[p][d] = sum_{d1} hA[p][d1] * hB[p][d1 ^ d] for every pass p in conv_mask.
+__device__ __forceinline__ u32 block_excl_scan(u32 v, u32* s_warp, u32& total);
+
+// hist[p][d] = sum_{d1} hA[p][d1] * hB[p][d1 ^ d] for every pass p in conv_mask
+// (both operand histograms staged in shared memory).  With scan = 1 every
+// pass's histogram is derived, and the block turns it into the pass's
+// bucket starts (exclusive prefix) right away, in place of k_scan_buckets.
 __global__ void __launch_bounds__(256) k_xor_conv(const u32* hA, const u32* hB, PassPlan P,
-                                                  u32 conv_mask, u32* hist) {
+                                                  u32 conv_mask, u32* hist, int scan) {
+    __shared__ u32 sa[kRadix], sb[kRadix], sw[kWarps];
     const int p = blockIdx.x;
     if (!((conv_mask >> p) & 1u)) return;
     const u32 R = 1u << P.bits[p];
     const u32 d = threadIdx.x;
-    if (d >= R) return;
+    sa[d] = hA[p * kRadix + d];
+    sb[d] = hB[p * kRadix + d];
+    __syncthreads();
     u32 acc = 0;
-    for (u32 d1 = 0; d1 < R; ++d1) acc += hA[p * kRadix + d1] * hB[p * kRadix + (d1 ^ d)];
-    hist[p * kRadix + d] = acc;
+    if (d < R)
+        for (u32 d1 = 0; d1 < R; ++d1) acc += sa[d1] * sb[d1 ^ d];
+    if (!scan) {
+        if (d < R) hist[p * kRadix + d] = acc;
+        return;
+    }
+    u32 total;
+    hist[p * kRadix + d] = block_excl_scan(acc, sw, total);
 }
 
 // Chunk c >= 1: bring chunk c of every term into the current order and
@@ -726,7 +758,7 @@ __global__ void __launch_bounds__(kThreads, KONLY ? (ITEMS <= 12 ? 4 : 3)
                  u32* __restrict__ vout, u32 n, int shift, int bits,
                  const u32* __restrict__ bstart, u32* lb, u32* tile_ctr, int* status, Src src,
                  double* __restrict__ val_out, const uint2* __restrict__ phs, u64 imask,
-                 u32 pf_ahead) {
+                 u32 pf_ahead, u32* lb_next) {
     extern __shared__ __align__(16) unsigned char dsm[];
     u64* skeys = reinterpret_cast<u64*>(dsm);
     u32* svals = reinterpret_cast<u32*>(dsm + sizeof(u64) * (kThreads * ITEMS));
@@ -749,6 +781,10 @@ __global__ void __launch_bounds__(kThreads, KONLY ? (ITEMS <= 12 ? 4 : 3)
     const u32 tile = S.tile;
     const u32 base = tile * (u32)(kThreads * ITEMS);
     const u32 dmask = (1u << bits) - 1u;
+    // The next pass's look-back words (the other of two regions; the pass
+    // before this one used it and is done): each tile clears its own, so no
+    // pass needs a separate clearing launch.  kThreads == kRadix.
+    if (lb_next) lb_next[(size_t)tile * kRadix + tid] = 0u;
 
     u64 keys[ITEMS];
     u32 vals[KONLY ? 1 : ITEMS];
@@ -893,291 +929,6 @@ __global__ void __launch_bounds__(kThreads, KONLY ? (ITEMS <= 12 ? 4 : 3)
 constexpr size_t radix_smem(int items) { return (sizeof(u64) + sizeof(u32)) * kThreads * items; }
 constexpr size_t radix_smem_konly(int items) { return sizeof(u64) * kThreads * items; }
 
-// ---------------------------------------------------------------------------
-// 3b. Warp-specialised digit pass over index-packed keys.  A persistent CTA
-//     holds two tile buffers in shared memory.  Two producer warps take the
-//     next tile from the pass counter as soon as a buffer is free, bulk-copy
-//     its keys in (the TMA engine: cp.async.bulk, completion counted on an
-//     mbarrier), count its digit histogram and publish the tile's look-back
-//     aggregate at once.  Eight consumer warps meanwhile rank, scatter,
-//     walk the look-back and write out the previous tile.  Because every
-//     taken tile publishes its aggregate one copy and one count after it is
-//     taken -- never after a whole tile of other work -- taking tiles ahead
-//     does not stall anyone's look-back, and the DRAM latency of the key
-//     load overlaps the consumers' work.  Nothing waits on an unstarted CTA,
-//     so the grid need not be co-resident.  Same results as
-//     k_radix_pass<..., KONLY>: the same stable ranking and scatter.
-// ---------------------------------------------------------------------------
-__device__ __forceinline__ u32 smem_u32(const void* p) {
-    return (u32)__cvta_generic_to_shared(p);
-}
-__device__ __forceinline__ void mbar_init(u64* bar, u32 count) {
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count)
-                 : "memory");
-}
-__device__ __forceinline__ void mbar_arrive(u64* bar) {
-    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
-}
-__device__ __forceinline__ void mbar_expect_tx(u64* bar, u32 bytes) {
-    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)),
-                 "r"(bytes)
-                 : "memory");
-}
-__device__ __forceinline__ bool mbar_try_wait(u64* bar, u32 parity) {
-    u32 ok;
-    asm volatile(
-        "{\n\t.reg .pred p;\n\t"
-        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-        "selp.u32 %0, 1, 0, p;\n\t}"
-        : "=r"(ok)
-        : "r"(smem_u32(bar)), "r"(parity)
-        : "memory");
-    return ok != 0;
-}
-// Bounded wait for the completion of the phase with the given parity; false
-// (and PL_ERR_TIMEOUT recorded) once g_spin_limit polls have run out.
-__device__ __forceinline__ bool mbar_wait(u64* bar, u32 parity, int* status) {
-    for (u32 spins = 0; !mbar_try_wait(bar, parity);) {
-        if (++spins > g_spin_limit) {
-            raise_status(status, PL_ERR_TIMEOUT);
-            return false;
-        }
-    }
-    return true;
-}
-// Global -> shared bulk copy without multicast; dst and src 16-byte aligned,
-// bytes a multiple of 16; completion counted on `bar` as transaction bytes.
-__device__ __forceinline__ void bulk_load(void* dst, const void* src, u32 bytes, u64* bar) {
-    asm volatile(
-        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
-        ::"r"(smem_u32(dst)), "l"(src), "r"(bytes), "r"(smem_u32(bar))
-        : "memory");
-}
-// Named barriers: 1 = the consumer warps, 2 = the producer warps.
-__device__ __forceinline__ void bar_consumers() { asm volatile("bar.sync 1, 256;" ::: "memory"); }
-__device__ __forceinline__ void bar_producers() { asm volatile("bar.sync 2, 64;" ::: "memory"); }
-
-constexpr int kWsProducers = 2;
-constexpr int kWsThreads = kThreads + 32 * kWsProducers;
-
-struct WsSmem {
-    u16 whist[kWarps * kRadix];  // per consumer warp: digit counts, then tile positions
-    u32 gofs[kRadix];
-    u32 swarp[kWarps];
-    u32 phist[kWsProducers * kRadix];  // per producer warp: digit counts
-    u64 full[2], empty[2], counted[2];
-    u32 tile[2];  // tile held by each buffer (>= ntiles: the end)
-    u32 ctile;    // the consumers' current tile, as consumer thread 0 read it
-};
-
-template <class Src, bool LAST, int ITEMS>
-__global__ void __launch_bounds__(kWsThreads, 3)
-    k_radix_pass_ws(const u64* __restrict__ kin, u64* __restrict__ kout, u32 n, u32 ntiles,
-                    int shift, int bits, const u32* __restrict__ bstart, u32* lb, u32* tile_ctr,
-                    int* status, Src src, double* __restrict__ val_out,
-                    const uint2* __restrict__ phs, u64 imask) {
-    constexpr u32 kTile = (u32)(kThreads * ITEMS);
-    extern __shared__ __align__(128) unsigned char dsm[];
-    u64* bufs = reinterpret_cast<u64*>(dsm);  // two tiles of kTile keys
-    __shared__ __align__(16) WsSmem S;
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    const u32 dmask = (1u << bits) - 1u;
-    if (tid == 0) {
-        for (int b = 0; b < 2; ++b) {
-            mbar_init(&S.full[b], 1);
-            mbar_init(&S.empty[b], 1);
-            mbar_init(&S.counted[b], 1);
-            S.tile[b] = 0xffffffffu;  // the end mark until a tile is taken
-        }
-        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-    }
-    __syncthreads();
-
-    if (warp >= kWarps) {
-        // ---------------- producers ----------------
-        const int pw = warp - kWarps;
-        u32* ph = S.phist + pw * kRadix;
-        for (int k = 0;; ++k) {
-            const int b = k & 1;
-            // A wait that runs out records PL_ERR_TIMEOUT and goes on: every
-            // iteration takes a new tile, so the loop still ends, and the
-            // group's barriers stay uniform.
-            if (k >= 2) mbar_wait(&S.empty[b], ((k >> 1) - 1) & 1, status);
-            if (pw == 0 && lane == 0) {
-                const u32 t = atomicAdd(tile_ctr, 1u);
-                S.tile[b] = t;
-                const u32 cnt = t < ntiles ? (min(kTile, n - t * kTile) & ~1u) : 0u;
-                if (cnt) {
-                    mbar_expect_tx(&S.full[b], cnt * 8u);
-                    bulk_load(bufs + (size_t)b * kTile, kin + (size_t)t * kTile, cnt * 8u,
-                              &S.full[b]);
-                } else {
-                    mbar_arrive(&S.full[b]);  // the end, or a one-key final tile
-                }
-            }
-            bar_producers();
-            const u32 tile = S.tile[b];
-            if (tile >= ntiles) break;
-            const u32 base = tile * kTile;
-            const u32 tile_n = min(kTile, n - base);
-            const u32 cpn = tile_n & ~1u;
-            for (int d = lane; d < kRadix; d += 32) ph[d] = 0;
-            __syncwarp();
-            mbar_wait(&S.full[b], (k >> 1) & 1, status);  // every issued copy is waited for
-            const u64* sk = bufs + (size_t)b * kTile;
-            for (u32 p0 = (u32)pw * 32; p0 < tile_n; p0 += 32 * kWsProducers) {
-                const u32 p = p0 + lane;
-                const bool valid = p < tile_n;
-                const u64 key = p < cpn ? sk[p] : (valid ? kin[base + p] : 0ull);
-                const u32 d = valid ? ((u32)(key >> shift) & dmask) : kSentinel;
-                const u32 peers = __match_any_sync(0xffffffffu, d);
-                if (valid && lane == __ffs(peers) - 1) atomicAdd(&ph[d], (u32)__popc(peers));
-            }
-            bar_producers();
-            // the aggregate goes out before the consumers may overwrite the
-            // buffer or publish this tile's inclusive prefix
-            for (int d = pw * 32 + lane; d < kRadix; d += 32 * kWsProducers) {
-                u32 c = 0;
-#pragma unroll
-                for (int q = 0; q < kWsProducers; ++q) c += S.phist[q * kRadix + d];
-                lb_publish(lb + d, tile, kRadix, c);
-            }
-            bar_producers();
-            if (pw == 0 && lane == 0) mbar_arrive(&S.counted[b]);
-        }
-        return;
-    }
-
-    // ---------------- consumers ----------------
-    // A wait that runs out records PL_ERR_TIMEOUT and goes on; the loop ends
-    // at the producers' end mark, which consumer thread 0 reads for all.
-    for (int k = 0;; ++k) {
-        const int b = k & 1;
-        mbar_wait(&S.full[b], (k >> 1) & 1, status);
-        if (tid == 0) S.ctile = S.tile[b];
-        reinterpret_cast<uint4*>(S.whist)[tid] = make_uint4(0, 0, 0, 0);  // 4 KB, 16 B each
-        bar_consumers();
-        const u32 tile = S.ctile;
-        if (tile >= ntiles) break;
-        u64* skeys = bufs + (size_t)b * kTile;
-        const u32 base = tile * kTile;
-        const u32 tile_n = min(kTile, n - base);
-        const u32 cpn = tile_n & ~1u;
-
-        u64 keys[ITEMS];
-        u32 rank[(ITEMS + 1) / 2];
-        const u32 wloc = (u32)warp * (ITEMS * 32);
-#pragma unroll
-        for (int t = 0; t < ITEMS; ++t) {
-            const u32 li = wloc + t * 32 + lane;
-            keys[t] = li < cpn ? skeys[li] : (li < tile_n ? kin[base + li] : 0ull);
-        }
-        u16* wh = S.whist + warp * kRadix;
-#pragma unroll
-        for (int t = 0; t < ITEMS; ++t) {
-            const bool valid = (wloc + t * 32 + lane) < tile_n;
-            const u32 d = valid ? ((u32)(keys[t] >> shift) & dmask) : kSentinel;
-            const u32 peers = __match_any_sync(0xffffffffu, d);
-            const int leader = __ffs(peers) - 1;
-            u32 before = 0;
-            if (valid && lane == leader) {
-                before = wh[d];
-                wh[d] = (u16)(before + __popc(peers));
-            }
-            before = __shfl_sync(0xffffffffu, before, leader);
-            const u32 r = before + __popc(peers & lanemask_lt());
-            rank[t / 2] = (t & 1) ? (rank[t / 2] | (r << 16)) : r;
-            __syncwarp();
-        }
-        bar_consumers();
-        const u32 d = tid;
-        u32 run = 0;
-#pragma unroll
-        for (int w = 0; w < kWarps; ++w) {
-            const u32 c = S.whist[w * kRadix + d];
-            S.whist[w * kRadix + d] = (u16)run;
-            run += c;
-        }
-        // exclusive scan of run over the 256 consumer threads
-        u32 inc = run;
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            const u32 t = __shfl_up_sync(0xffffffffu, inc, o);
-            if (lane >= o) inc += t;
-        }
-        if (lane == 31) S.swarp[warp] = inc;
-        bar_consumers();
-        u32 wpre = 0;
-#pragma unroll
-        for (int w = 0; w < kWarps; ++w) wpre += (w < warp) ? S.swarp[w] : 0u;
-        const u32 bl = wpre + inc - run;
-#pragma unroll
-        for (int w = 0; w < kWarps; ++w) S.whist[w * kRadix + d] += (u16)bl;
-        bar_consumers();
-        // the producers must be done reading the buffer before the in-place
-        // scatter (and have published this tile's aggregate)
-        mbar_wait(&S.counted[b], (k >> 1) & 1, status);
-#pragma unroll
-        for (int t = 0; t < ITEMS; ++t) {
-            if (wloc + t * 32 + lane < tile_n) {
-                const u32 dd = (u32)(keys[t] >> shift) & dmask;
-                const u32 pos = (u32)S.whist[warp * kRadix + dd] +
-                                ((rank[t / 2] >> ((t & 1) * 16)) & 0xffffu);
-                skeys[pos] = keys[t];
-            }
-        }
-        const u32 excl = lb_walk<4>(lb + d, tile, kRadix, run, status);
-        S.gofs[d] = bstart[d] + excl - bl;
-        bar_consumers();
-        if constexpr (LAST) {
-            constexpr int kGather = 8;
-            for (u32 p0 = 0; p0 < tile_n; p0 += kGather * kThreads) {
-                u64 kk[kGather];
-                u32 gg[kGather], pb[kGather];
-                double vv[kGather];
-#pragma unroll
-                for (int q = 0; q < kGather; ++q) {
-                    const u32 p = p0 + (u32)q * kThreads + tid;
-                    gg[q] = 0xffffffffu;
-                    kk[q] = 0;
-                    pb[q] = 0;
-                    vv[q] = 0.0;
-                    if (p < tile_n) {
-                        const u64 kv = skeys[p];
-                        const u32 idx = (u32)(kv & imask);
-                        kk[q] = kv;
-                        gg[q] = S.gofs[(u32)(kv >> shift) & dmask] + p;
-                        if (idx < n) src.flags_value(idx, phs, pb[q], vv[q]);
-                        else gg[q] = n;  // reported below
-                    }
-                }
-#pragma unroll
-                for (int q = 0; q < kGather; ++q) {
-                    if (gg[q] < n) {
-                        kout[gg[q]] = (kk[q] & ~imask) | (u64)(pb[q] & 1u);
-                        val_out[gg[q]] = (pb[q] & 2u) ? -vv[q] : vv[q];
-                    } else if (gg[q] != 0xffffffffu) {
-                        raise_status(status, PL_ERR_INTERNAL);
-                    }
-                }
-            }
-        } else {
-            for (u32 p = tid; p < tile_n; p += kThreads) {
-                const u64 kv = skeys[p];
-                const u32 g = S.gofs[(u32)(kv >> shift) & dmask] + p;
-                if (g >= n) raise_status(status, PL_ERR_INTERNAL);
-                else kout[g] = kv;
-            }
-        }
-        // generic-proxy accesses of the buffer are ordered before the next
-        // bulk copy into it
-        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-        bar_consumers();
-        if (tid == 0) mbar_arrive(&S.empty[b]);
-    }
-}
-
-constexpr size_t radix_smem_ws(int items) { return 2 * sizeof(u64) * kThreads * items; }
 
 
 // ---------------------------------------------------------------------------
@@ -1336,7 +1087,7 @@ __device__ __forceinline__ u32 fold_close(double* segval, u8* segflag, i64 h, do
 template <int MODE>
 __global__ void __launch_bounds__(32 * kFoldWarps, 6)
     k_fold(SegCtx C, double* segval, u8* segflag, u32* wfirst, u32* long_list, u32* counters,
-           FoldFilter F) {
+           FoldFilter F, u32 pf_ranges) {
     extern __shared__ __align__(16) unsigned char fsm[];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const u32 gwarp = blockIdx.x * kFoldWarps + warp;
@@ -1344,6 +1095,15 @@ __global__ void __launch_bounds__(32 * kFoldWarps, 6)
     if (w0 >= C.n) return;
     const u32 w1 = min(w0 + kFoldSpan, C.n);
     const u32 cnt = w1 - w0;
+    if (pf_ranges && lane == 0) {
+        // the range about one wave ahead goes to L2 now (whole ranges only)
+        const u64 pw0 = (u64)w0 + (u64)pf_ranges * kFoldSpan;
+        if (pw0 + kFoldSpan <= C.n) {
+            prefetch_l2(C.keys + pw0, 8u * kFoldSpan);
+            prefetch_l2(C.vals + pw0, 8u * kFoldSpan);
+            if (MODE != kCanonSplit && C.pay) prefetch_l2(C.pay + pw0, 4u * kFoldSpan);
+        }
+    }
     unsigned char* base = fsm + ((kFoldWarpSmem + 15) & ~size_t(15)) * warp;
     double* sv = reinterpret_cast<double*>(base);
     u32* hbw = reinterpret_cast<u32*>(base + 8 * kFoldSlots);
@@ -1948,7 +1708,7 @@ int max_chunks(int as) { return (128 * as + 2 + 63) / 64; }
 
 struct Bufs {
     u64 *ka, *kb, *planes;
-    u32 *pa, *pb, *hist, *lb, *counters;
+    u32 *pa, *pb, *hist, *lb, *lb2, *counters;  // lb / lb2: look-back words of even / odd passes
     u8* segflag;
     double *seg_sum, *sv;
     u32 *wfirst, *long_list;
@@ -1974,6 +1734,7 @@ void carve_all(Carve& c, i64 n, int nch, Bufs& B) {
     B.planes_bytes = sizeof(u64) * (nch > 1 ? (size_t)n * nch : 1);
     B.hist = c.take<u32>(kMaxPasses * kRadix);
     B.lb = c.take<u32>((size_t)rtiles * kRadix);
+    B.lb2 = c.take<u32>((size_t)rtiles * kRadix);
     B.segflag = c.take<u8>(n + 16);
     B.seg_sum = c.take<double>(n);
     B.wfirst = c.take<u32>(ngw);
@@ -2106,8 +1867,19 @@ int fold_segments(const SegCtx& C, Bufs& B, const FoldFilter& F, int nsm, cudaSt
     PL_CUDA_TRY(cudaFuncSetAttribute(k_fold<MODE>,
                                      cudaFuncAttributePreferredSharedMemoryCarveout,
                                      cudaSharedmemCarveoutMaxShared));
+    // L2 prefetch one wave of fold ranges ahead (off with PL_TUNE_RADIX_PREFETCH = -1)
+    static int per_sm = 0;
+    if (per_sm == 0) {
+        int b = 0;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_fold<MODE>, 32 * kFoldWarps,
+                                                          kFoldSmem) != cudaSuccess ||
+            b < 1)
+            b = 1;
+        per_sm = b;
+    }
+    const u32 pf = tuning(PL_TUNE_RADIX_PREFETCH) < 0 ? 0u : (u32)(per_sm * kFoldWarps * nsm);
     k_fold<MODE><<<fold_blocks, 32 * kFoldWarps, kFoldSmem, st>>>(
-        C, B.seg_sum, B.segflag, B.wfirst, B.long_list, B.counters, F), pl::note_launch();
+        C, B.seg_sum, B.segflag, B.wfirst, B.long_list, B.counters, F, pf), pl::note_launch();
     // at most one pending segment per fold range
     const int cw_blocks = (int)std::min<u32>((ngw + 7) / 8, (u32)nsm * 4);
     k_fold_carry<MODE><<<cw_blocks, 256, 0, st>>>(B.wfirst, ngw, B.long_list, B.counters,
@@ -2117,20 +1889,25 @@ int fold_segments(const SegCtx& C, Bufs& B, const FoldFilter& F, int nsm, cudaSt
 
 // Histograms that can be derived instead of counted: none for a plain sum.
 template <int AS>
-u32 derive_histograms(const SoASrc<AS>&, const KeyLayout&, const PassPlan&, Bufs&,
-                      cudaStream_t) {
+u32 derive_histograms(const SoASrc<AS>&, const KeyLayout&, const PassPlan&, Bufs&, cudaStream_t,
+                      bool* scanned, u64* = nullptr) {
+    *scanned = false;
     return 0u;
 }
 template <int AS>
-u32 derive_histograms(const WinSrc<AS>&, const KeyLayout&, const PassPlan&, Bufs&,
-                      cudaStream_t) {
+u32 derive_histograms(const WinSrc<AS>&, const KeyLayout&, const PassPlan&, Bufs&, cudaStream_t,
+                      bool* scanned, u64* = nullptr) {
+    *scanned = false;
     return 0u;
 }
 
 // Products: chunk-0 passes free of flags bits come from operand histograms.
+// When they are all the passes, the convolution also writes the bucket
+// starts and *scanned is set (no k_scan_buckets needed).
 template <int AS>
 u32 derive_histograms(const ProdSrc<AS>& src, const KeyLayout& L, const PassPlan& P, Bufs& B,
-                      cudaStream_t st) {
+                      cudaStream_t st, bool* scanned, u64* opk = nullptr) {
+    *scanned = false;
     const int np0 = P.first[1] - P.first[0];
     const int wf = L.width[2 * AS];  // the flags field occupies packed bits [0, wf)
     u32 mask = 0;
@@ -2142,12 +1919,24 @@ u32 derive_histograms(const ProdSrc<AS>& src, const KeyLayout& L, const PassPlan
     if (fill32_async(hA, 0u, sizeof(u32) * 16 * kRadix, st) != cudaSuccess) return 0u;
     const SoASrc<AS> a{src.ax, src.az, src.af, src.av, src.sa};
     const SoASrc<AS> b{src.bx, src.bz, src.bf, src.bv, src.sb};
-    k_operand_hist<AS><<<grid_for(src.n, 256, 64), 256, 0, st>>>(a, src.n, L, P, mask, hA),
+    const dim3 g(grid_for(std::max(src.n, src.m), 256, 64), 2);
+    k_operand_hist<AS><<<g, 256, 0, st>>>(a, src.n, hA, b, src.m, hB, L, P, mask, opk),
         pl::note_launch();
-    k_operand_hist<AS><<<grid_for(src.m, 256, 64), 256, 0, st>>>(b, src.m, L, P, mask, hB),
-        pl::note_launch();
-    k_xor_conv<<<np0, 256, 0, st>>>(hA, hB, P, mask, B.hist), pl::note_launch();
+    const bool all = np0 == P.npasses && mask == (1u << np0) - 1u;
+    k_xor_conv<<<np0, 256, 0, st>>>(hA, hB, P, mask, B.hist, all ? 1 : 0), pl::note_launch();
+    *scanned = all;
     return mask;
+}
+
+// Room for a product's operand packed keys (n_lhs + n_rhs words) in an
+// n-word buffer; none for a plain sum.
+template <class Src>
+bool operand_key_room(const Src&, u32) {
+    return false;
+}
+template <int AS>
+bool operand_key_room(const ProdSrc<AS>& src, u32 n) {
+    return (u64)src.n + src.m <= (u64)n;
 }
 
 // Keys per thread of a digit pass (8, 12 or 16; PL_TUNE_RADIX_ITEMS).
@@ -2185,7 +1974,8 @@ u32 prefetch_ahead(K* kernel, size_t smem, int& per_sm) {
 
 template <class Src, int ITEMS>
 int radix_pass(bool last, const u64* kin, const u32* vin, u64* kout, u32* vout, u32 n, int shift,
-               int bits, const u32* bstart, Bufs& B, u32* ctr, const Src& src, cudaStream_t st) {
+               int bits, const u32* bstart, Bufs& B, u32* lb, u32* lb_next, u32* ctr,
+               const Src& src, cudaStream_t st) {
     const u32 tiles = (n + kThreads * ITEMS - 1) / (kThreads * ITEMS);
     const SoASrc<1> nosrc{nullptr, nullptr, nullptr, nullptr, 0};
     const size_t sm = radix_smem(ITEMS);
@@ -2193,61 +1983,16 @@ int radix_pass(bool last, const u64* kin, const u32* vin, u64* kout, u32* vout, 
     if (last) {
         auto* k = k_radix_pass<Src, true, ITEMS, false>;
         PL_CUDA_TRY(radix_attrs(k, (int)sm));
-        k<<<tiles, kThreads, sm, st>>>(kin, vin, kout, vout, n, shift, bits, bstart, B.lb, ctr,
+        k<<<tiles, kThreads, sm, st>>>(kin, vin, kout, vout, n, shift, bits, bstart, lb, ctr,
                                        B.d_status, src, B.sv, nullptr, 0ull,
-                                       prefetch_ahead(k, sm, occ_last)),
+                                       prefetch_ahead(k, sm, occ_last), lb_next),
             pl::note_launch();
     } else {
         auto* k = k_radix_pass<SoASrc<1>, false, ITEMS, false>;
         PL_CUDA_TRY(radix_attrs(k, (int)sm));
-        k<<<tiles, kThreads, sm, st>>>(kin, vin, kout, vout, n, shift, bits, bstart, B.lb, ctr,
+        k<<<tiles, kThreads, sm, st>>>(kin, vin, kout, vout, n, shift, bits, bstart, lb, ctr,
                                        B.d_status, nosrc, nullptr, nullptr, 0ull,
-                                       prefetch_ahead(k, sm, occ_mid)),
-            pl::note_launch();
-    }
-    return PL_OK;
-}
-
-// Warp-specialised digit passes (k_radix_pass_ws) for index-packed keys:
-// PL_TUNE_RADIX_WS 1 on, 0 (default) / -1 off.
-bool radix_ws() { return tuning(PL_TUNE_RADIX_WS) > 0; }
-
-// One wave of k_radix_pass_ws: resident CTAs per SM (looked up once per
-// kernel instantiation into `per_sm`) x SMs, at most a CTA per tile.
-template <class K>
-int ws_grid(K* kernel, size_t smem, u32 tiles, int& per_sm) {
-    if (per_sm == 0) {
-        int b = 0;
-        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, kernel, kWsThreads, smem) !=
-                cudaSuccess ||
-            b < 1)
-            b = 1;
-        per_sm = b;
-    }
-    return (int)std::min<u32>(tiles, (u32)(per_sm * sm_count()));
-}
-
-template <class Src, int ITEMS>
-int radix_pass_ws(bool last, const u64* kin, u64* kout, u32 n, int shift, int bits,
-                  const u32* bstart, Bufs& B, u32* ctr, const Src& src, const uint2* phs,
-                  u64 imask, cudaStream_t st) {
-    const u32 tiles = (n + kThreads * ITEMS - 1) / (kThreads * ITEMS);
-    const size_t sm = radix_smem_ws(ITEMS);
-    static int occ_last = 0, occ_mid = 0;
-    if (last) {
-        auto* k = k_radix_pass_ws<Src, true, ITEMS>;
-        PL_CUDA_TRY(radix_attrs(k, (int)sm));
-        k<<<ws_grid(k, sm, tiles, occ_last), kWsThreads, sm, st>>>(
-            kin, kout, n, tiles, shift, bits, bstart, B.lb, ctr, B.d_status, src, B.sv, phs,
-            imask),
-            pl::note_launch();
-    } else {
-        const SoASrc<1> nosrc{nullptr, nullptr, nullptr, nullptr, 0};
-        auto* k = k_radix_pass_ws<SoASrc<1>, false, ITEMS>;
-        PL_CUDA_TRY(radix_attrs(k, (int)sm));
-        k<<<ws_grid(k, sm, tiles, occ_mid), kWsThreads, sm, st>>>(
-            kin, kout, n, tiles, shift, bits, bstart, B.lb, ctr, B.d_status, nosrc, nullptr,
-            nullptr, imask),
+                                       prefetch_ahead(k, sm, occ_mid), lb_next),
             pl::note_launch();
     }
     return PL_OK;
@@ -2256,28 +2001,25 @@ int radix_pass_ws(bool last, const u64* kin, u64* kout, u32 n, int shift, int bi
 // Digit pass over index-packed keys (no payload).
 template <class Src, int ITEMS>
 int radix_pass_konly(bool last, const u64* kin, u64* kout, u32 n, int shift, int bits,
-                     const u32* bstart, Bufs& B, u32* ctr, const Src& src, const uint2* phs,
-                     u64 imask, cudaStream_t st) {
-    if (radix_ws())
-        return radix_pass_ws<Src, ITEMS>(last, kin, kout, n, shift, bits, bstart, B, ctr, src,
-                                         phs, imask, st);
+                     const u32* bstart, Bufs& B, u32* lb, u32* lb_next, u32* ctr, const Src& src,
+                     const uint2* phs, u64 imask, cudaStream_t st) {
     const u32 tiles = (n + kThreads * ITEMS - 1) / (kThreads * ITEMS);
     const size_t sm = radix_smem_konly(ITEMS);
     static int occ_last = 0, occ_mid = 0;
     if (last) {
         auto* k = k_radix_pass<Src, true, ITEMS, true>;
         PL_CUDA_TRY(radix_attrs(k, (int)sm));
-        k<<<tiles, kThreads, sm, st>>>(kin, nullptr, kout, nullptr, n, shift, bits, bstart, B.lb,
+        k<<<tiles, kThreads, sm, st>>>(kin, nullptr, kout, nullptr, n, shift, bits, bstart, lb,
                                        ctr, B.d_status, src, B.sv, phs, imask,
-                                       prefetch_ahead(k, sm, occ_last)),
+                                       prefetch_ahead(k, sm, occ_last), lb_next),
             pl::note_launch();
     } else {
         const SoASrc<1> nosrc{nullptr, nullptr, nullptr, nullptr, 0};
         auto* k = k_radix_pass<SoASrc<1>, false, ITEMS, true>;
         PL_CUDA_TRY(radix_attrs(k, (int)sm));
-        k<<<tiles, kThreads, sm, st>>>(kin, nullptr, kout, nullptr, n, shift, bits, bstart, B.lb,
+        k<<<tiles, kThreads, sm, st>>>(kin, nullptr, kout, nullptr, n, shift, bits, bstart, lb,
                                        ctr, B.d_status, nosrc, nullptr, nullptr, imask,
-                                       prefetch_ahead(k, sm, occ_mid)),
+                                       prefetch_ahead(k, sm, occ_mid), lb_next),
             pl::note_launch();
     }
     return PL_OK;
@@ -2290,14 +2032,18 @@ int run_collate(const Src& src, u32 n, int mode, const KeyLayout& L, const PassP
     const int items = radix_items();
     const u32 rtiles = (n + kThreads * items - 1) / (kThreads * items);
     const int nsm = sm_count();
-    const FillReq fr[4] = {{B.hist, 0u, sizeof(u32) * (size_t)std::max(P.npasses, 1) * kRadix},
+    // the look-back words of the first digit pass; every pass clears the
+    // next one's
+    const FillReq fr[5] = {{B.hist, 0u, sizeof(u32) * (size_t)std::max(P.npasses, 1) * kRadix},
                            {B.counters, 0u, sizeof(u32) * (size_t)(P.npasses + 8)},
                            {B.d_status, 0u, sizeof(int)},
-                           {B.d_count, 0u, sizeof(i64)}};
-    PL_CUDA_TRY(fill32_multi(fr, 4, st));
+                           {B.d_count, 0u, sizeof(i64)},
+                           {B.lb, 0u, sizeof(u32) * (size_t)rtiles * kRadix}};
+    PL_CUDA_TRY(fill32_multi(fr, 5, st));
     const int gblocks = grid_for(n, 256, nsm * 8);
     cudaEvent_t e0 = timed_begin(st);
-    const u32 derived = derive_histograms<AS>(src, L, P, B, st);
+    bool scanned = false;
+    const u32 derived = derive_histograms<AS>(src, L, P, B, st, &scanned);
     timed_end(e0, st, "k_xor_conv", 0ull);
     e0 = timed_begin(st);
     k_pack<AS, Src><<<gblocks, 256, 0, st>>>(src, n, mode, L, P, ~derived, B.ka, B.pa, B.planes,
@@ -2316,23 +2062,24 @@ int run_collate(const Src& src, u32 n, int mode, const KeyLayout& L, const PassP
                                                     B.hist, B.d_status), pl::note_launch();
             timed_end(e0, st, "k_gather_chunk", 20ull * n);
         }
-        k_scan_buckets<<<np, kRadix, 0, st>>>(B.hist, p0), pl::note_launch();
+        if (!(c == 0 && scanned)) k_scan_buckets<<<np, kRadix, 0, st>>>(B.hist, p0), pl::note_launch();
         for (int p = p0; p < p0 + np; ++p) {
-            PL_CUDA_TRY(fill32_async(B.lb, 0u, sizeof(u32) * (size_t)rtiles * kRadix, st));
             cudaEvent_t ev0 = timed_begin(st);
             const bool last = (p == P.npasses - 1);
             const u32* bs = B.hist + (size_t)p * kRadix;
             u32* ctr = B.counters + 8 + p;
+            u32* lb = (p & 1) ? B.lb2 : B.lb;
+            u32* lbn = (p & 1) ? B.lb : B.lb2;
             int rc = PL_OK;
             if (items == 16)
                 rc = radix_pass<Src, 16>(last, kin, vin, kout, vout, n, P.shift[p], P.bits[p], bs,
-                                         B, ctr, src, st);
+                                         B, lb, lbn, ctr, src, st);
             else if (items == 12)
                 rc = radix_pass<Src, 12>(last, kin, vin, kout, vout, n, P.shift[p], P.bits[p], bs,
-                                         B, ctr, src, st);
+                                         B, lb, lbn, ctr, src, st);
             else
                 rc = radix_pass<Src, 8>(last, kin, vin, kout, vout, n, P.shift[p], P.bits[p], bs,
-                                        B, ctr, src, st);
+                                        B, lb, lbn, ctr, src, st);
             if (rc) return rc;
             // algorithmic bytes: read and write one u64 key + one u32 payload per
             // term (+ the u64 coefficient written by the last pass)
@@ -2396,39 +2143,48 @@ int run_collate_split(const Src& src, u32 n, const KeyLayout& L, const PassPlan&
     // then the (phase-0, phase-1) sums of the segments
     uint2* phs = reinterpret_cast<uint2*>(B.planes);
     double2* seg2 = reinterpret_cast<double2*>(reinterpret_cast<unsigned char*>(B.planes) + al(n));
-    const FillReq fr[4] = {{B.hist, 0u, sizeof(u32) * (size_t)std::max(P.npasses, 1) * kRadix},
+    // the look-back words of the first digit pass; every pass clears the
+    // next one's
+    const FillReq fr[5] = {{B.hist, 0u, sizeof(u32) * (size_t)std::max(P.npasses, 1) * kRadix},
                            {B.counters, 0u, sizeof(u32) * (size_t)(P.npasses + 8)},
                            {B.d_status, 0u, sizeof(int)},
-                           {B.d_count, 0u, sizeof(i64)}};
-    PL_CUDA_TRY(fill32_multi(fr, 4, st));
+                           {B.d_count, 0u, sizeof(i64)},
+                           {B.lb, 0u, sizeof(u32) * (size_t)rtiles * kRadix}};
+    PL_CUDA_TRY(fill32_multi(fr, 5, st));
     const int gblocks = grid_for(n, 256, nsm * 8);
     cudaEvent_t e0 = timed_begin(st);
-    const u32 derived = derive_histograms<AS>(src, L, P, B, st);
+    bool scanned = false;
+    // a product's operand packed keys go to B.sv, unused until the last
+    // digit pass writes the sorted coefficients there
+    u64* opk = operand_key_room(src, n) ? reinterpret_cast<u64*>(B.sv) : nullptr;
+    const u32 derived = derive_histograms<AS>(src, L, P, B, st, &scanned, opk);
     timed_end(e0, st, "k_xor_conv", 0ull);
     const u32 count_mask = ~derived & ((1u << P.npasses) - 1u);
+    if (!derived) opk = nullptr;  // not written
     e0 = timed_begin(st);
-    if (!pack_split_fast<AS>(src, n, L, count_mask, B.ka, phs, st))
+    if (!pack_split_fast<AS>(src, n, L, count_mask, B.ka, phs, opk, st))
         k_pack_split<AS, Src><<<gblocks, 256, 0, st>>>(src, n, L, P, count_mask, B.ka, phs,
                                                        B.hist), pl::note_launch();
     timed_end(e0, st, "k_pack", 8ull * n + n / 4);
-    k_scan_buckets<<<P.npasses, kRadix, 0, st>>>(B.hist, 0), pl::note_launch();
+    if (!scanned) k_scan_buckets<<<P.npasses, kRadix, 0, st>>>(B.hist, 0), pl::note_launch();
     u64 *kin = B.ka, *kout = B.kb;
     for (int p = 0; p < P.npasses; ++p) {
-        PL_CUDA_TRY(fill32_async(B.lb, 0u, sizeof(u32) * (size_t)rtiles * kRadix, st));
         cudaEvent_t ev0 = timed_begin(st);
         const bool last = (p == P.npasses - 1);
         const u32* bs = B.hist + (size_t)p * kRadix;
         u32* ctr = B.counters + 8 + p;
+        u32* lb = (p & 1) ? B.lb2 : B.lb;
+        u32* lbn = (p & 1) ? B.lb : B.lb2;
         int rc = PL_OK;
         if (items == 16)
-            rc = radix_pass_konly<Src, 16>(last, kin, kout, n, P.shift[p], P.bits[p], bs, B, ctr,
-                                           src, phs, imask, st);
+            rc = radix_pass_konly<Src, 16>(last, kin, kout, n, P.shift[p], P.bits[p], bs, B, lb,
+                                           lbn, ctr, src, phs, imask, st);
         else if (items == 12)
-            rc = radix_pass_konly<Src, 12>(last, kin, kout, n, P.shift[p], P.bits[p], bs, B, ctr,
-                                           src, phs, imask, st);
+            rc = radix_pass_konly<Src, 12>(last, kin, kout, n, P.shift[p], P.bits[p], bs, B, lb,
+                                           lbn, ctr, src, phs, imask, st);
         else
-            rc = radix_pass_konly<Src, 8>(last, kin, kout, n, P.shift[p], P.bits[p], bs, B, ctr,
-                                          src, phs, imask, st);
+            rc = radix_pass_konly<Src, 8>(last, kin, kout, n, P.shift[p], P.bits[p], bs, B, lb,
+                                          lbn, ctr, src, phs, imask, st);
         if (rc) return rc;
         // algorithmic bytes: read and write one u64 key per term (+ the two
         // phase / sign bits read and the u64 coefficient written by the last pass)

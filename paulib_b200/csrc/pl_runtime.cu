@@ -381,7 +381,7 @@ extern "C" int pl_set_tuning(int key, int64_t value) {
         pl::g_tuning[key].store(value);
         return pl::record_status(PL_OK, nullptr);
     }
-    if ((key == PL_TUNE_INDEX_KEYS || key == PL_TUNE_WINDOW_KEYS || key == PL_TUNE_RADIX_WS) &&
+    if ((key == PL_TUNE_INDEX_KEYS || key == PL_TUNE_WINDOW_KEYS) &&
         (value == 0 || value == 1 || value == -1)) {
         pl::g_tuning[key].store(value);
         return pl::record_status(PL_OK, nullptr);
