@@ -246,22 +246,26 @@ def run_product_collate(args, rank, local, ws):
 
     # ---- autotune: keys per thread of the digit pass -------------------
     tune_trials = []
-    # (L2 prefetch one wave ahead / off) x keys per thread
-    for prefetch in (0, -1):
-        for items in (8, 12, 16):
-            _abi.check(L.pl_set_tuning(_abi.PL_TUNE_RADIX_ITEMS, items), "pl_set_tuning")
-            _abi.check(L.pl_set_tuning(_abi.PL_TUNE_RADIX_PREFETCH, prefetch), "pl_set_tuning")
+    # (L2 prefetch one wave ahead / off) x keys per thread; --tune fixes one
+    # combination (profiling runs: fewer trial collates)
+    combos = [(p_, i_) for p_ in (0, -1) for i_ in (8, 12, 16)]
+    if args.tune:
+        i_, p_ = (int(v) for v in args.tune.split(","))
+        combos = [(p_, i_)]
+    for prefetch, items in combos:
+        _abi.check(L.pl_set_tuning(_abi.PL_TUNE_RADIX_ITEMS, items), "pl_set_tuning")
+        _abi.check(L.pl_set_tuning(_abi.PL_TUNE_RADIX_PREFETCH, prefetch), "pl_set_tuning")
+        step()
+        torch.cuda.synchronize()
+        t0 = torch.cuda.Event(enable_timing=True)
+        t1 = torch.cuda.Event(enable_timing=True)
+        t0.record(stream)
+        for _ in range(3):
             step()
-            torch.cuda.synchronize()
-            t0 = torch.cuda.Event(enable_timing=True)
-            t1 = torch.cuda.Event(enable_timing=True)
-            t0.record(stream)
-            for _ in range(3):
-                step()
-            t1.record(stream)
-            torch.cuda.synchronize()
-            tune_trials.append({"radix_items": items, "radix_prefetch": prefetch,
-                                "ms_per_step": t0.elapsed_time(t1) / 3})
+        t1.record(stream)
+        torch.cuda.synchronize()
+        tune_trials.append({"radix_items": items, "radix_prefetch": prefetch,
+                            "ms_per_step": t0.elapsed_time(t1) / 3})
     best = min(tune_trials, key=lambda t: t["ms_per_step"])
     best_items, best_pf = best["radix_items"], best["radix_prefetch"]
     if ws > 1:  # every rank uses rank 0's choice
@@ -742,6 +746,9 @@ def main(argv=None):
     ap.add_argument("--serve-load", type=float, default=1.2,
                     help="serve workload: arrival rate as a multiple of the plain path's capacity")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--tune", default="",
+                    help="ITEMS,PREFETCH: fix the digit-pass tuning instead of timing every "
+                         "combination (e.g. 16,0)")
     ap.add_argument("--no-extras", action="store_true",
                     help="product_collate: skip the GPU comparator, propagation and served "
                          "sub-objects")

@@ -464,9 +464,8 @@ PL_API int pl_serve(const pl_job* jobs, int64_t count, const pl_batch_opts* opts
 /* L2 prefetch distance of the digit passes, in tiles: each tile's CTA
  * bulk-prefetches into L2 the keys of the tile this many places ahead, so
  * the CTA that later takes that tile reads L2 instead of DRAM.  0 (default):
- * one wave (resident CTAs per SM x SMs); -1: off; k > 0: k tiles.  The
- * segment fold prefetches one wave of its ranges ahead unless this is -1.
- * Results are identical either way. */
+ * one wave (resident CTAs per SM x SMs); -1: off; k > 0: k tiles.  Results
+ * are identical either way. */
 #define PL_TUNE_RADIX_PREFETCH 6
 /* Polls a cross-CTA wait (decoupled look-back) makes before it records
  * PL_ERR_TIMEOUT and returns: 1 .. 2^30, 0 = the default 2^20 (with a 64 ns

@@ -931,6 +931,7 @@ constexpr size_t radix_smem_konly(int items) { return sizeof(u64) * kThreads * i
 
 
 
+
 // ---------------------------------------------------------------------------
 // 4. Segments: equal-key runs of the sorted order.
 // ---------------------------------------------------------------------------
@@ -1087,7 +1088,7 @@ __device__ __forceinline__ u32 fold_close(double* segval, u8* segflag, i64 h, do
 template <int MODE>
 __global__ void __launch_bounds__(32 * kFoldWarps, 6)
     k_fold(SegCtx C, double* segval, u8* segflag, u32* wfirst, u32* long_list, u32* counters,
-           FoldFilter F, u32 pf_ranges) {
+           FoldFilter F) {
     extern __shared__ __align__(16) unsigned char fsm[];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const u32 gwarp = blockIdx.x * kFoldWarps + warp;
@@ -1095,15 +1096,7 @@ __global__ void __launch_bounds__(32 * kFoldWarps, 6)
     if (w0 >= C.n) return;
     const u32 w1 = min(w0 + kFoldSpan, C.n);
     const u32 cnt = w1 - w0;
-    if (pf_ranges && lane == 0) {
-        // the range about one wave ahead goes to L2 now (whole ranges only)
-        const u64 pw0 = (u64)w0 + (u64)pf_ranges * kFoldSpan;
-        if (pw0 + kFoldSpan <= C.n) {
-            prefetch_l2(C.keys + pw0, 8u * kFoldSpan);
-            prefetch_l2(C.vals + pw0, 8u * kFoldSpan);
-            if (MODE != kCanonSplit && C.pay) prefetch_l2(C.pay + pw0, 4u * kFoldSpan);
-        }
-    }
+
     unsigned char* base = fsm + ((kFoldWarpSmem + 15) & ~size_t(15)) * warp;
     double* sv = reinterpret_cast<double*>(base);
     u32* hbw = reinterpret_cast<u32*>(base + 8 * kFoldSlots);
@@ -1867,19 +1860,8 @@ int fold_segments(const SegCtx& C, Bufs& B, const FoldFilter& F, int nsm, cudaSt
     PL_CUDA_TRY(cudaFuncSetAttribute(k_fold<MODE>,
                                      cudaFuncAttributePreferredSharedMemoryCarveout,
                                      cudaSharedmemCarveoutMaxShared));
-    // L2 prefetch one wave of fold ranges ahead (off with PL_TUNE_RADIX_PREFETCH = -1)
-    static int per_sm = 0;
-    if (per_sm == 0) {
-        int b = 0;
-        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_fold<MODE>, 32 * kFoldWarps,
-                                                          kFoldSmem) != cudaSuccess ||
-            b < 1)
-            b = 1;
-        per_sm = b;
-    }
-    const u32 pf = tuning(PL_TUNE_RADIX_PREFETCH) < 0 ? 0u : (u32)(per_sm * kFoldWarps * nsm);
     k_fold<MODE><<<fold_blocks, 32 * kFoldWarps, kFoldSmem, st>>>(
-        C, B.seg_sum, B.segflag, B.wfirst, B.long_list, B.counters, F, pf), pl::note_launch();
+        C, B.seg_sum, B.segflag, B.wfirst, B.long_list, B.counters, F), pl::note_launch();
     // at most one pending segment per fold range
     const int cw_blocks = (int)std::min<u32>((ngw + 7) / 8, (u32)nsm * 4);
     k_fold_carry<MODE><<<cw_blocks, 256, 0, st>>>(B.wfirst, ngw, B.long_list, B.counters,
