@@ -246,15 +246,14 @@ def run_product_collate(args, rank, local, ws):
 
     # ---- autotune: keys per thread of the digit pass -------------------
     tune_trials = []
-    # (L2 prefetch one wave ahead / off) x keys per thread; --tune fixes one
+    # (L2 prefetch one wave ahead / off) x keys per thread at a look-back
+    # window of 4, then the window at the best of those; --tune fixes one
     # combination (profiling runs: fewer trial collates)
-    combos = [(p_, i_) for p_ in (0, -1) for i_ in (8, 12, 16)]
-    if args.tune:
-        i_, p_ = (int(v) for v in args.tune.split(","))
-        combos = [(p_, i_)]
-    for prefetch, items in combos:
+    def trial(items, prefetch, window, wide=-1):
         _abi.check(L.pl_set_tuning(_abi.PL_TUNE_RADIX_ITEMS, items), "pl_set_tuning")
         _abi.check(L.pl_set_tuning(_abi.PL_TUNE_RADIX_PREFETCH, prefetch), "pl_set_tuning")
+        _abi.check(L.pl_set_tuning(_abi.PL_TUNE_RADIX_WINDOW, window), "pl_set_tuning")
+        _abi.check(L.pl_set_tuning(_abi.PL_TUNE_RADIX_WIDE, wide), "pl_set_tuning")
         step()
         torch.cuda.synchronize()
         t0 = torch.cuda.Event(enable_timing=True)
@@ -265,16 +264,31 @@ def run_product_collate(args, rank, local, ws):
         t1.record(stream)
         torch.cuda.synchronize()
         tune_trials.append({"radix_items": items, "radix_prefetch": prefetch,
+                            "radix_window": window, "radix_wide": wide,
                             "ms_per_step": t0.elapsed_time(t1) / 3})
+
+    if args.tune:
+        trial(*(int(v) for v in args.tune.split(",")))
+    else:
+        for wide in (-1, 1):  # 8-bit / 10-bit digits (10-bit needs >= 12 keys per thread)
+            for prefetch in (0, -1):
+                for items in ((8, 12, 16) if wide < 0 else (12, 16)):
+                    trial(items, prefetch, 4, wide)
+        b0 = min(tune_trials, key=lambda t: t["ms_per_step"])
+        for window in (2, 8, 16):
+            trial(b0["radix_items"], b0["radix_prefetch"], window, b0["radix_wide"])
     best = min(tune_trials, key=lambda t: t["ms_per_step"])
-    best_items, best_pf = best["radix_items"], best["radix_prefetch"]
+    best_items, best_pf, best_w, best_wide = (best["radix_items"], best["radix_prefetch"],
+                                              best["radix_window"], best["radix_wide"])
     if ws > 1:  # every rank uses rank 0's choice
         import torch.distributed as dist
-        t = torch.tensor([best_items, best_pf], device="cuda")
+        t = torch.tensor([best_items, best_pf, best_w, best_wide], device="cuda")
         dist.broadcast(t, 0)
-        best_items, best_pf = (int(v) for v in t.tolist())
+        best_items, best_pf, best_w, best_wide = (int(v) for v in t.tolist())
     _abi.check(L.pl_set_tuning(_abi.PL_TUNE_RADIX_ITEMS, best_items), "pl_set_tuning")
     _abi.check(L.pl_set_tuning(_abi.PL_TUNE_RADIX_PREFETCH, best_pf), "pl_set_tuning")
+    _abi.check(L.pl_set_tuning(_abi.PL_TUNE_RADIX_WINDOW, best_w), "pl_set_tuning")
+    _abi.check(L.pl_set_tuning(_abi.PL_TUNE_RADIX_WIDE, best_wide), "pl_set_tuning")
     for _ in range(args.warmup):
         n_out = step()
     torch.cuda.synchronize()
@@ -401,9 +415,12 @@ def run_product_collate(args, rank, local, ws):
         "config": product_config(ws, n, m),
         "result": {"terms_out": n_out},
         "tuned": {"radix_items": best_items, "radix_l2_prefetch": best_pf == 0,
+                  "radix_lookback_window": best_w, "radix_digit_bits": 10 if best_wide > 0 else 8,
                   "trials_ms_per_step": {
                       ("prefetch" if t["radix_prefetch"] == 0 else "plain")
-                      + f"-{t['radix_items']}": t["ms_per_step"] for t in tune_trials}},
+                      + f"-{t['radix_items']}-w{t['radix_window']}"
+                      + ("-d10" if t["radix_wide"] > 0 else "-d8"): t["ms_per_step"]
+                      for t in tune_trials}},
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d,
                 "d2h_bytes_per_step": int(statistics.mean(d2h)),
                 "path": "pinned host planes -> H2D -> pl_multiply_collate (C ABI) -> D2H of "
@@ -747,8 +764,8 @@ def main(argv=None):
                     help="serve workload: arrival rate as a multiple of the plain path's capacity")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--tune", default="",
-                    help="ITEMS,PREFETCH: fix the digit-pass tuning instead of timing every "
-                         "combination (e.g. 16,0)")
+                    help="ITEMS,PREFETCH,WINDOW[,WIDE]: fix the digit-pass tuning instead of "
+                         "timing the combinations (e.g. 16,0,4 or 12,0,8,1)")
     ap.add_argument("--no-extras", action="store_true",
                     help="product_collate: skip the GPU comparator, propagation and served "
                          "sub-objects")

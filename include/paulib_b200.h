@@ -467,6 +467,16 @@ PL_API int pl_serve(const pl_job* jobs, int64_t count, const pl_batch_opts* opts
  * one wave (resident CTAs per SM x SMs); -1: off; k > 0: k tiles.  Results
  * are identical either way. */
 #define PL_TUNE_RADIX_PREFETCH 6
+/* Look-back window of the digit passes: predecessor tiles read per round
+ * trip while a tile waits for its global bucket offsets: 2, 4 (default), 8
+ * or 16.  Results are identical either way. */
+#define PL_TUNE_RADIX_WINDOW 7
+/* Digit width of a product's index-packed keys: 1: 10-bit digits (1024
+ * buckets; a 4096 x 4096 product of 20-qubit strings sorts its 40 varying
+ * bits in 4 passes instead of 5) when that saves a pass and the digit pass
+ * runs 12 or 16 keys per thread; 0 (default) or -1: 8-bit digits.  Results
+ * are identical either way. */
+#define PL_TUNE_RADIX_WIDE 8
 /* Polls a cross-CTA wait (decoupled look-back) makes before it records
  * PL_ERR_TIMEOUT and returns: 1 .. 2^30, 0 = the default 2^20 (with a 64 ns
  * back-off past 64 polls: well under a second).  Written into the device

@@ -31,6 +31,7 @@
 #include <algorithm>
 #include <cstdio>
 #include <cstring>
+#include <type_traits>
 #include <vector>
 
 #include "pl_collate.cuh"
@@ -538,7 +539,9 @@ bool pack_split_fast(const ProdSrc<AS>& src, u32, const KeyLayout& L, u32 count_
 // (src2, n2) into h2.
 // With pk set, each term's packed key is stored as well: lhs at pk[0, n),
 // rhs at pk[n, n + n2).
-template <int AS>
+// R: bins per pass (256, or 1024 for 10-bit digits); the histograms of pass
+// p are at [p * R, p * R + R).
+template <int AS, int R = kRadix>
 __global__ void __launch_bounds__(256) k_operand_hist(SoASrc<AS> src, u32 n, u32* h,
                                                       SoASrc<AS> src2, u32 n2, u32* h2,
                                                       KeyLayout L, PassPlan P, u32 conv_mask,
@@ -549,9 +552,9 @@ __global__ void __launch_bounds__(256) k_operand_hist(SoASrc<AS> src, u32 n, u32
         n = n2;
         h = h2;
     }
-    __shared__ u32 sh[8 * kRadix];
+    __shared__ u32 sh[(R == kRadix ? 8 : 4) * R];
     const int np0 = P.first[1] - P.first[0];
-    for (int i = threadIdx.x; i < np0 * kRadix; i += blockDim.x) sh[i] = 0;
+    for (int i = threadIdx.x; i < np0 * R; i += blockDim.x) sh[i] = 0;
     __syncthreads();
     for (u32 i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         u64 xw[AS], zw[AS];
@@ -561,39 +564,42 @@ __global__ void __launch_bounds__(256) k_operand_hist(SoASrc<AS> src, u32 n, u32
         if (pk) pk[i] = k0;
         for (int p = 0; p < np0; ++p)
             if ((conv_mask >> p) & 1u)
-                atomicAdd(&sh[p * kRadix + ((u32)(k0 >> P.shift[p]) & ((1u << P.bits[p]) - 1u))],
-                          1u);
+                atomicAdd(&sh[p * R + ((u32)(k0 >> P.shift[p]) & ((1u << P.bits[p]) - 1u))], 1u);
     }
     __syncthreads();
-    for (int i = threadIdx.x; i < np0 * kRadix; i += blockDim.x)
+    for (int i = threadIdx.x; i < np0 * R; i += blockDim.x)
         if (sh[i]) atomicAdd(&h[i], sh[i]);
 }
 
 __device__ __forceinline__ u32 block_excl_scan(u32 v, u32* s_warp, u32& total);
+template <int NW>
+__device__ __forceinline__ u32 block_scan_n(u32 v, u32* s_warp, u32& total);
 
 // hist[p][d] = sum_{d1} hA[p][d1] * hB[p][d1 ^ d] for every pass p in conv_mask
 // (both operand histograms staged in shared memory).  With scan = 1 every
 // pass's histogram is derived, and the block turns it into the pass's
 // bucket starts (exclusive prefix) right away, in place of k_scan_buckets.
-__global__ void __launch_bounds__(256) k_xor_conv(const u32* hA, const u32* hB, PassPlan P,
-                                                  u32 conv_mask, u32* hist, int scan) {
-    __shared__ u32 sa[kRadix], sb[kRadix], sw[kWarps];
+// NB: bins per pass (256, or 1024 for 10-bit digits), one thread per bin.
+template <int NB>
+__global__ void __launch_bounds__(NB) k_xor_conv(const u32* hA, const u32* hB, PassPlan P,
+                                                 u32 conv_mask, u32* hist, int scan) {
+    __shared__ u32 sa[NB], sb[NB], sw[65];
     const int p = blockIdx.x;
     if (!((conv_mask >> p) & 1u)) return;
     const u32 R = 1u << P.bits[p];
     const u32 d = threadIdx.x;
-    sa[d] = hA[p * kRadix + d];
-    sb[d] = hB[p * kRadix + d];
+    sa[d] = hA[p * NB + d];
+    sb[d] = hB[p * NB + d];
     __syncthreads();
     u32 acc = 0;
     if (d < R)
         for (u32 d1 = 0; d1 < R; ++d1) acc += sa[d1] * sb[d1 ^ d];
     if (!scan) {
-        if (d < R) hist[p * kRadix + d] = acc;
+        if (d < R) hist[p * NB + d] = acc;
         return;
     }
     u32 total;
-    hist[p * kRadix + d] = block_excl_scan(acc, sw, total);
+    hist[p * NB + d] = block_scan_n<NB / 32>(acc, sw, total);
 }
 
 // Chunk c >= 1: bring chunk c of every term into the current order and
@@ -758,7 +764,7 @@ __global__ void __launch_bounds__(kThreads, KONLY ? (ITEMS <= 12 ? 4 : 3)
                  u32* __restrict__ vout, u32 n, int shift, int bits,
                  const u32* __restrict__ bstart, u32* lb, u32* tile_ctr, int* status, Src src,
                  double* __restrict__ val_out, const uint2* __restrict__ phs, u64 imask,
-                 u32 pf_ahead, u32* lb_next) {
+                 u32 pf_ahead, u32* lb_next, int lbw) {
     extern __shared__ __align__(16) unsigned char dsm[];
     u64* skeys = reinterpret_cast<u64*>(dsm);
     u32* svals = reinterpret_cast<u32*>(dsm + sizeof(u64) * (kThreads * ITEMS));
@@ -840,7 +846,11 @@ __global__ void __launch_bounds__(kThreads, KONLY ? (ITEMS <= 12 ? 4 : 3)
             if constexpr (!KONLY) svals[pos] = vals[t];
         }
     }
-    const u32 excl = lb_walk<4>(lb + d, tile, kRadix, run, status);
+    // look-back window: predecessors read per L2 round trip
+    const u32 excl = lbw >= 16 ? lb_walk<16>(lb + d, tile, kRadix, run, status)
+                     : lbw >= 8 ? lb_walk<8>(lb + d, tile, kRadix, run, status)
+                     : lbw >= 4 ? lb_walk<4>(lb + d, tile, kRadix, run, status)
+                                : lb_walk<2>(lb + d, tile, kRadix, run, status);
     S.gofs[d] = bstart[d] + excl - bl;  // modulo 2^32; gofs[d] + p >= 0 for p >= bl
     __syncthreads();
     const u32 tile_n = min((u32)(kThreads * ITEMS), n - base);
@@ -928,6 +938,228 @@ __global__ void __launch_bounds__(kThreads, KONLY ? (ITEMS <= 12 ? 4 : 3)
 
 constexpr size_t radix_smem(int items) { return (sizeof(u64) + sizeof(u32)) * kThreads * items; }
 constexpr size_t radix_smem_konly(int items) { return sizeof(u64) * kThreads * items; }
+
+// ---------------------------------------------------------------------------
+// 3b. Digit pass with 10-bit digits over index-packed keys (1024 buckets):
+//     a product's 40 varying x / z bits sort in 4 passes instead of 5.  The
+//     same onesweep structure as k_radix_pass; each thread owns 4
+//     consecutive buckets (scan, look-back, offsets), the per-warp counts
+//     are 16-bit, and the four look-back walks run interleaved (all their
+//     window loads in flight at once).
+// ---------------------------------------------------------------------------
+constexpr int kRadixW = 1024;
+constexpr int kBpt = kRadixW / kThreads;  // buckets per thread
+
+struct RadixSmemW {
+    u16 whist[kWarps * kRadixW];  // per warp: digit counts, then tile positions
+    u32 gofs[kRadixW];
+    u32 swarp[kWarps];
+    u32 tile;
+};
+
+// Decoupled look-back for this thread's kBpt buckets (columns col, col + 1,
+// ...) at once; publishes each inclusive prefix and returns the exclusive
+// ones in excl.  Bounded like lb_walk.
+template <int W>
+__device__ __forceinline__ void lb_walk_w(u32* lb, u32 tile, u32 col, const u32 (&cnt)[kBpt],
+                                          u32 (&excl)[kBpt], int* status) {
+#pragma unroll
+    for (int b = 0; b < kBpt; ++b) excl[b] = 0;
+    if (tile == 0) return;
+    i64 t[kBpt];
+    bool done[kBpt];
+#pragma unroll
+    for (int b = 0; b < kBpt; ++b) {
+        t[b] = (i64)tile - 1;
+        done[b] = false;
+    }
+    u32 spins = 0;
+    for (;;) {
+        u32 w[kBpt][W];
+#pragma unroll
+        for (int b = 0; b < kBpt; ++b)
+#pragma unroll
+            for (int k = 0; k < W; ++k)
+                w[b][k] = (!done[b] && t[b] - k >= 0)
+                              ? ld_volatile(lb + (size_t)(t[b] - k) * kRadixW + col + b)
+                              : kFlagPre;
+        bool all = true, moved = false;
+#pragma unroll
+        for (int b = 0; b < kBpt; ++b) {
+            if (done[b]) continue;
+            int k = 0;
+            for (; k < W; ++k) {
+                const u32 fl = w[b][k] >> 30;
+                if (fl == 0) break;
+                excl[b] += w[b][k] & kCountMask;
+                if (fl == 2) {
+                    done[b] = true;
+                    break;
+                }
+            }
+            if (!done[b]) {
+                t[b] -= k;
+                all = false;
+                moved = moved || k > 0;
+            } else {
+                moved = true;
+            }
+        }
+        if (all) break;
+        if (!moved) {
+            if (++spins > g_spin_limit) {
+                raise_status(status, PL_ERR_TIMEOUT);
+                break;
+            }
+            if (spins > 64) __nanosleep(64);
+        }
+    }
+#pragma unroll
+    for (int b = 0; b < kBpt; ++b)
+        st_volatile(lb + (size_t)tile * kRadixW + col + b, kFlagPre | ((excl[b] + cnt[b]) & kCountMask));
+}
+
+template <class Src, bool LAST, int ITEMS>
+__global__ void __launch_bounds__(kThreads, ITEMS <= 12 ? 4 : 3)
+    k_radix_pass_w(const u64* __restrict__ kin, u64* __restrict__ kout, u32 n, int shift,
+                   int bits, const u32* __restrict__ bstart, u32* lb, u32* tile_ctr, int* status,
+                   Src src, double* __restrict__ val_out, const uint2* __restrict__ phs,
+                   u64 imask, u32 pf_ahead, u32* lb_next, int lbw) {
+    constexpr u32 kTile = (u32)(kThreads * ITEMS);
+    extern __shared__ __align__(16) unsigned char dsm[];
+    u64* skeys = reinterpret_cast<u64*>(dsm);
+    __shared__ __align__(16) RadixSmemW S;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    if (tid == 0) {
+        const u32 t = atomicAdd(tile_ctr, 1u);
+        S.tile = t;
+        const u32 pt = t + pf_ahead;
+        if (pf_ahead && (u64)(pt + 1) * kTile <= n)
+            prefetch_l2(kin + (size_t)pt * kTile, 8u * kTile);
+    }
+    // 16 KB of 16-bit counts: four 16-byte stores per thread
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+        reinterpret_cast<uint4*>(S.whist)[tid + i * kThreads] = make_uint4(0, 0, 0, 0);
+    __syncthreads();
+    const u32 tile = S.tile;
+    const u32 base = tile * kTile;
+    const u32 dmask = (1u << bits) - 1u;
+    const u32 col = (u32)tid * kBpt;  // this thread's first bucket
+    if (lb_next) {
+#pragma unroll
+        for (int b = 0; b < kBpt; ++b) lb_next[(size_t)tile * kRadixW + col + b] = 0u;
+    }
+    u64 keys[ITEMS];
+    u32 rank[(ITEMS + 1) / 2];
+    const u32 wbase = base + (u32)warp * (ITEMS * 32);
+#pragma unroll
+    for (int t = 0; t < ITEMS; ++t) {
+        const u32 idx = wbase + t * 32 + lane;
+        keys[t] = idx < n ? kin[idx] : 0ull;
+    }
+    u16* wh = S.whist + warp * kRadixW;
+#pragma unroll
+    for (int t = 0; t < ITEMS; ++t) {
+        const bool valid = (wbase + t * 32 + lane) < n;
+        const u32 d = valid ? ((u32)(keys[t] >> shift) & dmask) : kSentinel;
+        const u32 peers = __match_any_sync(0xffffffffu, d);
+        const int leader = __ffs(peers) - 1;
+        u32 before = 0;
+        if (valid && lane == leader) {
+            before = wh[d];
+            wh[d] = (u16)(before + __popc(peers));
+        }
+        before = __shfl_sync(0xffffffffu, before, leader);
+        const u32 r = before + __popc(peers & lanemask_lt());
+        rank[t / 2] = (t & 1) ? (rank[t / 2] | (r << 16)) : r;
+        __syncwarp();
+    }
+    __syncthreads();
+    // per bucket: exclusive prefix over warps; the thread's 4 buckets in a row
+    u32 run[kBpt], tot = 0;
+#pragma unroll
+    for (int b = 0; b < kBpt; ++b) {
+        u32 r = 0;
+#pragma unroll
+        for (int w = 0; w < kWarps; ++w) {
+            const u32 c = S.whist[w * kRadixW + col + b];
+            S.whist[w * kRadixW + col + b] = (u16)r;
+            r += c;
+        }
+        run[b] = r;
+        tot += r;
+    }
+    u32 total;
+    u32 bl[kBpt];
+    bl[0] = block_excl_scan(tot, S.swarp, total);
+#pragma unroll
+    for (int b = 1; b < kBpt; ++b) bl[b] = bl[b - 1] + run[b - 1];
+#pragma unroll
+    for (int b = 0; b < kBpt; ++b) {
+#pragma unroll
+        for (int w = 0; w < kWarps; ++w) S.whist[w * kRadixW + col + b] += (u16)bl[b];
+        lb_publish(lb + col + b, tile, kRadixW, run[b]);
+    }
+    __syncthreads();
+#pragma unroll
+    for (int t = 0; t < ITEMS; ++t) {
+        if (wbase + t * 32 + lane < n) {
+            const u32 dd = (u32)(keys[t] >> shift) & dmask;
+            const u32 pos = (u32)S.whist[warp * kRadixW + dd] +
+                            ((rank[t / 2] >> ((t & 1) * 16)) & 0xffffu);
+            skeys[pos] = keys[t];
+        }
+    }
+    u32 excl[kBpt];
+    if (lbw >= 8) lb_walk_w<8>(lb, tile, col, run, excl, status);
+    else if (lbw >= 4) lb_walk_w<4>(lb, tile, col, run, excl, status);
+    else lb_walk_w<2>(lb, tile, col, run, excl, status);
+#pragma unroll
+    for (int b = 0; b < kBpt; ++b) S.gofs[col + b] = bstart[col + b] + excl[b] - bl[b];
+    __syncthreads();
+    const u32 tile_n = min(kTile, n - base);
+    if constexpr (LAST) {
+        constexpr int kGather = 8;
+        for (u32 p0 = 0; p0 < tile_n; p0 += kGather * kThreads) {
+            u64 kk[kGather];
+            u32 gg[kGather], ph[kGather];
+            double vv[kGather];
+#pragma unroll
+            for (int q = 0; q < kGather; ++q) {
+                const u32 p = p0 + (u32)q * kThreads + tid;
+                gg[q] = 0xffffffffu;
+                kk[q] = 0;
+                ph[q] = 0;
+                vv[q] = 0.0;
+                if (p < tile_n) {
+                    const u64 k = skeys[p];
+                    const u32 idx = (u32)(k & imask);
+                    kk[q] = k;
+                    gg[q] = S.gofs[(u32)(k >> shift) & dmask] + p;
+                    if (idx < n) src.flags_value(idx, phs, ph[q], vv[q]);
+                    else gg[q] = n;  // reported below
+                }
+            }
+#pragma unroll
+            for (int q = 0; q < kGather; ++q) {
+                if (gg[q] < n) {
+                    kout[gg[q]] = (kk[q] & ~imask) | (u64)(ph[q] & 1u);
+                    val_out[gg[q]] = (ph[q] & 2u) ? -vv[q] : vv[q];
+                } else if (gg[q] != 0xffffffffu) {
+                    raise_status(status, PL_ERR_INTERNAL);
+                }
+            }
+        }
+        return;
+    }
+    for (u32 p = tid; p < tile_n; p += kThreads) {
+        const u64 k = skeys[p];
+        const u32 g = S.gofs[(u32)(k >> shift) & dmask] + p;
+        if (g >= n) raise_status(status, PL_ERR_INTERNAL);
+        else kout[g] = k;
+    }
+}
 
 
 
@@ -1430,18 +1662,35 @@ __device__ __forceinline__ u32 block_scan_n(u32 v, u32* s_warp, u32& total) {
 
 // Output offsets of the emit tiles (exclusive scan of the kept counts; one
 // CTA) and the output size.
+// Up to 16 counts per thread (16384 tiles) are loaded at once, before any
+// is added, so the scan waits for one round of loads instead of a chain.
 __global__ void __launch_bounds__(1024) k_tile_scan(const u32* tile_kept, u32 tiles,
                                                     u32* tile_off, i64* d_out_count) {
     __shared__ u32 sw[65];
     const u32 per = (tiles + 1023u) / 1024u;
     const u32 b = threadIdx.x * per, e = min(b + per, tiles);
-    u32 s = 0;
-    for (u32 i = b; i < e; ++i) s += tile_kept[i];
     u32 total;
-    u32 run = block_scan_n<32>(s, sw, total);
-    for (u32 i = b; i < e; ++i) {
-        tile_off[i] = run;
-        run += tile_kept[i];
+    if (per <= 16) {
+        u32 c[16];
+#pragma unroll
+        for (int k = 0; k < 16; ++k) c[k] = b + k < e ? tile_kept[b + k] : 0u;
+        u32 s = 0;
+#pragma unroll
+        for (int k = 0; k < 16; ++k) s += c[k];
+        u32 run = block_scan_n<32>(s, sw, total);
+#pragma unroll
+        for (int k = 0; k < 16; ++k) {
+            if (b + k < e) tile_off[b + k] = run;
+            run += c[k];
+        }
+    } else {
+        u32 s = 0;
+        for (u32 i = b; i < e; ++i) s += tile_kept[i];
+        u32 run = block_scan_n<32>(s, sw, total);
+        for (u32 i = b; i < e; ++i) {
+            tile_off[i] = run;
+            run += tile_kept[i];
+        }
     }
     if (threadIdx.x == 0) *d_out_count = (i64)total;
 }
@@ -1680,7 +1929,7 @@ inline size_t al(size_t b) { return (b + 255) & ~size_t(255); }
 // digit pass p; then the operand histograms of a product (kHistScratch,
 // 16 * kRadix words); the last word is the windowed-key check.
 constexpr int kHistScratch = 8 + kMaxPasses;
-constexpr int kCounterWords = kHistScratch + 16 * 256 + 8;
+constexpr int kCounterWords = kHistScratch + 16 * kRadixW + 8;
 
 // Bump allocator over the workspace; with base == nullptr it only measures.
 struct Carve {
@@ -1726,8 +1975,12 @@ void carve_all(Carve& c, i64 n, int nch, Bufs& B) {
     B.planes = c.take<u64>(nch > 1 ? (size_t)n * nch : 1);
     B.planes_bytes = sizeof(u64) * (nch > 1 ? (size_t)n * nch : 1);
     B.hist = c.take<u32>(kMaxPasses * kRadix);
-    B.lb = c.take<u32>((size_t)rtiles * kRadix);
-    B.lb2 = c.take<u32>((size_t)rtiles * kRadix);
+    // look-back words: 256 per tile of >= 2048 keys, or 1024 per tile of >= 3072
+    // keys (10-bit digits)
+    const size_t lbw = std::max<size_t>((size_t)rtiles * kRadix,
+                                        (size_t)((n + 3071) / 3072 + 1) * kRadixW);
+    B.lb = c.take<u32>(lbw);
+    B.lb2 = c.take<u32>(lbw);
     B.segflag = c.take<u8>(n + 16);
     B.seg_sum = c.take<double>(n);
     B.wfirst = c.take<u32>(ngw);
@@ -1806,7 +2059,7 @@ void build_layout(int as, int mode, const u64* orm, const u64* andm, KeyLayout& 
 // a stable sort by (x, z).  False when the word would exceed 64 bits or no
 // x / z bit varies.
 bool build_layout_split(int as, const u64* orm, const u64* andm, u32 n, KeyLayout& L,
-                        PassPlan& P, u64& imask) {
+                        PassPlan& P, u64& imask, int digit_max = 8) {
     const int nf = 2 * as + 1;
     std::memset(&L, 0, sizeof(L));
     std::memset(&P, 0, sizeof(P));
@@ -1831,7 +2084,7 @@ bool build_layout_split(int as, const u64* orm, const u64* andm, u32 n, KeyLayou
     L.total_bits = off;
     L.nchunks = 1;
     L.seg_mask0 = ~1ull;  // bit 0 carries the phase once the last pass has run
-    const int passes = (xz + 7) / 8;
+    const int passes = (xz + digit_max - 1) / digit_max;
     const int dw = (xz + passes - 1) / passes;
     int np = 0;
     for (int p = 0; p < passes; ++p) {
@@ -1872,13 +2125,13 @@ int fold_segments(const SegCtx& C, Bufs& B, const FoldFilter& F, int nsm, cudaSt
 // Histograms that can be derived instead of counted: none for a plain sum.
 template <int AS>
 u32 derive_histograms(const SoASrc<AS>&, const KeyLayout&, const PassPlan&, Bufs&, cudaStream_t,
-                      bool* scanned, u64* = nullptr) {
+                      bool* scanned, u64* = nullptr, int = kRadix) {
     *scanned = false;
     return 0u;
 }
 template <int AS>
 u32 derive_histograms(const WinSrc<AS>&, const KeyLayout&, const PassPlan&, Bufs&, cudaStream_t,
-                      bool* scanned, u64* = nullptr) {
+                      bool* scanned, u64* = nullptr, int = kRadix) {
     *scanned = false;
     return 0u;
 }
@@ -1888,7 +2141,7 @@ u32 derive_histograms(const WinSrc<AS>&, const KeyLayout&, const PassPlan&, Bufs
 // starts and *scanned is set (no k_scan_buckets needed).
 template <int AS>
 u32 derive_histograms(const ProdSrc<AS>& src, const KeyLayout& L, const PassPlan& P, Bufs& B,
-                      cudaStream_t st, bool* scanned, u64* opk = nullptr) {
+                      cudaStream_t st, bool* scanned, u64* opk = nullptr, int R = kRadix) {
     *scanned = false;
     const int np0 = P.first[1] - P.first[0];
     const int wf = L.width[2 * AS];  // the flags field occupies packed bits [0, wf)
@@ -1896,16 +2149,29 @@ u32 derive_histograms(const ProdSrc<AS>& src, const KeyLayout& L, const PassPlan
     for (int p = 0; p < np0; ++p)
         if (P.shift[p] >= wf) mask |= 1u << p;
     if (!mask) return 0u;
-    u32* hA = B.counters + kHistScratch;          // scratch after the pass counters
-    u32* hB = hA + 8 * kRadix;
-    if (fill32_async(hA, 0u, sizeof(u32) * 16 * kRadix, st) != cudaSuccess) return 0u;
+    // scratch after the pass counters: 8 passes x R bins per operand (R =
+    // 1024: at most 4 passes, 4 x R)
+    u32* hA = B.counters + kHistScratch;
+    u32* hB = hA + (R == kRadix ? 8 : 4) * R;
+    if (fill32_async(hA, 0u, sizeof(u32) * (R == kRadix ? 16 : 8) * R, st) != cudaSuccess)
+        return 0u;
     const SoASrc<AS> a{src.ax, src.az, src.af, src.av, src.sa};
     const SoASrc<AS> b{src.bx, src.bz, src.bf, src.bv, src.sb};
     const dim3 g(grid_for(std::max(src.n, src.m), 256, 64), 2);
-    k_operand_hist<AS><<<g, 256, 0, st>>>(a, src.n, hA, b, src.m, hB, L, P, mask, opk),
-        pl::note_launch();
     const bool all = np0 == P.npasses && mask == (1u << np0) - 1u;
-    k_xor_conv<<<np0, 256, 0, st>>>(hA, hB, P, mask, B.hist, all ? 1 : 0), pl::note_launch();
+    if (R == kRadixW) {
+        if (!all || np0 > 4) return 0u;  // 10-bit digits need every histogram derived
+        k_operand_hist<AS, kRadixW><<<g, 256, 0, st>>>(a, src.n, hA, b, src.m, hB, L, P, mask,
+                                                       opk),
+            pl::note_launch();
+        k_xor_conv<kRadixW><<<np0, kRadixW, 0, st>>>(hA, hB, P, mask, B.hist, 1),
+            pl::note_launch();
+    } else {
+        k_operand_hist<AS><<<g, 256, 0, st>>>(a, src.n, hA, b, src.m, hB, L, P, mask, opk),
+            pl::note_launch();
+        k_xor_conv<kRadix><<<np0, kRadix, 0, st>>>(hA, hB, P, mask, B.hist, all ? 1 : 0),
+            pl::note_launch();
+    }
     *scanned = all;
     return mask;
 }
@@ -1919,6 +2185,12 @@ bool operand_key_room(const Src&, u32) {
 template <int AS>
 bool operand_key_room(const ProdSrc<AS>& src, u32 n) {
     return (u64)src.n + src.m <= (u64)n;
+}
+
+// Look-back window of a digit pass (2, 4, 8 or 16; PL_TUNE_RADIX_WINDOW).
+int radix_window() {
+    const long long v = tuning(PL_TUNE_RADIX_WINDOW);
+    return v == 2 || v == 8 || v == 16 ? (int)v : 4;
 }
 
 // Keys per thread of a digit pass (8, 12 or 16; PL_TUNE_RADIX_ITEMS).
@@ -1967,18 +2239,50 @@ int radix_pass(bool last, const u64* kin, const u32* vin, u64* kout, u32* vout, 
         PL_CUDA_TRY(radix_attrs(k, (int)sm));
         k<<<tiles, kThreads, sm, st>>>(kin, vin, kout, vout, n, shift, bits, bstart, lb, ctr,
                                        B.d_status, src, B.sv, nullptr, 0ull,
-                                       prefetch_ahead(k, sm, occ_last), lb_next),
+                                       prefetch_ahead(k, sm, occ_last), lb_next, radix_window()),
             pl::note_launch();
     } else {
         auto* k = k_radix_pass<SoASrc<1>, false, ITEMS, false>;
         PL_CUDA_TRY(radix_attrs(k, (int)sm));
         k<<<tiles, kThreads, sm, st>>>(kin, vin, kout, vout, n, shift, bits, bstart, lb, ctr,
                                        B.d_status, nosrc, nullptr, nullptr, 0ull,
-                                       prefetch_ahead(k, sm, occ_mid), lb_next),
+                                       prefetch_ahead(k, sm, occ_mid), lb_next, radix_window()),
             pl::note_launch();
     }
     return PL_OK;
 }
+
+// 10-bit digit pass over index-packed keys (k_radix_pass_w).
+template <class Src, int ITEMS>
+int radix_pass_w(bool last, const u64* kin, u64* kout, u32 n, int shift, int bits,
+                 const u32* bstart, Bufs& B, u32* lb, u32* lb_next, u32* ctr, const Src& src,
+                 const uint2* phs, u64 imask, cudaStream_t st) {
+    const u32 tiles = (n + kThreads * ITEMS - 1) / (kThreads * ITEMS);
+    const size_t sm = radix_smem_konly(ITEMS);
+    static int occ_last = 0, occ_mid = 0;
+    if (last) {
+        auto* k = k_radix_pass_w<Src, true, ITEMS>;
+        PL_CUDA_TRY(radix_attrs(k, (int)sm));
+        k<<<tiles, kThreads, sm, st>>>(kin, kout, n, shift, bits, bstart, lb, ctr, B.d_status,
+                                       src, B.sv, phs, imask, prefetch_ahead(k, sm, occ_last),
+                                       lb_next, radix_window()),
+            pl::note_launch();
+    } else {
+        const SoASrc<1> nosrc{nullptr, nullptr, nullptr, nullptr, 0};
+        auto* k = k_radix_pass_w<SoASrc<1>, false, ITEMS>;
+        PL_CUDA_TRY(radix_attrs(k, (int)sm));
+        k<<<tiles, kThreads, sm, st>>>(kin, kout, n, shift, bits, bstart, lb, ctr, B.d_status,
+                                       nosrc, nullptr, nullptr, imask,
+                                       prefetch_ahead(k, sm, occ_mid), lb_next, radix_window()),
+            pl::note_launch();
+    }
+    return PL_OK;
+}
+
+template <class S>
+struct IsProd : std::false_type {};
+template <int AS>
+struct IsProd<ProdSrc<AS>> : std::true_type {};
 
 // Digit pass over index-packed keys (no payload).
 template <class Src, int ITEMS>
@@ -1993,7 +2297,7 @@ int radix_pass_konly(bool last, const u64* kin, u64* kout, u32 n, int shift, int
         PL_CUDA_TRY(radix_attrs(k, (int)sm));
         k<<<tiles, kThreads, sm, st>>>(kin, nullptr, kout, nullptr, n, shift, bits, bstart, lb,
                                        ctr, B.d_status, src, B.sv, phs, imask,
-                                       prefetch_ahead(k, sm, occ_last), lb_next),
+                                       prefetch_ahead(k, sm, occ_last), lb_next, radix_window()),
             pl::note_launch();
     } else {
         const SoASrc<1> nosrc{nullptr, nullptr, nullptr, nullptr, 0};
@@ -2001,7 +2305,7 @@ int radix_pass_konly(bool last, const u64* kin, u64* kout, u32 n, int shift, int
         PL_CUDA_TRY(radix_attrs(k, (int)sm));
         k<<<tiles, kThreads, sm, st>>>(kin, nullptr, kout, nullptr, n, shift, bits, bstart, lb,
                                        ctr, B.d_status, nosrc, nullptr, nullptr, imask,
-                                       prefetch_ahead(k, sm, occ_mid), lb_next),
+                                       prefetch_ahead(k, sm, occ_mid), lb_next, radix_window()),
             pl::note_launch();
     }
     return PL_OK;
@@ -2114,12 +2418,14 @@ int run_collate(const Src& src, u32 n, int mode, const KeyLayout& L, const PassP
 
 // canonicalize() on index-packed keys (layout from build_layout_split;
 // filters: zero and cutoff, no weight filter).
+// wide: 10-bit digits (a product at >= 12 keys per thread; try_split decides).
 template <int AS, class Src>
 int run_collate_split(const Src& src, u32 n, const KeyLayout& L, const PassPlan& P, u64 imask,
                       const CollateArgs& a, const SoAOut& out, i64* out_count, Bufs& B,
-                      cudaStream_t st) {
+                      cudaStream_t st, bool wide = false) {
     const int items = radix_items();
     const u32 rtiles = (n + kThreads * items - 1) / (kThreads * items);
+    const int R = wide ? kRadixW : kRadix;
     const int nsm = sm_count();
     // the chunk-plane buffer is unused with one chunk: phase / sign bit planes,
     // then the (phase-0, phase-1) sums of the segments
@@ -2127,11 +2433,11 @@ int run_collate_split(const Src& src, u32 n, const KeyLayout& L, const PassPlan&
     double2* seg2 = reinterpret_cast<double2*>(reinterpret_cast<unsigned char*>(B.planes) + al(n));
     // the look-back words of the first digit pass; every pass clears the
     // next one's
-    const FillReq fr[5] = {{B.hist, 0u, sizeof(u32) * (size_t)std::max(P.npasses, 1) * kRadix},
+    const FillReq fr[5] = {{B.hist, 0u, sizeof(u32) * (size_t)std::max(P.npasses, 1) * R},
                            {B.counters, 0u, sizeof(u32) * (size_t)(P.npasses + 8)},
                            {B.d_status, 0u, sizeof(int)},
                            {B.d_count, 0u, sizeof(i64)},
-                           {B.lb, 0u, sizeof(u32) * (size_t)rtiles * kRadix}};
+                           {B.lb, 0u, sizeof(u32) * (size_t)rtiles * R}};
     PL_CUDA_TRY(fill32_multi(fr, 5, st));
     const int gblocks = grid_for(n, 256, nsm * 8);
     cudaEvent_t e0 = timed_begin(st);
@@ -2139,7 +2445,8 @@ int run_collate_split(const Src& src, u32 n, const KeyLayout& L, const PassPlan&
     // a product's operand packed keys go to B.sv, unused until the last
     // digit pass writes the sorted coefficients there
     u64* opk = operand_key_room(src, n) ? reinterpret_cast<u64*>(B.sv) : nullptr;
-    const u32 derived = derive_histograms<AS>(src, L, P, B, st, &scanned, opk);
+    const u32 derived = derive_histograms<AS>(src, L, P, B, st, &scanned, opk, R);
+    if (wide && !scanned) return record_status(PL_ERR_INTERNAL, "collate: 10-bit digit plan");
     timed_end(e0, st, "k_xor_conv", 0ull);
     const u32 count_mask = ~derived & ((1u << P.npasses) - 1u);
     if (!derived) opk = nullptr;  // not written
@@ -2153,12 +2460,23 @@ int run_collate_split(const Src& src, u32 n, const KeyLayout& L, const PassPlan&
     for (int p = 0; p < P.npasses; ++p) {
         cudaEvent_t ev0 = timed_begin(st);
         const bool last = (p == P.npasses - 1);
-        const u32* bs = B.hist + (size_t)p * kRadix;
+        const u32* bs = B.hist + (size_t)p * R;
         u32* ctr = B.counters + 8 + p;
         u32* lb = (p & 1) ? B.lb2 : B.lb;
         u32* lbn = (p & 1) ? B.lb : B.lb2;
         int rc = PL_OK;
-        if (items == 16)
+        if (wide) {
+            if constexpr (IsProd<Src>::value) {
+                if (items == 16)
+                    rc = radix_pass_w<Src, 16>(last, kin, kout, n, P.shift[p], P.bits[p], bs, B,
+                                               lb, lbn, ctr, src, phs, imask, st);
+                else
+                    rc = radix_pass_w<Src, 12>(last, kin, kout, n, P.shift[p], P.bits[p], bs, B,
+                                               lb, lbn, ctr, src, phs, imask, st);
+            } else {
+                rc = record_status(PL_ERR_INTERNAL, "collate: 10-bit digits without a product");
+            }
+        } else if (items == 16)
             rc = radix_pass_konly<Src, 16>(last, kin, kout, n, P.shift[p], P.bits[p], bs, B, lb,
                                            lbn, ctr, src, phs, imask, st);
         else if (items == 12)
@@ -2209,6 +2527,18 @@ bool try_split(const Src& src, u32 n, const u64* orm, const u64* andm, const Col
     PassPlan P;
     u64 imask = 0;
     if (!build_layout_split(AS, orm, andm, n, L, P, imask)) return false;
+    // a product (every histogram derived) sorts 10-bit digits where that saves
+    // a pass (PL_TUNE_RADIX_WIDE; tiles of >= 12 keys per thread)
+    if (IsProd<Src>::value && tuning(PL_TUNE_RADIX_WIDE) > 0 && radix_items() >= 12) {
+        KeyLayout Lw;
+        PassPlan Pw;
+        u64 iw = 0;
+        if (build_layout_split(AS, orm, andm, n, Lw, Pw, iw, 10) && Pw.npasses < P.npasses &&
+            Pw.npasses <= 4) {
+            *rc = run_collate_split<AS>(src, n, Lw, Pw, iw, a, out, out_count, B, st, true);
+            return true;
+        }
+    }
     *rc = run_collate_split<AS>(src, n, L, P, imask, a, out, out_count, B, st);
     return true;
 }

@@ -187,7 +187,7 @@ static void keep_pool_cached() {
     cudaGetLastError();
     done[dev] = true;
 }
-static std::atomic<long long> g_tuning[8] = {};
+static std::atomic<long long> g_tuning[16] = {};
 
 // PL_TUNE_FAIL_ALLOC: the k-th allocation from now fails (then the
 // injection is spent).
@@ -215,7 +215,7 @@ void dev_free(void* p, cudaStream_t st) {
 void capture_lock() { g_alloc_mu.lock(); }
 void capture_unlock() { g_alloc_mu.unlock(); }
 
-long long tuning(int key) { return key >= 0 && key < 8 ? g_tuning[key].load() : 0; }
+long long tuning(int key) { return key >= 0 && key < 16 ? g_tuning[key].load() : 0; }
 
 void note_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
 void note_launches(unsigned long long n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
@@ -373,6 +373,11 @@ extern "C" int pl_set_tuning(int key, int64_t value) {
         pl::g_tuning[key].store(value);
         return pl::record_status(PL_OK, nullptr);
     }
+    if (key == PL_TUNE_RADIX_WINDOW &&
+        (value == 0 || value == 2 || value == 4 || value == 8 || value == 16)) {
+        pl::g_tuning[key].store(value);
+        return pl::record_status(PL_OK, nullptr);
+    }
     if (key == PL_TUNE_RADIX_ITEMS && (value == 0 || value == 8 || value == 12 || value == 16)) {
         pl::g_tuning[key].store(value);
         return pl::record_status(PL_OK, nullptr);
@@ -381,7 +386,7 @@ extern "C" int pl_set_tuning(int key, int64_t value) {
         pl::g_tuning[key].store(value);
         return pl::record_status(PL_OK, nullptr);
     }
-    if ((key == PL_TUNE_INDEX_KEYS || key == PL_TUNE_WINDOW_KEYS) &&
+    if ((key == PL_TUNE_INDEX_KEYS || key == PL_TUNE_WINDOW_KEYS || key == PL_TUNE_RADIX_WIDE) &&
         (value == 0 || value == 1 || value == -1)) {
         pl::g_tuning[key].store(value);
         return pl::record_status(PL_OK, nullptr);
@@ -390,7 +395,7 @@ extern "C" int pl_set_tuning(int key, int64_t value) {
 }
 
 extern "C" int pl_get_tuning(int key, int64_t* value) {
-    if (!value || key < 1 || key >= 8) return pl::record_status(PL_ERR_INVALID_ARG, "pl_get_tuning");
+    if (!value || key < 1 || key >= 16) return pl::record_status(PL_ERR_INVALID_ARG, "pl_get_tuning");
     *value = pl::g_tuning[key].load();
     return pl::record_status(PL_OK, nullptr);
 }

@@ -191,3 +191,49 @@ def test_l2_prefetch_digit_pass_product(cuda, items):
         with tuned(_abi.PL_TUNE_RADIX_PREFETCH, -1):
             off = gpu_multiply_collate(a, b)
     assert on.n > 0 and _bits_equal(on, off)
+
+
+@pytest.mark.parametrize("window", [2, 8, 16])
+@pytest.mark.parametrize("n,nq,seed", [(3, 5, 51), (4097, 12, 52), (300001, 12, 53)])
+def test_lookback_window(cuda, window, n, nq, seed):
+    # every look-back window gives the same result as the default of 4
+    p = random_sum(n, 1, seed, nq, "normal")
+    with tuned(_abi.PL_TUNE_RADIX_WINDOW, window):
+        on = gpu_collate(p, CANON)
+        again = gpu_collate(p, CANON)
+    off = gpu_collate(p, CANON)
+    assert _bits_equal(on, off) and _bits_equal(on, again)
+
+
+@pytest.mark.parametrize("items", [12, 16])
+@pytest.mark.parametrize("terms,seed", [(4096, 0), (1024, 5), (2048, 7)])
+def test_ten_bit_digits_product(cuda, oracle, items, terms, seed):
+    # A product's index-packed keys sorted with 10-bit digits (1024 buckets,
+    # 4 passes for 40 varying bits instead of 5) against 8-bit digits:
+    # bit-identical; the smaller cases also against the oracle.
+    a, b = W.product_operands(seed=seed, terms=terms)
+    a, b = as_planes(a), as_planes(b)
+    with tuned(_abi.PL_TUNE_RADIX_ITEMS, items):
+        with tuned(_abi.PL_TUNE_RADIX_WIDE, 1):
+            on = gpu_multiply_collate(a, b)
+            again = gpu_multiply_collate(a, b)
+        with tuned(_abi.PL_TUNE_RADIX_WIDE, -1):
+            off = gpu_multiply_collate(a, b)
+    assert on.n > 0 and _bits_equal(on, off) and _bits_equal(on, again)
+    if terms <= 1024:
+        prod = oracle.multiply(a, b)
+        o = oracle.canonicalize(prod)
+        assert_keys_equal(on, o)
+        assert_values_close(on, o, abs_scale(oracle, prod))
+
+
+@pytest.mark.parametrize("window", [2, 4, 8])
+def test_ten_bit_digits_lookback_window(cuda, window):
+    a, b = W.product_operands(seed=3, terms=2048)
+    a, b = as_planes(a), as_planes(b)
+    with tuned(_abi.PL_TUNE_RADIX_ITEMS, 12), tuned(_abi.PL_TUNE_RADIX_WINDOW, window):
+        with tuned(_abi.PL_TUNE_RADIX_WIDE, 1):
+            on = gpu_multiply_collate(a, b)
+        with tuned(_abi.PL_TUNE_RADIX_WIDE, -1):
+            off = gpu_multiply_collate(a, b)
+    assert _bits_equal(on, off)
