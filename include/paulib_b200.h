@@ -445,8 +445,9 @@ PL_API int pl_serve(const pl_job* jobs, int64_t count, const pl_batch_opts* opts
 
 /* ---- tuning ------------------------------------------------------------- */
 
-/* Keys per thread of the collate engine's onesweep digit pass: 8 (default),
- * 12 or 16 (tiles of 2048, 3072 or 4096 keys).  Process-wide. */
+/* Keys per thread of the collate engine's onesweep digit pass: 8, 12 or 16
+ * (tiles of 2048, 3072 or 4096 keys); 0 (default): 12 for index-packed
+ * keys, 8 for key + payload passes.  Process-wide. */
 #define PL_TUNE_RADIX_ITEMS 1
 /* canonicalize() of a sum (or of a product) whose varying x / z bits and
  * term index fit one 64-bit word sorts index-packed keys: 8 bytes per key
@@ -468,8 +469,9 @@ PL_API int pl_serve(const pl_job* jobs, int64_t count, const pl_batch_opts* opts
  * are identical either way. */
 #define PL_TUNE_RADIX_PREFETCH 6
 /* Look-back window of the digit passes: predecessor tiles read per round
- * trip while a tile waits for its global bucket offsets: 2, 4 (default), 8
- * or 16.  Results are identical either way. */
+ * trip while a tile waits for its global bucket offsets: 2, 4, 8 or 16; 0
+ * (default): 8 for index-packed keys, 4 for key + payload passes.  Results
+ * are identical either way. */
 #define PL_TUNE_RADIX_WINDOW 7
 /* Digit width of a product's index-packed keys: 1: 10-bit digits (1024
  * buckets; a 4096 x 4096 product of 20-qubit strings sorts its 40 varying

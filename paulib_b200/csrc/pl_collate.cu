@@ -2188,15 +2188,21 @@ bool operand_key_room(const ProdSrc<AS>& src, u32 n) {
 }
 
 // Look-back window of a digit pass (2, 4, 8 or 16; PL_TUNE_RADIX_WINDOW).
-int radix_window() {
+// Unset: 8 for index-packed keys (measured best on the product workload), 4
+// for key + payload passes.
+int radix_window(bool konly = false) {
     const long long v = tuning(PL_TUNE_RADIX_WINDOW);
-    return v == 2 || v == 8 || v == 16 ? (int)v : 4;
+    if (v == 2 || v == 4 || v == 8 || v == 16) return (int)v;
+    return konly ? 8 : 4;
 }
 
-// Keys per thread of a digit pass (8, 12 or 16; PL_TUNE_RADIX_ITEMS).
-int radix_items() {
+// Keys per thread of a digit pass (8, 12 or 16; PL_TUNE_RADIX_ITEMS).  Unset:
+// 12 for index-packed keys (measured best on the product workload), 8 for
+// key + payload passes (their 12 extra bytes of shared memory per key).
+int radix_items(bool konly = false) {
     const long long v = tuning(PL_TUNE_RADIX_ITEMS);
-    return v == 12 || v == 16 ? (int)v : 8;
+    if (v == 8 || v == 12 || v == 16) return (int)v;
+    return konly ? 12 : 8;
 }
 
 // Dynamic shared memory of a digit pass.  (The default carveout is kept:
@@ -2265,7 +2271,7 @@ int radix_pass_w(bool last, const u64* kin, u64* kout, u32 n, int shift, int bit
         PL_CUDA_TRY(radix_attrs(k, (int)sm));
         k<<<tiles, kThreads, sm, st>>>(kin, kout, n, shift, bits, bstart, lb, ctr, B.d_status,
                                        src, B.sv, phs, imask, prefetch_ahead(k, sm, occ_last),
-                                       lb_next, radix_window()),
+                                       lb_next, radix_window(true)),
             pl::note_launch();
     } else {
         const SoASrc<1> nosrc{nullptr, nullptr, nullptr, nullptr, 0};
@@ -2273,7 +2279,7 @@ int radix_pass_w(bool last, const u64* kin, u64* kout, u32 n, int shift, int bit
         PL_CUDA_TRY(radix_attrs(k, (int)sm));
         k<<<tiles, kThreads, sm, st>>>(kin, kout, n, shift, bits, bstart, lb, ctr, B.d_status,
                                        nosrc, nullptr, nullptr, imask,
-                                       prefetch_ahead(k, sm, occ_mid), lb_next, radix_window()),
+                                       prefetch_ahead(k, sm, occ_mid), lb_next, radix_window(true)),
             pl::note_launch();
     }
     return PL_OK;
@@ -2297,7 +2303,7 @@ int radix_pass_konly(bool last, const u64* kin, u64* kout, u32 n, int shift, int
         PL_CUDA_TRY(radix_attrs(k, (int)sm));
         k<<<tiles, kThreads, sm, st>>>(kin, nullptr, kout, nullptr, n, shift, bits, bstart, lb,
                                        ctr, B.d_status, src, B.sv, phs, imask,
-                                       prefetch_ahead(k, sm, occ_last), lb_next, radix_window()),
+                                       prefetch_ahead(k, sm, occ_last), lb_next, radix_window(true)),
             pl::note_launch();
     } else {
         const SoASrc<1> nosrc{nullptr, nullptr, nullptr, nullptr, 0};
@@ -2305,7 +2311,7 @@ int radix_pass_konly(bool last, const u64* kin, u64* kout, u32 n, int shift, int
         PL_CUDA_TRY(radix_attrs(k, (int)sm));
         k<<<tiles, kThreads, sm, st>>>(kin, nullptr, kout, nullptr, n, shift, bits, bstart, lb,
                                        ctr, B.d_status, nosrc, nullptr, nullptr, imask,
-                                       prefetch_ahead(k, sm, occ_mid), lb_next, radix_window()),
+                                       prefetch_ahead(k, sm, occ_mid), lb_next, radix_window(true)),
             pl::note_launch();
     }
     return PL_OK;
@@ -2423,7 +2429,7 @@ template <int AS, class Src>
 int run_collate_split(const Src& src, u32 n, const KeyLayout& L, const PassPlan& P, u64 imask,
                       const CollateArgs& a, const SoAOut& out, i64* out_count, Bufs& B,
                       cudaStream_t st, bool wide = false) {
-    const int items = radix_items();
+    const int items = radix_items(true);
     const u32 rtiles = (n + kThreads * items - 1) / (kThreads * items);
     const int R = wide ? kRadixW : kRadix;
     const int nsm = sm_count();
@@ -2529,7 +2535,7 @@ bool try_split(const Src& src, u32 n, const u64* orm, const u64* andm, const Col
     if (!build_layout_split(AS, orm, andm, n, L, P, imask)) return false;
     // a product (every histogram derived) sorts 10-bit digits where that saves
     // a pass (PL_TUNE_RADIX_WIDE; tiles of >= 12 keys per thread)
-    if (IsProd<Src>::value && tuning(PL_TUNE_RADIX_WIDE) > 0 && radix_items() >= 12) {
+    if (IsProd<Src>::value && tuning(PL_TUNE_RADIX_WIDE) > 0 && radix_items(true) >= 12) {
         KeyLayout Lw;
         PassPlan Pw;
         u64 iw = 0;
