@@ -479,6 +479,12 @@ PL_API int pl_serve(const pl_job* jobs, int64_t count, const pl_batch_opts* opts
  * runs 12 or 16 keys per thread; 0 (default) or -1: 8-bit digits.  Results
  * are identical either way. */
 #define PL_TUNE_RADIX_WIDE 8
+/* Polls a digit-pass tile makes without progress while it waits for its
+ * predecessors' look-back words before each further poll sleeps 64 ns: 1 ..
+ * 1024; 0 (default): 16 for index-packed keys, 64 for key + payload passes.  A spinning thread takes issue slots from the
+ * warps of other tiles that rank and scatter.  Results are identical either
+ * way. */
+#define PL_TUNE_RADIX_BACKOFF 9
 /* Polls a cross-CTA wait (decoupled look-back) makes before it records
  * PL_ERR_TIMEOUT and returns: 1 .. 2^30, 0 = the default 2^20 (with a 64 ns
  * back-off past 64 polls: well under a second).  Written into the device

@@ -688,8 +688,11 @@ __device__ __forceinline__ void lb_publish(u32* lb, u32 tile, u32 stride, u32 cn
     st_volatile(lb + (size_t)tile * stride, (tile == 0 ? kFlagPre : kFlagAgg) | cnt);
 }
 
+// hot: polls without progress before each further poll sleeps 64 ns (a
+// spinning thread takes issue slots from the warps that do work).
 template <int W = 4>
-__device__ __forceinline__ u32 lb_walk(u32* lb, u32 tile, u32 stride, u32 cnt, int* status) {
+__device__ __forceinline__ u32 lb_walk(u32* lb, u32 tile, u32 stride, u32 cnt, int* status,
+                                       u32 hot = 64) {
     if (tile == 0) return 0;
     u32* mine = lb + (size_t)tile * stride;
     u32 excl = 0;
@@ -718,7 +721,7 @@ __device__ __forceinline__ u32 lb_walk(u32* lb, u32 tile, u32 stride, u32 cnt, i
                 raise_status(status, PL_ERR_TIMEOUT);
                 break;
             }
-            if (spins > 64) __nanosleep(64);
+            if (spins > hot) __nanosleep(64);
         }
     }
     st_volatile(mine, kFlagPre | ((excl + cnt) & kCountMask));
@@ -846,11 +849,14 @@ __global__ void __launch_bounds__(kThreads, KONLY ? (ITEMS <= 12 ? 4 : 3)
             if constexpr (!KONLY) svals[pos] = vals[t];
         }
     }
-    // look-back window: predecessors read per L2 round trip
-    const u32 excl = lbw >= 16 ? lb_walk<16>(lb + d, tile, kRadix, run, status)
-                     : lbw >= 8 ? lb_walk<8>(lb + d, tile, kRadix, run, status)
-                     : lbw >= 4 ? lb_walk<4>(lb + d, tile, kRadix, run, status)
-                                : lb_walk<2>(lb + d, tile, kRadix, run, status);
+    // look-back window (predecessors read per L2 round trip) in the low 8
+    // bits of lbw, hot polls before backing off above them
+    const int win = lbw & 0xff;
+    const u32 hot = (u32)lbw >> 8;
+    const u32 excl = win >= 16 ? lb_walk<16>(lb + d, tile, kRadix, run, status, hot)
+                     : win >= 8 ? lb_walk<8>(lb + d, tile, kRadix, run, status, hot)
+                     : win >= 4 ? lb_walk<4>(lb + d, tile, kRadix, run, status, hot)
+                                : lb_walk<2>(lb + d, tile, kRadix, run, status, hot);
     S.gofs[d] = bstart[d] + excl - bl;  // modulo 2^32; gofs[d] + p >= 0 for p >= bl
     __syncthreads();
     const u32 tile_n = min((u32)(kThreads * ITEMS), n - base);
@@ -1112,8 +1118,8 @@ __global__ void __launch_bounds__(kThreads, ITEMS <= 12 ? 4 : 3)
         }
     }
     u32 excl[kBpt];
-    if (lbw >= 8) lb_walk_w<8>(lb, tile, col, run, excl, status);
-    else if (lbw >= 4) lb_walk_w<4>(lb, tile, col, run, excl, status);
+    if ((lbw & 0xff) >= 8) lb_walk_w<8>(lb, tile, col, run, excl, status);
+    else if ((lbw & 0xff) >= 4) lb_walk_w<4>(lb, tile, col, run, excl, status);
     else lb_walk_w<2>(lb, tile, col, run, excl, status);
 #pragma unroll
     for (int b = 0; b < kBpt; ++b) S.gofs[col + b] = bstart[col + b] + excl[b] - bl[b];
@@ -2189,11 +2195,15 @@ bool operand_key_room(const ProdSrc<AS>& src, u32 n) {
 
 // Look-back window of a digit pass (2, 4, 8 or 16; PL_TUNE_RADIX_WINDOW).
 // Unset: 8 for index-packed keys (measured best on the product workload), 4
-// for key + payload passes.
+// for key + payload passes.  Returned with the hot polls before a waiting
+// thread backs off (PL_TUNE_RADIX_BACKOFF; unset 16 for index-packed keys,
+// 64 otherwise) in the bits above 8.
 int radix_window(bool konly = false) {
     const long long v = tuning(PL_TUNE_RADIX_WINDOW);
-    if (v == 2 || v == 4 || v == 8 || v == 16) return (int)v;
-    return konly ? 8 : 4;
+    const int w = (v == 2 || v == 4 || v == 8 || v == 16) ? (int)v : (konly ? 8 : 4);
+    const long long b = tuning(PL_TUNE_RADIX_BACKOFF);
+    const int hot = (b >= 1 && b <= 1024) ? (int)b : (konly ? 16 : 64);
+    return w | (hot << 8);
 }
 
 // Keys per thread of a digit pass (8, 12 or 16; PL_TUNE_RADIX_ITEMS).  Unset:

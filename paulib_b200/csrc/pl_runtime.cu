@@ -373,6 +373,10 @@ extern "C" int pl_set_tuning(int key, int64_t value) {
         pl::g_tuning[key].store(value);
         return pl::record_status(PL_OK, nullptr);
     }
+    if (key == PL_TUNE_RADIX_BACKOFF && value >= 0 && value <= 1024) {
+        pl::g_tuning[key].store(value);
+        return pl::record_status(PL_OK, nullptr);
+    }
     if (key == PL_TUNE_RADIX_WINDOW &&
         (value == 0 || value == 2 || value == 4 || value == 8 || value == 16)) {
         pl::g_tuning[key].store(value);

@@ -237,3 +237,14 @@ def test_ten_bit_digits_lookback_window(cuda, window):
         with tuned(_abi.PL_TUNE_RADIX_WIDE, -1):
             off = gpu_multiply_collate(a, b)
     assert _bits_equal(on, off)
+
+
+@pytest.mark.parametrize("backoff", [1, 4, 1024])
+def test_lookback_backoff(cuda, backoff):
+    # how soon a waiting tile backs off changes nothing in the result
+    a, b = W.product_operands(seed=9, terms=2048)
+    a, b = as_planes(a), as_planes(b)
+    with tuned(_abi.PL_TUNE_RADIX_BACKOFF, backoff):
+        on = gpu_multiply_collate(a, b)
+    off = gpu_multiply_collate(a, b)
+    assert _bits_equal(on, off)
