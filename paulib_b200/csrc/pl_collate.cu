@@ -1334,7 +1334,14 @@ __global__ void __launch_bounds__(32 * kFoldWarps, 6)
     if (w0 >= C.n) return;
     const u32 w1 = min(w0 + kFoldSpan, C.n);
     const u32 cnt = w1 - w0;
-
+    if (lane == 0 && (C.n - w0) >= kFoldSpan + kLook) {
+        // the whole range and its lookahead go to L2 at once, so the staging
+        // batches after the first find them there instead of each waiting on
+        // DRAM in turn
+        prefetch_l2(C.keys + w0, 8u * (kFoldSpan + kLook));
+        prefetch_l2(C.vals + w0, 8u * (kFoldSpan + kLook));
+        if (MODE != kCanonSplit && C.pay) prefetch_l2(C.pay + w0, 4u * (kFoldSpan + kLook));
+    }
     unsigned char* base = fsm + ((kFoldWarpSmem + 15) & ~size_t(15)) * warp;
     double* sv = reinterpret_cast<double*>(base);
     u32* hbw = reinterpret_cast<u32*>(base + 8 * kFoldSlots);
@@ -1769,6 +1776,11 @@ __global__ void __launch_bounds__(kThreads)
     const u32 nh = rng_heads[g];
     const u32 w0 = g * kFoldSpan;
     i64 o = rng_off[g];
+    if (lane == 0 && nh > 32 * kRecBatch) {
+        // the range's later record batches go to L2 now (whole 16-byte units)
+        prefetch_l2(rkey + w0, 8u * (nh & ~1u));
+        prefetch_l2(rs + w0, 16u * nh);
+    }
     for (u32 k0 = 0; k0 < nh; k0 += 32 * kRecBatch) {
         u64 key[kRecBatch];
         double2 v[kRecBatch];
