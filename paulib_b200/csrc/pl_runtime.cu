@@ -12,6 +12,7 @@
 #include <cstdio>
 #include <mutex>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "pl_collate.cuh"
@@ -60,14 +61,22 @@ struct ReadArgs {
     unsigned int words[kMaxReads];
     int n;
 };
-__global__ void __launch_bounds__(32) k_readback(ReadArgs a, unsigned int* dst) {
+// Copies the requested words into the mapped host buffer, then -- after
+// every lane's writes are visible system-wide -- writes the call's sequence
+// number into the buffer's token word, which the host polls.
+__global__ void __launch_bounds__(32) k_readback(ReadArgs a, unsigned int* dst,
+                                                 unsigned int* token, unsigned int seq) {
     for (int r = 0; r < a.n; ++r)
         for (unsigned int i = threadIdx.x; i < a.words[r]; i += 32) dst[a.dst_off[r] + i] = a.src[r][i];
+    __threadfence_system();
+    __syncwarp();
+    if (threadIdx.x == 0) *reinterpret_cast<volatile unsigned int*>(token) = seq;
 }
 struct PinnedBuf {
     void* host = nullptr;
     unsigned int* dev = nullptr;
-    size_t bytes = 0;
+    size_t bytes = 0;    // data bytes; the token word follows them
+    unsigned int seq = 0;
     ~PinnedBuf() {
         if (host) cudaFreeHost(host);
     }
@@ -140,21 +149,49 @@ cudaError_t readback_sync(const ReadReq* reqs, int n, cudaStream_t st) {
         if (b.host) cudaFreeHost(b.host);
         b.host = nullptr;
         b.bytes = 0;
-        const size_t want = total < 4096 ? 4096 : total;
-        cudaError_t e = cudaHostAlloc(&b.host, want, cudaHostAllocMapped | cudaHostAllocPortable);
+        const size_t want = total < 4096 ? 4096 : (total + 63) & ~size_t(63);
+        cudaError_t e =
+            cudaHostAlloc(&b.host, want + 64, cudaHostAllocMapped | cudaHostAllocPortable);
         if (e != cudaSuccess) return e;
         void* d = nullptr;
         e = cudaHostGetDevicePointer(&d, b.host, 0);
         if (e != cudaSuccess) return e;
         b.dev = static_cast<unsigned int*>(d);
         b.bytes = want;
+        *reinterpret_cast<volatile unsigned int*>(static_cast<unsigned char*>(b.host) + want) = 0;
+        b.seq = 0;
     }
-    k_readback<<<1, 32, 0, st>>>(a, b.dev);
+    const unsigned int seq = ++b.seq == 0 ? ++b.seq : b.seq;  // never 0 (the initial value)
+    unsigned int* dtok = b.dev + b.bytes / 4;
+    k_readback<<<1, 32, 0, st>>>(a, b.dev, dtok, seq);
     note_launch();
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
-    e = cudaStreamSynchronize(st);
-    if (e != cudaSuccess) return e;
+    // Wait for the token instead of synchronising the stream: the read-back
+    // runs after all earlier work of the stream, so its token means that work
+    // is done too.  A poll of host memory needs no driver call; the stream is
+    // queried now and then, for errors and in case the token write is not
+    // yet visible, and the thread yields once the wait gets long, leaving the
+    // core to threads that launch work.
+    const volatile unsigned int* htok = reinterpret_cast<const volatile unsigned int*>(
+        static_cast<const unsigned char*>(b.host) + b.bytes);
+    for (unsigned long long i = 1; *htok != seq; ++i) {
+        if ((i & 1023u) == 0) {
+            e = cudaStreamQuery(st);
+            if (e == cudaSuccess) {
+                if (*htok == seq) break;
+                // completed: the token write must be visible now; one more
+                // look, then fall back to the copy as written
+                break;
+            }
+            if (e != cudaErrorNotReady) return e;
+        }
+        if (i > 4096) std::this_thread::yield();
+#if defined(__x86_64__)
+        else __builtin_ia32_pause();
+#endif
+    }
+    std::atomic_thread_fence(std::memory_order_acquire);
     const unsigned char* h = static_cast<const unsigned char*>(b.host);
     for (int r = 0; r < n; ++r) std::memcpy(reqs[r].host, h + (size_t)a.dst_off[r] * 4, reqs[r].bytes);
     return cudaSuccess;
