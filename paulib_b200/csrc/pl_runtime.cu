@@ -12,7 +12,6 @@
 #include <cstdio>
 #include <mutex>
 #include <string>
-#include <thread>
 #include <vector>
 
 #include "pl_collate.cuh"
@@ -171,8 +170,8 @@ cudaError_t readback_sync(const ReadReq* reqs, int n, cudaStream_t st) {
     // runs after all earlier work of the stream, so its token means that work
     // is done too.  A poll of host memory needs no driver call; the stream is
     // queried now and then, for errors and in case the token write is not
-    // yet visible, and the thread yields once the wait gets long, leaving the
-    // core to threads that launch work.
+    // yet visible.  The thread spins (with a pause) rather than yielding: on
+    // a busy host a yield can hand the core away for a whole time slice.
     const volatile unsigned int* htok = reinterpret_cast<const volatile unsigned int*>(
         static_cast<const unsigned char*>(b.host) + b.bytes);
     for (unsigned long long i = 1; *htok != seq; ++i) {
@@ -186,9 +185,8 @@ cudaError_t readback_sync(const ReadReq* reqs, int n, cudaStream_t st) {
             }
             if (e != cudaErrorNotReady) return e;
         }
-        if (i > 4096) std::this_thread::yield();
 #if defined(__x86_64__)
-        else __builtin_ia32_pause();
+        __builtin_ia32_pause();
 #endif
     }
     std::atomic_thread_fence(std::memory_order_acquire);
