@@ -249,7 +249,8 @@ def run_product_collate(args, rank, local, ws):
     # (L2 prefetch one wave ahead / off) x keys per thread at a look-back
     # window of 4, then the window at the best of those; --tune fixes one
     # combination (profiling runs: fewer trial collates)
-    def trial(items, prefetch, window, wide=-1, backoff=64):
+    def trial(items, prefetch, window, wide=-1, backoff=64, gather=-1):
+        _abi.check(L.pl_set_tuning(_abi.PL_TUNE_FOLD_GATHER, gather), "pl_set_tuning")
         _abi.check(L.pl_set_tuning(_abi.PL_TUNE_RADIX_BACKOFF, backoff), "pl_set_tuning")
         _abi.check(L.pl_set_tuning(_abi.PL_TUNE_RADIX_ITEMS, items), "pl_set_tuning")
         _abi.check(L.pl_set_tuning(_abi.PL_TUNE_RADIX_PREFETCH, prefetch), "pl_set_tuning")
@@ -266,7 +267,8 @@ def run_product_collate(args, rank, local, ws):
         torch.cuda.synchronize()
         tune_trials.append({"radix_items": items, "radix_prefetch": prefetch,
                             "radix_window": window, "radix_wide": wide,
-                            "radix_backoff": backoff, "ms_per_step": t0.elapsed_time(t1) / 3})
+                            "radix_backoff": backoff, "fold_gather": gather,
+                            "ms_per_step": t0.elapsed_time(t1) / 3})
 
     if args.tune:
         trial(*(int(v) for v in args.tune.split(",")))
@@ -282,20 +284,24 @@ def run_product_collate(args, rank, local, ws):
         for backoff in (1, 4, 16):
             trial(b1["radix_items"], b1["radix_prefetch"], b1["radix_window"], b1["radix_wide"],
                   backoff)
+        b2 = min(tune_trials, key=lambda t: t["ms_per_step"])
+        trial(b2["radix_items"], b2["radix_prefetch"], b2["radix_window"], b2["radix_wide"],
+              b2["radix_backoff"], 1)
     best = min(tune_trials, key=lambda t: t["ms_per_step"])
-    best_items, best_pf, best_w, best_wide, best_bo = (
+    best_items, best_pf, best_w, best_wide, best_bo, best_g = (
         best["radix_items"], best["radix_prefetch"], best["radix_window"], best["radix_wide"],
-        best["radix_backoff"])
+        best["radix_backoff"], best["fold_gather"])
     if ws > 1:  # every rank uses rank 0's choice
         import torch.distributed as dist
-        t = torch.tensor([best_items, best_pf, best_w, best_wide, best_bo], device="cuda")
+        t = torch.tensor([best_items, best_pf, best_w, best_wide, best_bo, best_g], device="cuda")
         dist.broadcast(t, 0)
-        best_items, best_pf, best_w, best_wide, best_bo = (int(v) for v in t.tolist())
+        best_items, best_pf, best_w, best_wide, best_bo, best_g = (int(v) for v in t.tolist())
     _abi.check(L.pl_set_tuning(_abi.PL_TUNE_RADIX_ITEMS, best_items), "pl_set_tuning")
     _abi.check(L.pl_set_tuning(_abi.PL_TUNE_RADIX_PREFETCH, best_pf), "pl_set_tuning")
     _abi.check(L.pl_set_tuning(_abi.PL_TUNE_RADIX_WINDOW, best_w), "pl_set_tuning")
     _abi.check(L.pl_set_tuning(_abi.PL_TUNE_RADIX_WIDE, best_wide), "pl_set_tuning")
     _abi.check(L.pl_set_tuning(_abi.PL_TUNE_RADIX_BACKOFF, best_bo), "pl_set_tuning")
+    _abi.check(L.pl_set_tuning(_abi.PL_TUNE_FOLD_GATHER, best_g), "pl_set_tuning")
     for _ in range(args.warmup):
         n_out = step()
     torch.cuda.synchronize()
@@ -423,12 +429,13 @@ def run_product_collate(args, rank, local, ws):
         "result": {"terms_out": n_out},
         "tuned": {"radix_items": best_items, "radix_l2_prefetch": best_pf == 0,
                   "radix_lookback_window": best_w, "radix_digit_bits": 10 if best_wide > 0 else 8,
-                  "radix_lookback_hot_polls": best_bo,
+                  "radix_lookback_hot_polls": best_bo, "fold_gathers_coefficients": best_g > 0,
                   "trials_ms_per_step": {
                       ("prefetch" if t["radix_prefetch"] == 0 else "plain")
                       + f"-{t['radix_items']}-w{t['radix_window']}"
                       + ("-d10" if t["radix_wide"] > 0 else "-d8")
-                      + f"-b{t['radix_backoff']}": t["ms_per_step"]
+                      + f"-b{t['radix_backoff']}"
+                      + ("-fg" if t["fold_gather"] > 0 else ""): t["ms_per_step"]
                       for t in tune_trials}},
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d,
                 "d2h_bytes_per_step": int(statistics.mean(d2h)),
@@ -773,8 +780,9 @@ def main(argv=None):
                     help="serve workload: arrival rate as a multiple of the plain path's capacity")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--tune", default="",
-                    help="ITEMS,PREFETCH,WINDOW[,WIDE[,BACKOFF]]: fix the digit-pass tuning "
-                         "instead of timing the combinations (e.g. 16,0,4 or 12,0,8,-1,64)")
+                    help="ITEMS,PREFETCH,WINDOW[,WIDE[,BACKOFF[,FOLD_GATHER]]]: fix the "
+                         "digit-pass tuning instead of timing the combinations "
+                         "(e.g. 16,0,4 or 12,0,8,-1,16,1)")
     ap.add_argument("--no-extras", action="store_true",
                     help="product_collate: skip the GPU comparator, propagation and served "
                          "sub-objects")

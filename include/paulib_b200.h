@@ -485,6 +485,12 @@ PL_API int pl_serve(const pl_job* jobs, int64_t count, const pl_batch_opts* opts
  * warps of other tiles that rank and scatter.  Results are identical either
  * way. */
 #define PL_TUNE_RADIX_BACKOFF 9
+/* Where canonicalize() of a product takes each sorted term's phase and
+ * coefficient: 1: the segment fold gathers them from the operands by the
+ * term's index, so the last digit pass moves keys only; 0 (default) or -1:
+ * the last digit pass gathers them and writes the coefficients in sorted
+ * order.  Results are identical either way. */
+#define PL_TUNE_FOLD_GATHER 10
 /* Polls a cross-CTA wait (decoupled look-back) makes before it records
  * PL_ERR_TIMEOUT and returns: 1 .. 2^30, 0 = the default 2^20 (with a 64 ns
  * back-off past 64 polls: well under a second).  Written into the device

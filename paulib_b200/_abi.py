@@ -64,6 +64,7 @@ PL_TUNE_RADIX_PREFETCH = 6
 PL_TUNE_RADIX_WINDOW = 7
 PL_TUNE_RADIX_WIDE = 8
 PL_TUNE_RADIX_BACKOFF = 9
+PL_TUNE_FOLD_GATHER = 10
 PL_OPT_GRAPHS = 1
 PL_OPT_GATE_LOG = 2
 PL_ORDER_GIVEN = 0

@@ -1323,10 +1323,38 @@ __device__ __forceinline__ u32 fold_close(double* segval, u8* segflag, i64 h, do
     return keep ? 1u : 0u;
 }
 
-template <int MODE>
+// Where the fold takes each sorted term's fold word and coefficient: from
+// the sorted arrays (NoGather), or -- for a product whose last digit pass
+// moved keys only, index bits kept -- from the term's index: its phase / sign
+// bits from the bit planes and its coefficient lhs_j * rhs_i from the
+// operands (ProdGather), the values the last pass would have written.
+struct NoGather {
+    static constexpr bool kOn = false;
+    __device__ __forceinline__ void get(u64, u32&, double&) const {}
+};
+template <int AS>
+struct ProdGather {
+    ProdSrc<AS> src;
+    const uint2* phs;
+    u64 imask;
+    u32 n;  // products
+    int* status;
+    static constexpr bool kOn = true;
+    __device__ __forceinline__ void get(u64 key, u32& pe, double& ve) const {
+        const u32 idx = (u32)(key & imask);
+        u32 fl = 0;
+        double v = 0.0;
+        if (idx < n) src.flags_value(idx, phs, fl, v);
+        else raise_status(status, PL_ERR_INTERNAL);
+        pe = (fl & 1u) << 31;
+        ve = (fl & 2u) ? -v : v;
+    }
+};
+
+template <int MODE, class G = NoGather>
 __global__ void __launch_bounds__(32 * kFoldWarps, 6)
     k_fold(SegCtx C, double* segval, u8* segflag, u32* wfirst, u32* long_list, u32* counters,
-           FoldFilter F) {
+           FoldFilter F, G g) {
     extern __shared__ __align__(16) unsigned char fsm[];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const u32 gwarp = blockIdx.x * kFoldWarps + warp;
@@ -1339,7 +1367,7 @@ __global__ void __launch_bounds__(32 * kFoldWarps, 6)
         // batches after the first find them there instead of each waiting on
         // DRAM in turn
         prefetch_l2(C.keys + w0, 8u * (kFoldSpan + kLook));
-        prefetch_l2(C.vals + w0, 8u * (kFoldSpan + kLook));
+        if (!G::kOn) prefetch_l2(C.vals + w0, 8u * (kFoldSpan + kLook));
         if (MODE != kCanonSplit && C.pay) prefetch_l2(C.pay + w0, 4u * (kFoldSpan + kLook));
     }
     unsigned char* base = fsm + ((kFoldWarpSmem + 15) & ~size_t(15)) * warp;
@@ -1367,8 +1395,19 @@ __global__ void __launch_bounds__(32 * kFoldWarps, 6)
             const u32 i = (c0 + b) * 32 + lane;
             const bool valid = i < cnt;
             ke[b] = valid ? C.keys[w0 + i] : 0ull;
-            pe[b] = valid ? fold_word<MODE>(C, w0 + i, ke[b]) : 0u;
-            ve[b] = valid ? C.vals[w0 + i] : 0.0;
+            if constexpr (!G::kOn) {
+                pe[b] = valid ? fold_word<MODE>(C, w0 + i, ke[b]) : 0u;
+                ve[b] = valid ? C.vals[w0 + i] : 0.0;
+            }
+        }
+        if constexpr (G::kOn) {
+            // all the batch's keys are in flight first; then their gathers
+#pragma unroll
+            for (int b = 0; b < kBatch; ++b) {
+                pe[b] = 0u;
+                ve[b] = 0.0;
+                if ((c0 + b) * 32 + lane < cnt) g.get(ke[b], pe[b], ve[b]);
+            }
         }
 #pragma unroll
         for (int b = 0; b < kBatch; ++b) {
@@ -1416,8 +1455,14 @@ __global__ void __launch_bounds__(32 * kFoldWarps, 6)
             const u32 q = (u32)b * 32 + lane;
             const bool valid = q < look;
             ke[b] = valid ? C.keys[w1 + q] : 0ull;
-            pe[b] = valid ? fold_word<MODE>(C, w1 + q, ke[b]) : 0u;
-            ve[b] = valid ? C.vals[w1 + q] : 0.0;
+            if constexpr (G::kOn) {
+                pe[b] = 0u;
+                ve[b] = 0.0;
+                if (valid) g.get(ke[b], pe[b], ve[b]);
+            } else {
+                pe[b] = valid ? fold_word<MODE>(C, w1 + q, ke[b]) : 0u;
+                ve[b] = valid ? C.vals[w1 + q] : 0.0;
+            }
         }
 #pragma unroll
         for (int b = 0; b < (int)(kLook / 32); ++b) {
@@ -2120,19 +2165,20 @@ bool build_layout_split(int as, const u64* orm, const u64* andm, u32 n, KeyLayou
 
 // Segment sums: the warp fold, then the carry pass for the segments still
 // open after their range and its lookahead.
-template <int MODE>
-int fold_segments(const SegCtx& C, Bufs& B, const FoldFilter& F, int nsm, cudaStream_t st) {
+template <int MODE, class G = NoGather>
+int fold_segments(const SegCtx& C, Bufs& B, const FoldFilter& F, int nsm, cudaStream_t st,
+                  G g = G{}) {
     const u32 n = C.n;
     const u32 ngw = (n + kFoldSpan - 1) / kFoldSpan;
     const u32 fold_blocks = (ngw + kFoldWarps - 1) / kFoldWarps;
-    PL_CUDA_TRY(cudaFuncSetAttribute(k_fold<MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     (int)kFoldSmem));
+    PL_CUDA_TRY(cudaFuncSetAttribute(k_fold<MODE, G>,
+                                     cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kFoldSmem));
     // six CTAs (24 warps) per SM: 6 x 37 KB of staging
-    PL_CUDA_TRY(cudaFuncSetAttribute(k_fold<MODE>,
+    PL_CUDA_TRY(cudaFuncSetAttribute(k_fold<MODE, G>,
                                      cudaFuncAttributePreferredSharedMemoryCarveout,
                                      cudaSharedmemCarveoutMaxShared));
-    k_fold<MODE><<<fold_blocks, 32 * kFoldWarps, kFoldSmem, st>>>(
-        C, B.seg_sum, B.segflag, B.wfirst, B.long_list, B.counters, F), pl::note_launch();
+    k_fold<MODE, G><<<fold_blocks, 32 * kFoldWarps, kFoldSmem, st>>>(
+        C, B.seg_sum, B.segflag, B.wfirst, B.long_list, B.counters, F, g), pl::note_launch();
     // at most one pending segment per fold range
     const int cw_blocks = (int)std::min<u32>((ngw + 7) / 8, (u32)nsm * 4);
     k_fold_carry<MODE><<<cw_blocks, 256, 0, st>>>(B.wfirst, ngw, B.long_list, B.counters,
@@ -2484,10 +2530,13 @@ int run_collate_split(const Src& src, u32 n, const KeyLayout& L, const PassPlan&
                                                        B.hist), pl::note_launch();
     timed_end(e0, st, "k_pack", 8ull * n + n / 4);
     if (!scanned) k_scan_buckets<<<P.npasses, kRadix, 0, st>>>(B.hist, 0), pl::note_launch();
+    // a product's fold may take phases and coefficients from the operands
+    // itself (PL_TUNE_FOLD_GATHER), so the last digit pass moves keys only
+    const bool fold_gather = IsProd<Src>::value && tuning(PL_TUNE_FOLD_GATHER) > 0;
     u64 *kin = B.ka, *kout = B.kb;
     for (int p = 0; p < P.npasses; ++p) {
         cudaEvent_t ev0 = timed_begin(st);
-        const bool last = (p == P.npasses - 1);
+        const bool last = (p == P.npasses - 1) && !fold_gather;
         const u32* bs = B.hist + (size_t)p * R;
         u32* ctr = B.counters + 8 + p;
         u32* lb = (p & 1) ? B.lb2 : B.lb;
@@ -2519,12 +2568,23 @@ int run_collate_split(const Src& src, u32 n, const KeyLayout& L, const PassPlan&
         timed_end(ev0, st, "k_radix_pass", 16ull * n + (last ? 8ull * n + n / 4 : 0ull));
         std::swap(kin, kout);
     }
-    SegCtx C{kin, nullptr, B.sv, B.planes, n, 1, L.seg_mask0, kCanon};
+    // with the fold gathering, the sorted keys keep their index bits, which
+    // segment detection ignores
+    SegCtx C{kin, nullptr, B.sv, B.planes, n, 1, fold_gather ? ~imask : L.seg_mask0, kCanon};
     const u32 ngw = (n + kFoldSpan - 1) / kFoldSpan;
     const FoldFilter F{1,      a.cutoff,    nullptr,    seg2,      B.rpre,
                        B.ptail, reinterpret_cast<u64*>(B.seg_sum), B.rng_heads, B.rng_kept};
     e0 = timed_begin(st);
-    int rc = fold_segments<kCanonSplit>(C, B, F, nsm, st);
+    int rc = PL_OK;
+    if constexpr (IsProd<Src>::value) {
+        if (fold_gather)
+            rc = fold_segments<kCanonSplit>(C, B, F, nsm, st,
+                                            ProdGather<AS>{src, phs, imask, n, B.d_status});
+        else
+            rc = fold_segments<kCanonSplit>(C, B, F, nsm, st);
+    } else {
+        rc = fold_segments<kCanonSplit>(C, B, F, nsm, st);
+    }
     if (rc != PL_OK) return rc;
     timed_end(e0, st, "k_fold", 16ull * n);
     e0 = timed_begin(st);

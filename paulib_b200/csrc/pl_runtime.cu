@@ -425,7 +425,8 @@ extern "C" int pl_set_tuning(int key, int64_t value) {
         pl::g_tuning[key].store(value);
         return pl::record_status(PL_OK, nullptr);
     }
-    if ((key == PL_TUNE_INDEX_KEYS || key == PL_TUNE_WINDOW_KEYS || key == PL_TUNE_RADIX_WIDE) &&
+    if ((key == PL_TUNE_INDEX_KEYS || key == PL_TUNE_WINDOW_KEYS || key == PL_TUNE_RADIX_WIDE ||
+         key == PL_TUNE_FOLD_GATHER) &&
         (value == 0 || value == 1 || value == -1)) {
         pl::g_tuning[key].store(value);
         return pl::record_status(PL_OK, nullptr);

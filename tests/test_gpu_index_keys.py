@@ -248,3 +248,35 @@ def test_lookback_backoff(cuda, backoff):
         on = gpu_multiply_collate(a, b)
     off = gpu_multiply_collate(a, b)
     assert _bits_equal(on, off)
+
+
+@pytest.mark.parametrize("items", [8, 12, 16])
+@pytest.mark.parametrize("terms,seed", [(4096, 0), (1024, 5), (96, 2)])
+def test_fold_gathers_coefficients(cuda, oracle, items, terms, seed):
+    # The fold taking each product's phase and coefficient from the operands
+    # by index (the last digit pass moving keys only) against the last pass
+    # gathering them: bit-identical; the smaller cases also against the oracle.
+    a, b = W.product_operands(seed=seed, terms=terms)
+    a, b = as_planes(a), as_planes(b)
+    with tuned(_abi.PL_TUNE_RADIX_ITEMS, items):
+        with tuned(_abi.PL_TUNE_FOLD_GATHER, 1):
+            on = gpu_multiply_collate(a, b)
+            again = gpu_multiply_collate(a, b)
+        with tuned(_abi.PL_TUNE_FOLD_GATHER, -1):
+            off = gpu_multiply_collate(a, b)
+    assert on.n > 0 and _bits_equal(on, off) and _bits_equal(on, again)
+    if terms <= 1024:
+        prod = oracle.multiply(a, b)
+        o = oracle.canonicalize(prod)
+        assert_keys_equal(on, o)
+        assert_values_close(on, o, abs_scale(oracle, prod))
+
+
+def test_fold_gathers_with_cutoff(cuda, oracle):
+    a, b = W.product_operands(seed=13, terms=512)
+    a, b = as_planes(a), as_planes(b)
+    with tuned(_abi.PL_TUNE_FOLD_GATHER, 1):
+        on = gpu_multiply_collate(a, b, cutoff=0.05)
+    with tuned(_abi.PL_TUNE_FOLD_GATHER, -1):
+        off = gpu_multiply_collate(a, b, cutoff=0.05)
+    assert _bits_equal(on, off)
