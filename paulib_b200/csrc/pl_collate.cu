@@ -353,6 +353,42 @@ __global__ void __launch_bounds__(256) k_masks(SoASrc<AS> src, u32 n, int mode, 
 // ---------------------------------------------------------------------------
 // Masks of the windowed virtual key (as k_masks) and whether every term fits
 // the window form (bad[0] != 0: some term does not).
+// OR masks of the x / z words of both operands of a product, one launch and
+// no initialisation: blockIdx.y picks the operand, and each block writes its
+// partial OR to part[(y * gridDim.x + x) * 2AS + f]; the host ORs the blocks.
+template <int AS>
+__global__ void __launch_bounds__(256) k_operand_or(SoASrc<AS> a, u32 na, SoASrc<AS> b, u32 nb,
+                                                    u64* part) {
+    __shared__ u64 sw[kWarps][2 * AS];
+    const SoASrc<AS>& src = blockIdx.y ? b : a;
+    const u32 n = blockIdx.y ? nb : na;
+    u64 o[2 * AS];
+#pragma unroll
+    for (int f = 0; f < 2 * AS; ++f) o[f] = 0;
+    for (u32 i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        u64 xw[AS], zw[AS];
+        u32 fl;
+        src.key(i, xw, zw, fl);
+#pragma unroll
+        for (int k = 0; k < AS; ++k) {
+            o[k] |= xw[k];
+            o[AS + k] |= zw[k];
+        }
+    }
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+    for (int f = 0; f < 2 * AS; ++f) {
+        for (int d = 16; d > 0; d >>= 1) o[f] |= __shfl_xor_sync(0xffffffffu, o[f], d);
+        if (lane == 0) sw[warp][f] = o[f];
+    }
+    __syncthreads();
+    if (threadIdx.x < 2 * AS) {
+        u64 v = 0;
+        for (int w = 0; w < kWarps; ++w) v |= sw[w][threadIdx.x];
+        part[((size_t)blockIdx.y * gridDim.x + blockIdx.x) * (2 * AS) + threadIdx.x] = v;
+    }
+}
+
 template <int AS>
 __global__ void __launch_bounds__(256) k_win_masks(WinSrc<AS> src, u32 n, int mode, u64* orm,
                                                    u64* andm, u32* bad) {
@@ -2756,20 +2792,24 @@ int multiply_collate(int as, const SoAView& lhs, const SoAView& rhs, const SoAOu
         // Varying bits of a product lie inside OR(lhs) | OR(rhs) word by word;
         // the operand masks give a conservative layout without touching the
         // n*m products.
-        // both operands' masks, one read-back
-        u64 hor[2][kMaxFields];
-        const SoAView* ops[2] = {&lhs, &rhs};
-        const FillReq fm[2] = {{B.orm, 0u, 8 * 2 * kMaxFields},
-                               {B.andm, 0xffffffffu, 8 * 2 * kMaxFields}};
-        PL_CUDA_TRY(fill32_multi(fm, 2, st));
-        for (int w = 0; w < 2; ++w) {
-            SoASrc<AS> s{ops[w]->x, ops[w]->z, ops[w]->f, ops[w]->v, ops[w]->stride};
-            k_masks<AS><<<grid_for(ops[w]->n, 256, sm_count() * 4), 256, 0, st>>>(
-                s, (u32)ops[w]->n, a.mode, B.orm + w * kMaxFields, B.andm + w * kMaxFields),
-                pl::note_launch();
-        }
-        const ReadReq rr[1] = {{hor, B.orm, 8 * 2 * kMaxFields}};
+        // both operands' OR masks: one launch of per-block partials (no
+        // clearing launch), one read-back, reduced here
+        u64 hor[2][kMaxFields] = {};
+        constexpr int kOrBlocks = 16;
+        const SoASrc<AS> sa{lhs.x, lhs.z, lhs.f, lhs.v, lhs.stride};
+        const SoASrc<AS> sb{rhs.x, rhs.z, rhs.f, rhs.v, rhs.stride};
+        const int gx = grid_for(std::max(lhs.n, rhs.n), 256, kOrBlocks);
+        // the operand-histogram scratch, unused until after this read-back
+        // (8192 u64 words; the partials take at most 2 x 16 x 32)
+        u64* part = reinterpret_cast<u64*>(B.counters + kHistScratch);
+        k_operand_or<AS><<<dim3(gx, 2), 256, 0, st>>>(sa, (u32)lhs.n, sb, (u32)rhs.n, part),
+            pl::note_launch();
+        u64 hpart[2 * kOrBlocks * 2 * AS];
+        const ReadReq rr[1] = {{hpart, part, sizeof(u64) * 2 * (size_t)gx * 2 * AS}};
         PL_CUDA_TRY(readback_sync(rr, 1, st));
+        for (int w = 0; w < 2; ++w)
+            for (int g = 0; g < gx; ++g)
+                for (int f = 0; f < 2 * AS; ++f) hor[w][f] |= hpart[(w * gx + g) * 2 * AS + f];
         u64 por[kMaxFields], pand[kMaxFields];
         for (int f = 0; f < 2 * AS; ++f) {
             por[f] = hor[0][f] | hor[1][f];
