@@ -2225,13 +2225,13 @@ int fold_segments(const SegCtx& C, Bufs& B, const FoldFilter& F, int nsm, cudaSt
 // Histograms that can be derived instead of counted: none for a plain sum.
 template <int AS>
 u32 derive_histograms(const SoASrc<AS>&, const KeyLayout&, const PassPlan&, Bufs&, cudaStream_t,
-                      bool* scanned, u64* = nullptr, int = kRadix) {
+                      bool* scanned, u64* = nullptr, int = kRadix, bool = false) {
     *scanned = false;
     return 0u;
 }
 template <int AS>
 u32 derive_histograms(const WinSrc<AS>&, const KeyLayout&, const PassPlan&, Bufs&, cudaStream_t,
-                      bool* scanned, u64* = nullptr, int = kRadix) {
+                      bool* scanned, u64* = nullptr, int = kRadix, bool = false) {
     *scanned = false;
     return 0u;
 }
@@ -2241,7 +2241,8 @@ u32 derive_histograms(const WinSrc<AS>&, const KeyLayout&, const PassPlan&, Bufs
 // starts and *scanned is set (no k_scan_buckets needed).
 template <int AS>
 u32 derive_histograms(const ProdSrc<AS>& src, const KeyLayout& L, const PassPlan& P, Bufs& B,
-                      cudaStream_t st, bool* scanned, u64* opk = nullptr, int R = kRadix) {
+                      cudaStream_t st, bool* scanned, u64* opk = nullptr, int R = kRadix,
+                      bool prefilled = false) {
     *scanned = false;
     const int np0 = P.first[1] - P.first[0];
     const int wf = L.width[2 * AS];  // the flags field occupies packed bits [0, wf)
@@ -2253,7 +2254,8 @@ u32 derive_histograms(const ProdSrc<AS>& src, const KeyLayout& L, const PassPlan
     // 1024: at most 4 passes, 4 x R)
     u32* hA = B.counters + kHistScratch;
     u32* hB = hA + (R == kRadix ? 8 : 4) * R;
-    if (fill32_async(hA, 0u, sizeof(u32) * (R == kRadix ? 16 : 8) * R, st) != cudaSuccess)
+    if (!prefilled &&
+        fill32_async(hA, 0u, sizeof(u32) * (R == kRadix ? 16 : 8) * R, st) != cudaSuccess)
         return 0u;
     const SoASrc<AS> a{src.ax, src.az, src.af, src.av, src.sa};
     const SoASrc<AS> b{src.bx, src.bz, src.bf, src.bv, src.sb};
@@ -2543,19 +2545,22 @@ int run_collate_split(const Src& src, u32 n, const KeyLayout& L, const PassPlan&
     double2* seg2 = reinterpret_cast<double2*>(reinterpret_cast<unsigned char*>(B.planes) + al(n));
     // the look-back words of the first digit pass; every pass clears the
     // next one's
-    const FillReq fr[5] = {{B.hist, 0u, sizeof(u32) * (size_t)std::max(P.npasses, 1) * R},
+    // (and the operand-histogram scratch a product's derived histograms use)
+    const FillReq fr[6] = {{B.hist, 0u, sizeof(u32) * (size_t)std::max(P.npasses, 1) * R},
                            {B.counters, 0u, sizeof(u32) * (size_t)(P.npasses + 8)},
                            {B.d_status, 0u, sizeof(int)},
                            {B.d_count, 0u, sizeof(i64)},
-                           {B.lb, 0u, sizeof(u32) * (size_t)rtiles * R}};
-    PL_CUDA_TRY(fill32_multi(fr, 5, st));
+                           {B.lb, 0u, sizeof(u32) * (size_t)rtiles * R},
+                           {B.counters + kHistScratch, 0u,
+                            sizeof(u32) * (size_t)(R == kRadix ? 16 : 8) * R}};
+    PL_CUDA_TRY(fill32_multi(fr, 6, st));
     const int gblocks = grid_for(n, 256, nsm * 8);
     cudaEvent_t e0 = timed_begin(st);
     bool scanned = false;
     // a product's operand packed keys go to B.sv, unused until the last
     // digit pass writes the sorted coefficients there
     u64* opk = operand_key_room(src, n) ? reinterpret_cast<u64*>(B.sv) : nullptr;
-    const u32 derived = derive_histograms<AS>(src, L, P, B, st, &scanned, opk, R);
+    const u32 derived = derive_histograms<AS>(src, L, P, B, st, &scanned, opk, R, true);
     if (wide && !scanned) return record_status(PL_ERR_INTERNAL, "collate: 10-bit digit plan");
     timed_end(e0, st, "k_xor_conv", 0ull);
     const u32 count_mask = ~derived & ((1u << P.npasses) - 1u);
