@@ -1686,10 +1686,18 @@ __global__ void __launch_bounds__(32 * kFoldWarps, 6)
 // the first one with a head; its sum is its value at the end of its range
 // plus those ranges' prefix partials, added 32 ranges at a time in a fixed
 // tree.  One warp per pending segment.
-template <int MODE>
-__global__ void __launch_bounds__(256) k_fold_carry(const u32* wfirst, u32 ngw,
-                                                    const u32* long_list, const u32* counters,
-                                                    double* segval, u8* segflag, FoldFilter F) {
+//
+// SCAN (kCanonSplit, 1024-thread blocks): the last block to finish then turns
+// the ranges' kept counts into their output offsets (the tile scan), so the
+// record emit follows without a launch in between.  done: a zeroed counter.
+__device__ __forceinline__ void tile_scan_block(const u32* tile_kept, u32 tiles, u32* tile_off,
+                                                i64* d_out_count, u32* sw);
+
+template <int MODE, bool SCAN = false>
+__global__ void __launch_bounds__(SCAN ? 1024 : 256)
+    k_fold_carry(const u32* wfirst, u32 ngw, const u32* long_list, const u32* counters,
+                 double* segval, u8* segflag, FoldFilter F, u32* rng_off = nullptr,
+                 i64* d_out_count = nullptr, u32* done = nullptr) {
     const u32 npend = counters[2];
     const int lane = threadIdx.x & 31;
     const u32 nw = (gridDim.x * blockDim.x) >> 5;
@@ -1720,6 +1728,20 @@ __global__ void __launch_bounds__(256) k_fold_carry(const u32* wfirst, u32 ngw,
             } else if (F.on && keep) {
                 atomicAdd(&F.tile_kept[h / kETile], keep);
             }
+        }
+    }
+    if constexpr (SCAN) {
+        __shared__ u32 s_last;
+        __shared__ u32 sw[65];
+        __syncthreads();  // this block's carries (and their count atomics) are done
+        if (threadIdx.x == 0) {
+            __threadfence();
+            s_last = atomicAdd(done, 1u) == gridDim.x - 1 ? 1u : 0u;
+        }
+        __syncthreads();
+        if (s_last) {
+            __threadfence();
+            tile_scan_block(F.rng_kept, ngw, rng_off, d_out_count, sw);
         }
     }
 }
@@ -1761,13 +1783,20 @@ __device__ __forceinline__ u32 block_scan_n(u32 v, u32* s_warp, u32& total) {
 __global__ void __launch_bounds__(1024) k_tile_scan(const u32* tile_kept, u32 tiles,
                                                     u32* tile_off, i64* d_out_count) {
     __shared__ u32 sw[65];
+    tile_scan_block(tile_kept, tiles, tile_off, d_out_count, sw);
+}
+
+// The scan itself, by one 1024-thread block (counts read past L1: another
+// block of the same kernel may have just added to them).
+__device__ __forceinline__ void tile_scan_block(const u32* tile_kept, u32 tiles, u32* tile_off,
+                                                i64* d_out_count, u32* sw) {
     const u32 per = (tiles + 1023u) / 1024u;
     const u32 b = threadIdx.x * per, e = min(b + per, tiles);
     u32 total;
     if (per <= 16) {
         u32 c[16];
 #pragma unroll
-        for (int k = 0; k < 16; ++k) c[k] = b + k < e ? tile_kept[b + k] : 0u;
+        for (int k = 0; k < 16; ++k) c[k] = b + k < e ? __ldcg(tile_kept + b + k) : 0u;
         u32 s = 0;
 #pragma unroll
         for (int k = 0; k < 16; ++k) s += c[k];
@@ -1779,11 +1808,11 @@ __global__ void __launch_bounds__(1024) k_tile_scan(const u32* tile_kept, u32 ti
         }
     } else {
         u32 s = 0;
-        for (u32 i = b; i < e; ++i) s += tile_kept[i];
+        for (u32 i = b; i < e; ++i) s += __ldcg(tile_kept + i);
         u32 run = block_scan_n<32>(s, sw, total);
         for (u32 i = b; i < e; ++i) {
             tile_off[i] = run;
-            run += tile_kept[i];
+            run += __ldcg(tile_kept + i);
         }
     }
     if (threadIdx.x == 0) *d_out_count = (i64)total;
@@ -2216,9 +2245,20 @@ int fold_segments(const SegCtx& C, Bufs& B, const FoldFilter& F, int nsm, cudaSt
     k_fold<MODE, G><<<fold_blocks, 32 * kFoldWarps, kFoldSmem, st>>>(
         C, B.seg_sum, B.segflag, B.wfirst, B.long_list, B.counters, F, g), pl::note_launch();
     // at most one pending segment per fold range
-    const int cw_blocks = (int)std::min<u32>((ngw + 7) / 8, (u32)nsm * 4);
-    k_fold_carry<MODE><<<cw_blocks, 256, 0, st>>>(B.wfirst, ngw, B.long_list, B.counters,
-                                                  B.seg_sum, B.segflag, F), pl::note_launch();
+    if constexpr (MODE == kCanonSplit) {
+        // ... and the tile scan in the last block (counters[4]: zeroed at the
+        // start of the call)
+        const int cw = (int)std::max<u32>(1u, std::min<u32>((ngw + 31) / 32, (u32)nsm));
+        k_fold_carry<MODE, true><<<cw, 1024, 0, st>>>(B.wfirst, ngw, B.long_list, B.counters,
+                                                       B.seg_sum, B.segflag, F, B.rng_off,
+                                                       B.d_count, B.counters + 4),
+            pl::note_launch();
+    } else {
+        const int cw_blocks = (int)std::min<u32>((ngw + 7) / 8, (u32)nsm * 4);
+        k_fold_carry<MODE><<<cw_blocks, 256, 0, st>>>(B.wfirst, ngw, B.long_list, B.counters,
+                                                      B.seg_sum, B.segflag, F),
+            pl::note_launch();
+    }
     return PL_OK;
 }
 
@@ -2629,7 +2669,7 @@ int run_collate_split(const Src& src, u32 n, const KeyLayout& L, const PassPlan&
     if (rc != PL_OK) return rc;
     timed_end(e0, st, "k_fold", 16ull * n);
     e0 = timed_begin(st);
-    k_tile_scan<<<1, 1024, 0, st>>>(B.rng_kept, ngw, B.rng_off, B.d_count), pl::note_launch();
+    // (the tile scan ran in the carry pass's last block)
     k_emit_records<AS><<<(ngw + kWarps - 1) / kWarps, kThreads, 0, st>>>(
         L, reinterpret_cast<const u64*>(B.seg_sum), seg2, B.rng_heads, B.rng_off, ngw, a.cutoff,
         out, B.d_status),
